@@ -1,0 +1,182 @@
+/* rbk.h -- C ABI of the B200 state-vector engine (librbk.so).
+ *
+ * One state vector of 2^n amplitudes lives in one GPU's HBM, as
+ * complex<double> (RBK_C128, n <= 33) or complex<float> (RBK_C64, n <= 34).
+ * Gates are the ones of RIKEN-braket's ket library and bra's .qcx
+ * instruction set; each entry point below names the reference function it
+ * replaces.  Reference paths are relative to the RIKEN-braket project root.
+ *
+ * Conventions
+ *  - Every function returns an rbk_status; 0 (RBK_OK) is success.  On failure
+ *    rbk_last_error() returns a message for the calling thread.  No C++
+ *    exception crosses this interface.
+ *  - Qubit q is bit q of the amplitude index (ket::qubit, ket/include/ket/qubit.hpp:10-53).
+ *    Control qubits are given as an array of qubit indices (ket::control).
+ *  - Gate angles and coefficients are turned into gate coefficients on the
+ *    host in double precision, with the same formulas as ket (std::sin,
+ *    std::cos, std::exp(i theta)); kernels receive coefficients, never angles.
+ *  - Gates are queued on the state and executed in fused passes when a result
+ *    is read (download, reductions, rbk_state_synchronize, rbk_flush).  The
+ *    queue is invisible except through timing: every read sees all gates
+ *    issued before it.  rbk_state_set_deferred(s, 0) executes each gate as
+ *    soon as it is issued (one pass per gate, like ket).
+ *  - A state is used from one host thread at a time.  Every state has its own
+ *    CUDA stream.  Host waits are bounded (RBK_ERR_TIMEOUT).
+ */
+#ifndef RBK_H
+#define RBK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef enum rbk_status {
+  RBK_OK = 0,
+  RBK_ERR_INVALID = 1,      /* bad argument: qubit out of range, repeated qubit, null pointer, size */
+  RBK_ERR_CUDA = 2,         /* a CUDA call failed (message has the CUDA error string) */
+  RBK_ERR_OOM = 3,          /* device memory exhausted */
+  RBK_ERR_TIMEOUT = 4,      /* a bounded host wait expired */
+  RBK_ERR_UNSUPPORTED = 5,  /* operation not available for this precision / size */
+  RBK_ERR_STATE = 6         /* call out of order, e.g. END FUSION without BEGIN FUSION */
+} rbk_status;
+
+typedef enum rbk_precision { RBK_C128 = 0, RBK_C64 = 1 } rbk_precision;
+
+typedef struct rbk_state rbk_state;
+
+/* Execution statistics of one state since creation (or the last reset_stats). */
+typedef struct rbk_stats {
+  uint64_t gates_issued;     /* gate calls accepted */
+  uint64_t passes;           /* fused read+write passes over the whole state */
+  uint64_t gate_launches;    /* unfused single-gate kernel launches */
+  uint64_t reduction_passes; /* read-only passes (observables) */
+  uint64_t relabel_passes;   /* passes that only moved qubits (layout changes) */
+  uint64_t kernel_launches;  /* all kernels launched */
+} rbk_stats;
+
+const char* rbk_last_error(void);
+int rbk_version(void);
+
+/* ---- state lifecycle ------------------------------------------------------
+ * Replaces std::vector<complex> state creation in bra::nompi_state
+ * (bra/src/nompi_state.cpp:120-137, make_initial_data) and the single-process
+ * ket::mpi::state<Complex, false> (ket/include/ket/mpi/state.hpp:1973-2100,
+ * ctor :1990-2000): the state is |initial_index>. */
+int rbk_state_create(int num_qubits, int precision, uint64_t initial_index, int device, rbk_state** out);
+int rbk_state_destroy(rbk_state* s);
+int rbk_state_num_qubits(const rbk_state* s, int* out);
+int rbk_state_precision(const rbk_state* s, int* out);
+/* Sets the state to |index> (drops queued gates). */
+int rbk_state_reset(rbk_state* s, uint64_t index);
+/* Copies count amplitudes starting at logical index offset from / to host
+ * memory (interleaved re, im of the state's precision).  Logical order: the
+ * layout permutation is undone first (see rbk_state_get_permutation). */
+int rbk_state_upload(rbk_state* s, const void* host, uint64_t offset, uint64_t count);
+int rbk_state_download(rbk_state* s, void* host, uint64_t offset, uint64_t count);
+/* Executes queued gates and waits for the device (bounded wait). */
+int rbk_state_synchronize(rbk_state* s);
+int rbk_flush(rbk_state* s);
+/* 1: queue gates and fuse them (default); 0: one pass per gate as issued. */
+int rbk_state_set_deferred(rbk_state* s, int deferred);
+/* Upper bound on dense 2x2 gates per fused pass (0 = built-in default). */
+int rbk_state_set_pass_budget(rbk_state* s, int max_dense_gates_per_pass);
+int rbk_state_get_stats(const rbk_state* s, rbk_stats* out);
+int rbk_state_reset_stats(rbk_state* s);
+/* Milliseconds of device time spent in this state's kernels since the last
+ * reset_stats (CUDA events around each executed queue). */
+int rbk_state_device_ms(rbk_state* s, double* out);
+
+/* ---- layout map ----------------------------------------------------------
+ * The single-device use of ket::mpi::qubit_permutation
+ * (ket/include/ket/mpi/qubit_permutation.hpp:40-302): perm[q] is the physical
+ * bit that holds logical qubit q.  SWAP gates and pass relabelling only change
+ * the map.  rbk_state_canonicalize moves the data so that perm is the
+ * identity (the in-place swap of swap_permutated_local_qubits,
+ * ket/include/ket/mpi/utility/detail/swap_permutated_local_qubits.hpp:26-81,
+ * done several qubits per pass). */
+int rbk_state_get_permutation(rbk_state* s, uint32_t* perm);
+int rbk_state_canonicalize(rbk_state* s);
+/* Device pointer to the amplitudes in physical order (after a flush). */
+int rbk_state_device_pointer(rbk_state* s, void** out);
+
+/* ---- fusion (bra BEGIN FUSION / END FUSION, bra/src/state.cpp:2193-2217,
+ *      bra/src/nompi_state.cpp:1285-1357) --------------------------------- */
+int rbk_begin_fusion(rbk_state* s);
+int rbk_end_fusion(rbk_state* s);
+
+/* ---- gates -----------------------------------------------------------------
+ * `controls` may be NULL when num_controls is 0. */
+
+/* ket::gate::hadamard (ket/include/ket/gate/hadamard.hpp:34-140) */
+int rbk_hadamard(rbk_state* s, uint32_t target, const uint32_t* controls, int num_controls);
+/* ket::gate::pauli_x / not_ / controlled_not (pauli_x.hpp:34-165, not_.hpp:33-51) */
+int rbk_pauli_x(rbk_state* s, uint32_t target, const uint32_t* controls, int num_controls);
+/* ket::gate::pauli_y (pauli_y.hpp:36-134) */
+int rbk_pauli_y(rbk_state* s, uint32_t target, const uint32_t* controls, int num_controls);
+/* ket::gate::pauli_z on control qubits: Z c = pauli_z(c), CZ c1 c2 = pauli_z(c1, c2)
+ * (pauli_z.hpp:58-137).  qubits holds 1 + num_controls qubit indices. */
+int rbk_pauli_z(rbk_state* s, const uint32_t* qubits, int num_qubits);
+/* ket::gate::phase_shift_coeff: multiplies the amplitudes whose listed qubits
+ * are all one by (re, im) (phase_shift.hpp:63-142); U1, CU1, S, T, "U c1 c2 k". */
+int rbk_phase_shift_coeff(rbk_state* s, double re, double im, const uint32_t* qubits, int num_qubits);
+/* ket::gate::phase_shift (U1 with a real phase; phase_shift.hpp:513-521) */
+int rbk_phase_shift(rbk_state* s, double phase, const uint32_t* qubits, int num_qubits);
+/* "U c1 c2 k" / "R c k": phase 2 pi / 2^k from bra's phase table
+ * (bra/src/state.cpp:148 and :2650-2669, generate_phase_coefficients.hpp:20-39);
+ * negative k applies the adjoint. */
+int rbk_controlled_phase_shift_k(rbk_state* s, int k, const uint32_t* qubits, int num_qubits);
+/* ket::gate::phase_shift2 = U2 (phase_shift.hpp:660-709) */
+int rbk_phase_shift2(rbk_state* s, double phase1, double phase2, uint32_t target, const uint32_t* controls, int num_controls);
+/* ket::gate::phase_shift3 = U3 (phase_shift.hpp:1200-1332) */
+int rbk_phase_shift3(rbk_state* s, double phase1, double phase2, double phase3, uint32_t target,
+                     const uint32_t* controls, int num_controls);
+/* ket::gate::exponential_pauli_{x,y,z}: exp(i theta P) (exponential_pauli_y.hpp:40-85,
+ * :473-481; exponential_pauli_z.hpp:40-78, :369-377) */
+int rbk_exponential_pauli_x(rbk_state* s, double phase, uint32_t target, const uint32_t* controls, int num_controls);
+int rbk_exponential_pauli_y(rbk_state* s, double phase, uint32_t target, const uint32_t* controls, int num_controls);
+int rbk_exponential_pauli_z(rbk_state* s, double phase, uint32_t target, const uint32_t* controls, int num_controls);
+/* ket::gate::swap (swap.hpp:34-75).  Uncontrolled swaps only relabel the layout map. */
+int rbk_swap(rbk_state* s, uint32_t qubit1, uint32_t qubit2, const uint32_t* controls, int num_controls);
+/* Any 2x2 unitary: m = {m00re, m00im, m01re, m01im, m10re, m10im, m11re, m11im}
+ * (the generic 1-target form of ket::gate::gate, ket/include/ket/gate/gate.hpp). */
+int rbk_apply_matrix2(rbk_state* s, const double* m, uint32_t target, const uint32_t* controls, int num_controls);
+/* diag(d0, d1) on target: d = {d0re, d0im, d1re, d1im}. */
+int rbk_apply_diagonal2(rbk_state* s, const double* d, uint32_t target, const uint32_t* controls, int num_controls);
+
+/* ---- observables ---------------------------------------------------------- */
+/* sum |a_i|^2 */
+int rbk_norm2(rbk_state* s, double* out);
+/* |a_i|^2 for logical indices [offset, offset + count) into host memory
+ * (measure.hpp:16-46, generate_events.hpp:18-51 use these). */
+int rbk_probabilities(rbk_state* s, double* host_out, uint64_t offset, uint64_t count);
+/* DO MEASUREMENT: ket::all_spin_expectation_values (all_spin_expectation_values.hpp:22-42,
+ * spin_expectation_value.hpp:21-80): out[3q + {0,1,2}] = <S_x>, <S_y>, <S_z> of
+ * logical qubit q, in spin-1/2 units (half the Pauli expectation). */
+int rbk_spin_expectation_values(rbk_state* s, double* out);
+/* EXPECTATION: sum_t coeff_t <psi|P_t|psi> (bra/src/nompi_state.cpp:1155-1202,
+ * ket/include/ket/gate/utility/pauli_index_coeff.hpp:17-59).  strings holds
+ * num_terms strings of n characters from "IXYZ", character k acting on
+ * logical qubit k; coeffs holds num_terms (re, im) pairs; out = (re, im). */
+int rbk_expectation_pauli(rbk_state* s, int num_terms, const char* strings, const double* coeffs, double* out);
+/* ket::inner_product(a, b) = <b|a> = sum conj(b_i) a_i (inner_product.hpp:30-56); out = (re, im).
+ * Both states must have the same size and precision. */
+int rbk_inner_product(rbk_state* a, rbk_state* b, double* out);
+/* ket::fidelity: |<b|a>|^2 (fidelity.hpp) */
+int rbk_fidelity(rbk_state* a, rbk_state* b, double* out);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBK_H */

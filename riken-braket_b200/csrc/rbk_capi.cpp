@@ -1,0 +1,931 @@
+// rbk_capi.cpp -- the C ABI of include/rbk.h: state handles, named gates,
+// the deferred gate queue, execution of planned passes, observables.
+#include "rbk.h"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "rbk_internal.h"
+#include "rbk_kernels.h"
+#include "rbk_plan.h"
+
+using rbk::hgate;
+
+struct rbk_state {
+  int n = 0;
+  int precision = RBK_C128;
+  int device = 0;
+  void* amps = nullptr;
+  cudaStream_t stream = nullptr;
+  double* d_partials = nullptr;
+  double* d_out = nullptr;
+  double* h_out = nullptr;  // pinned
+  std::vector<int> perm, inv;
+  std::vector<hgate> queue;
+  bool deferred = true;
+  bool in_fusion = false;
+  int dense_budget = 0;
+  rbk_stats stats{};
+  cudaEvent_t ev_first = nullptr, ev_last = nullptr, ev_sync = nullptr;
+  bool timing_started = false;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg)
+{
+  g_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+  const int code = (e == cudaErrorMemoryAllocation) ? RBK_ERR_OOM : RBK_ERR_CUDA;
+  return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RBK_CUDA(call)                                    \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+struct device_guard {
+  int prev = -1;
+  explicit device_guard(int dev)
+  {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~device_guard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+double wait_timeout_seconds()
+{
+  const char* v = std::getenv("RBK_TIMEOUT_S");
+  if (v) { const double t = std::atof(v); if (t > 0) return t; }
+  return 600.0;
+}
+
+// Bounded wait for everything issued on the state's stream.
+int bounded_sync(rbk_state* s)
+{
+  RBK_CUDA(cudaEventRecord(s->ev_sync, s->stream));
+  const auto t0 = std::chrono::steady_clock::now();
+  const double limit = wait_timeout_seconds();
+  int sleep_us = 20;
+  while (true) {
+    const cudaError_t e = cudaEventQuery(s->ev_sync);
+    if (e == cudaSuccess) return RBK_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(e, "device execution");
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > limit) return fail(RBK_ERR_TIMEOUT, "timed out waiting for the device");
+    std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+    if (sleep_us < 2000) sleep_us *= 2;
+  }
+}
+
+inline size_t amp_bytes(int precision) { return precision == RBK_C128 ? 16 : 8; }
+
+rbk::plan_params params_of(const rbk_state* s)
+{
+  rbk::plan_params p{};
+  p.n = s->n;
+  if (s->precision == RBK_C128) {
+    p.K = rbk::tiling<double>::K; p.R = rbk::tiling<double>::R; p.LOW = rbk::tiling<double>::LOW; p.vbits = 0;
+  } else {
+    p.K = rbk::tiling<float>::K; p.R = rbk::tiling<float>::R; p.LOW = rbk::tiling<float>::LOW; p.vbits = 1;
+  }
+  p.dense_budget = s->dense_budget > 0 ? s->dense_budget : (s->precision == RBK_C128 ? 12 : 16);
+  return p;
+}
+
+int tile_bits(const rbk_state* s) { return s->precision == RBK_C128 ? rbk::tiling<double>::K : rbk::tiling<float>::K; }
+
+int mark_launch_start(rbk_state* s)
+{
+  if (!s->timing_started) {
+    RBK_CUDA(cudaEventRecord(s->ev_first, s->stream));
+    s->timing_started = true;
+  }
+  return RBK_OK;
+}
+
+int run_passes(rbk_state* s, const std::vector<rbk::dev_pass>& passes)
+{
+  for (const auto& pass : passes) {
+    const cudaError_t e = s->precision == RBK_C128
+      ? rbk::launch_tile_pass<double>(s->amps, s->n, pass, s->stream)
+      : rbk::launch_tile_pass<float>(s->amps, s->n, pass, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tile pass launch");
+    ++s->stats.kernel_launches;
+  }
+  return RBK_OK;
+}
+
+int flush(rbk_state* s)
+{
+  if (s->queue.empty()) return RBK_OK;
+  device_guard g(s->device);
+  int rc = mark_launch_start(s);
+  if (rc) return rc;
+  try {
+    if (s->n >= tile_bits(s)) {
+      std::vector<rbk::dev_pass> passes;
+      rbk::plan_passes(params_of(s), s->queue, s->perm, s->inv, passes);
+      rc = run_passes(s, passes);
+      if (rc) { s->queue.clear(); return rc; }
+      s->stats.passes += passes.size();
+    } else {
+      for (const hgate& h : s->queue) {
+        if (h.kind == rbk::HK_SWAP) {
+          const int pa = s->perm[h.target], pb = s->perm[h.target2];
+          s->perm[h.target] = pb; s->perm[h.target2] = pa;
+          s->inv[pa] = h.target2; s->inv[pb] = h.target;
+          continue;
+        }
+        const rbk::gate_rec r = rbk::to_physical(h, s->perm);
+        const cudaError_t e = s->precision == RBK_C128 ? rbk::launch_gate<double>(s->amps, s->n, r, s->stream)
+                                                      : rbk::launch_gate<float>(s->amps, s->n, r, s->stream);
+        if (e != cudaSuccess) { s->queue.clear(); return cuda_fail(e, "gate launch"); }
+        ++s->stats.gate_launches;
+        ++s->stats.kernel_launches;
+      }
+    }
+  } catch (std::exception const& ex) {
+    s->queue.clear();
+    return fail(RBK_ERR_STATE, std::string("planner: ") + ex.what());
+  }
+  s->queue.clear();
+  RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
+  return RBK_OK;
+}
+
+int canonicalize(rbk_state* s)
+{
+  int rc = flush(s);
+  if (rc) return rc;
+  bool identity = true;
+  for (int q = 0; q < s->n; ++q) identity = identity && s->perm[q] == q;
+  if (identity) return RBK_OK;
+  device_guard g(s->device);
+  if (s->n < tile_bits(s)) {
+    // Small states: swap qubits home one transposition at a time.
+    for (int q = 0; q < s->n; ++q) {
+      while (s->perm[q] != q) {
+        const int other = s->inv[q];  // logical qubit sitting on physical bit q
+        const int pq = s->perm[q];
+        // Swap physical bits pq and q with three controlled-X permutations.
+        for (int step = 0; step < 3; ++step) {
+          rbk::gate_rec r{};
+          r.kind = rbk::OPK_X;
+          r.target = static_cast<uint8_t>(step == 1 ? pq : q);
+          r.cmask = 1ull << (step == 1 ? q : pq);
+          const cudaError_t e = s->precision == RBK_C128 ? rbk::launch_gate<double>(s->amps, s->n, r, s->stream)
+                                                        : rbk::launch_gate<float>(s->amps, s->n, r, s->stream);
+          if (e != cudaSuccess) return cuda_fail(e, "swap launch");
+          ++s->stats.kernel_launches;
+        }
+        s->perm[q] = q; s->inv[q] = q;
+        s->perm[other] = pq; s->inv[pq] = other;
+      }
+    }
+    return RBK_OK;
+  }
+  std::vector<rbk::dev_pass> passes;
+  try {
+    rbk::plan_canonicalize(params_of(s), s->perm, s->inv, passes);
+  } catch (std::exception const& ex) {
+    return fail(RBK_ERR_STATE, std::string("planner: ") + ex.what());
+  }
+  rc = mark_launch_start(s);
+  if (rc) return rc;
+  rc = run_passes(s, passes);
+  if (rc) return rc;
+  s->stats.relabel_passes += passes.size();
+  RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
+  return RBK_OK;
+}
+
+int check_state(const rbk_state* s)
+{
+  if (!s) return fail(RBK_ERR_INVALID, "null state");
+  return RBK_OK;
+}
+
+// Validates target/control qubits: in range and pairwise distinct.
+int check_qubits(const rbk_state* s, const uint32_t* qs, int count, uint64_t* mask_out)
+{
+  if (count < 0) return fail(RBK_ERR_INVALID, "negative qubit count");
+  if (count > 0 && !qs) return fail(RBK_ERR_INVALID, "null qubit array");
+  uint64_t m = 0;
+  for (int i = 0; i < count; ++i) {
+    if (qs[i] >= static_cast<uint32_t>(s->n)) return fail(RBK_ERR_INVALID, "qubit index out of range");
+    const uint64_t b = 1ull << qs[i];
+    if (m & b) return fail(RBK_ERR_INVALID, "repeated qubit");
+    m |= b;
+  }
+  *mask_out = m;
+  return RBK_OK;
+}
+
+int enqueue(rbk_state* s, const hgate& g)
+{
+  s->queue.push_back(g);
+  ++s->stats.gates_issued;
+  if (!s->deferred && !s->in_fusion) return flush(s);
+  return RBK_OK;
+}
+
+int enqueue_target(rbk_state* s, uint8_t kind, uint32_t target, const uint32_t* controls, int nc,
+                   const double* m, uint8_t diag_one = 0)
+{
+  int rc = check_state(s);
+  if (rc) return rc;
+  uint64_t cm = 0;
+  rc = check_qubits(s, controls, nc, &cm);
+  if (rc) return rc;
+  if (target >= static_cast<uint32_t>(s->n)) return fail(RBK_ERR_INVALID, "target qubit out of range");
+  if (cm & (1ull << target)) return fail(RBK_ERR_INVALID, "target qubit is also a control qubit");
+  hgate g{};
+  g.kind = kind;
+  g.target = static_cast<int8_t>(target);
+  g.target2 = -1;
+  g.diag_one = diag_one;
+  g.cmask = cm;
+  if (m) std::memcpy(g.m, m, sizeof(g.m));
+  return enqueue(s, g);
+}
+
+using cplx = std::complex<double>;
+
+// ket::utility::exp_i (ket/include/ket/utility/exp_i.hpp:21-36)
+cplx exp_i(double theta) { return std::exp(cplx{0.0, theta}); }
+
+constexpr double kOneDivRootTwo = 0.707106781186547524400844362104849039284835937688474036588;
+constexpr double kTwoPi = 6.28318530717958647692528676655900576839433879875021164195;
+
+void put(double* m, int k, cplx v) { m[2 * k] = v.real(); m[2 * k + 1] = v.imag(); }
+
+// Phase on the all-ones subspace of `qubits` (phase_shift_coeff form).
+int enqueue_phase(rbk_state* s, cplx coeff, const uint32_t* qubits, int nq)
+{
+  int rc = check_state(s);
+  if (rc) return rc;
+  if (nq < 1) return fail(RBK_ERR_INVALID, "phase shift needs at least one qubit");
+  uint64_t mask = 0;
+  rc = check_qubits(s, qubits, nq, &mask);
+  if (rc) return rc;
+  hgate g{};
+  g.target2 = -1;
+  if (coeff == cplx{-1.0, 0.0}) {
+    g.kind = rbk::OPK_NEG;
+    g.target = -1;
+    g.cmask = mask;
+  } else {
+    g.kind = rbk::OPK_DIAG;
+    g.target = static_cast<int8_t>(qubits[nq - 1]);
+    g.cmask = mask & ~(1ull << qubits[nq - 1]);
+    g.diag_one = 1;
+    put(g.m, 0, cplx{1.0, 0.0});
+    put(g.m, 1, coeff);
+  }
+  return enqueue(s, g);
+}
+
+template <typename F>
+int guarded(F&& f)
+{
+  try { return f(); }
+  catch (std::bad_alloc const&) { return fail(RBK_ERR_OOM, "host memory exhausted"); }
+  catch (std::exception const& e) { return fail(RBK_ERR_STATE, e.what()); }
+}
+
+// Reductions need an identity-free view: the kernels work on physical bits.
+template <typename Fn>
+int launch_reduction(rbk_state* s, Fn&& fn)
+{
+  int rc = flush(s);
+  if (rc) return rc;
+  device_guard g(s->device);
+  rc = mark_launch_start(s);
+  if (rc) return rc;
+  const cudaError_t e = fn();
+  if (e != cudaSuccess) return cuda_fail(e, "reduction launch");
+  s->stats.kernel_launches += 2;
+  ++s->stats.reduction_passes;
+  RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
+  return RBK_OK;
+}
+
+int read_out(rbk_state* s, int count)
+{
+  RBK_CUDA(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream));
+  return bounded_sync(s);
+}
+
+// sum over one flip-mask group of Pauli terms (physical masks).
+int pauli_group(rbk_state* s, uint64_t flip, const rbk::pauli_terms& t, double* out2)
+{
+  int rc = launch_reduction(s, [&] {
+    return s->precision == RBK_C128 ? rbk::launch_pauli<double>(s->amps, s->n, flip, t, s->d_partials, s->d_out, s->stream)
+                                    : rbk::launch_pauli<float>(s->amps, s->n, flip, t, s->d_partials, s->d_out, s->stream);
+  });
+  if (rc) return rc;
+  rc = read_out(s, 2);
+  if (rc) return rc;
+  out2[0] = s->h_out[0];
+  out2[1] = s->h_out[1];
+  return RBK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rbk_last_error(void) { return g_error.c_str(); }
+int rbk_version(void) { return 1; }
+
+int rbk_state_create(int num_qubits, int precision, uint64_t initial_index, int device, rbk_state** out)
+{
+  return guarded([&]() -> int {
+    if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    if (precision != RBK_C128 && precision != RBK_C64) return fail(RBK_ERR_INVALID, "unknown precision");
+    const int max_q = precision == RBK_C128 ? 33 : 34;
+    if (num_qubits < 1 || num_qubits > max_q) return fail(RBK_ERR_INVALID, "number of qubits out of range");
+    if (initial_index >= (1ull << num_qubits)) return fail(RBK_ERR_INVALID, "initial index out of range");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(RBK_ERR_CUDA, "no CUDA device available");
+    if (device < 0 || device >= ndev) return fail(RBK_ERR_INVALID, "device index out of range");
+    device_guard g(device);
+    auto* s = new rbk_state();
+    s->n = num_qubits;
+    s->precision = precision;
+    s->device = device;
+    s->perm.resize(num_qubits);
+    s->inv.resize(num_qubits);
+    for (int q = 0; q < num_qubits; ++q) s->perm[q] = s->inv[q] = q;
+    auto cleanup = [&](int rc) { rbk_state_destroy(s); return rc; };
+    const size_t bytes = amp_bytes(precision) << num_qubits;
+    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaStreamCreate"));
+    e = cudaMalloc(&s->amps, bytes);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(state)"));
+    e = cudaMalloc(reinterpret_cast<void**>(&s->d_partials), sizeof(double) * rbk::reduction_scratch_doubles());
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(scratch)"));
+    e = cudaMalloc(reinterpret_cast<void**>(&s->d_out), sizeof(double) * 4 * (rbk::kMaxQubits + 8));
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(results)"));
+    e = cudaMallocHost(reinterpret_cast<void**>(&s->h_out), sizeof(double) * 4 * (rbk::kMaxQubits + 8));
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMallocHost"));
+    for (cudaEvent_t* ev : {&s->ev_first, &s->ev_last, &s->ev_sync}) {
+      e = cudaEventCreate(ev);
+      if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaEventCreate"));
+    }
+    e = precision == RBK_C128 ? rbk::launch_set_basis<double>(s->amps, num_qubits, initial_index, s->stream)
+                              : rbk::launch_set_basis<float>(s->amps, num_qubits, initial_index, s->stream);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "set basis"));
+    ++s->stats.kernel_launches;
+    const int rc = bounded_sync(s);
+    if (rc) return cleanup(rc);
+    *out = s;
+    return RBK_OK;
+  });
+}
+
+int rbk_state_destroy(rbk_state* s)
+{
+  if (!s) return RBK_OK;
+  device_guard g(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->amps) cudaFree(s->amps);
+  if (s->d_partials) cudaFree(s->d_partials);
+  if (s->d_out) cudaFree(s->d_out);
+  if (s->h_out) cudaFreeHost(s->h_out);
+  for (cudaEvent_t ev : {s->ev_first, s->ev_last, s->ev_sync}) if (ev) cudaEventDestroy(ev);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return RBK_OK;
+}
+
+int rbk_state_num_qubits(const rbk_state* s, int* out)
+{
+  if (int rc = check_state(s)) return rc;
+  if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+  *out = s->n;
+  return RBK_OK;
+}
+
+int rbk_state_precision(const rbk_state* s, int* out)
+{
+  if (int rc = check_state(s)) return rc;
+  if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+  *out = s->precision;
+  return RBK_OK;
+}
+
+int rbk_state_reset(rbk_state* s, uint64_t index)
+{
+  if (int rc = check_state(s)) return rc;
+  if (index >= (1ull << s->n)) return fail(RBK_ERR_INVALID, "index out of range");
+  s->queue.clear();
+  s->in_fusion = false;
+  for (int q = 0; q < s->n; ++q) s->perm[q] = s->inv[q] = q;
+  device_guard g(s->device);
+  if (int rc = mark_launch_start(s)) return rc;
+  const cudaError_t e = s->precision == RBK_C128 ? rbk::launch_set_basis<double>(s->amps, s->n, index, s->stream)
+                                                : rbk::launch_set_basis<float>(s->amps, s->n, index, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "set basis");
+  ++s->stats.kernel_launches;
+  RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
+  return RBK_OK;
+}
+
+int rbk_state_upload(rbk_state* s, const void* host, uint64_t offset, uint64_t count)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    const uint64_t size = 1ull << s->n;
+    if (!host && count) return fail(RBK_ERR_INVALID, "null host pointer");
+    if (offset > size || count > size - offset) return fail(RBK_ERR_INVALID, "range out of bounds");
+    if (offset == 0 && count == size) {
+      s->queue.clear();
+      for (int q = 0; q < s->n; ++q) s->perm[q] = s->inv[q] = q;
+    } else if (int rc = canonicalize(s)) {
+      return rc;
+    }
+    device_guard g(s->device);
+    const size_t ab = amp_bytes(s->precision);
+    RBK_CUDA(cudaMemcpyAsync(static_cast<char*>(s->amps) + offset * ab, host, count * ab, cudaMemcpyHostToDevice, s->stream));
+    return bounded_sync(s);
+  });
+}
+
+int rbk_state_download(rbk_state* s, void* host, uint64_t offset, uint64_t count)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    const uint64_t size = 1ull << s->n;
+    if (!host && count) return fail(RBK_ERR_INVALID, "null host pointer");
+    if (offset > size || count > size - offset) return fail(RBK_ERR_INVALID, "range out of bounds");
+    if (int rc = canonicalize(s)) return rc;
+    device_guard g(s->device);
+    const size_t ab = amp_bytes(s->precision);
+    RBK_CUDA(cudaMemcpyAsync(host, static_cast<const char*>(s->amps) + offset * ab, count * ab, cudaMemcpyDeviceToHost, s->stream));
+    return bounded_sync(s);
+  });
+}
+
+int rbk_state_synchronize(rbk_state* s)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (int rc = flush(s)) return rc;
+    device_guard g(s->device);
+    return bounded_sync(s);
+  });
+}
+
+int rbk_flush(rbk_state* s)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    return flush(s);
+  });
+}
+
+int rbk_state_set_deferred(rbk_state* s, int deferred)
+{
+  if (int rc = check_state(s)) return rc;
+  s->deferred = deferred != 0;
+  if (!s->deferred && !s->in_fusion) return guarded([&] { return flush(s); });
+  return RBK_OK;
+}
+
+int rbk_state_set_pass_budget(rbk_state* s, int max_dense)
+{
+  if (int rc = check_state(s)) return rc;
+  if (max_dense < 0) return fail(RBK_ERR_INVALID, "negative budget");
+  s->dense_budget = max_dense;
+  return RBK_OK;
+}
+
+int rbk_state_get_stats(const rbk_state* s, rbk_stats* out)
+{
+  if (int rc = check_state(s)) return rc;
+  if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+  *out = s->stats;
+  return RBK_OK;
+}
+
+int rbk_state_reset_stats(rbk_state* s)
+{
+  if (int rc = check_state(s)) return rc;
+  s->stats = rbk_stats{};
+  s->timing_started = false;
+  return RBK_OK;
+}
+
+int rbk_state_device_ms(rbk_state* s, double* out)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+    if (int rc = flush(s)) return rc;
+    device_guard g(s->device);
+    if (int rc = bounded_sync(s)) return rc;
+    if (!s->timing_started) { *out = 0.0; return RBK_OK; }
+    float ms = 0.f;
+    RBK_CUDA(cudaEventElapsedTime(&ms, s->ev_first, s->ev_last));
+    *out = ms;
+    return RBK_OK;
+  });
+}
+
+int rbk_state_get_permutation(rbk_state* s, uint32_t* perm)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!perm) return fail(RBK_ERR_INVALID, "null output pointer");
+    if (int rc = flush(s)) return rc;
+    for (int q = 0; q < s->n; ++q) perm[q] = static_cast<uint32_t>(s->perm[q]);
+    return RBK_OK;
+  });
+}
+
+int rbk_state_canonicalize(rbk_state* s)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    return canonicalize(s);
+  });
+}
+
+int rbk_state_device_pointer(rbk_state* s, void** out)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+    if (int rc = flush(s)) return rc;
+    *out = s->amps;
+    return RBK_OK;
+  });
+}
+
+int rbk_begin_fusion(rbk_state* s)
+{
+  if (int rc = check_state(s)) return rc;
+  if (s->in_fusion) return fail(RBK_ERR_STATE, "BEGIN FUSION inside a fusion block");
+  s->in_fusion = true;
+  return RBK_OK;
+}
+
+int rbk_end_fusion(rbk_state* s)
+{
+  if (int rc = check_state(s)) return rc;
+  if (!s->in_fusion) return fail(RBK_ERR_STATE, "END FUSION without BEGIN FUSION");
+  s->in_fusion = false;
+  if (!s->deferred) return guarded([&] { return flush(s); });
+  return RBK_OK;
+}
+
+// ---- gates ------------------------------------------------------------------
+
+int rbk_hadamard(rbk_state* s, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    double m[8];
+    put(m, 0, {kOneDivRootTwo, 0.0}); put(m, 1, {kOneDivRootTwo, 0.0});
+    put(m, 2, {kOneDivRootTwo, 0.0}); put(m, 3, {-kOneDivRootTwo, 0.0});
+    return enqueue_target(s, rbk::OPK_MAT, target, controls, nc, m);
+  });
+}
+
+int rbk_pauli_x(rbk_state* s, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&] { return enqueue_target(s, rbk::OPK_X, target, controls, nc, nullptr); });
+}
+
+int rbk_pauli_y(rbk_state* s, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&] { return enqueue_target(s, rbk::OPK_Y, target, controls, nc, nullptr); });
+}
+
+int rbk_pauli_z(rbk_state* s, const uint32_t* qubits, int nq)
+{
+  return guarded([&] { return enqueue_phase(s, cplx{-1.0, 0.0}, qubits, nq); });
+}
+
+int rbk_phase_shift_coeff(rbk_state* s, double re, double im, const uint32_t* qubits, int nq)
+{
+  return guarded([&] { return enqueue_phase(s, cplx{re, im}, qubits, nq); });
+}
+
+int rbk_phase_shift(rbk_state* s, double phase, const uint32_t* qubits, int nq)
+{
+  return guarded([&] { return enqueue_phase(s, exp_i(phase), qubits, nq); });
+}
+
+int rbk_controlled_phase_shift_k(rbk_state* s, int k, const uint32_t* qubits, int nq)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    const int ak = k < 0 ? -k : k;
+    if (ak > s->n) return fail(RBK_ERR_INVALID, "phase exponent larger than the number of qubits");
+    // bra's table entry: exp_i(2 pi / 2^k) (generate_phase_coefficients.hpp:20-39)
+    cplx c = exp_i(kTwoPi / static_cast<double>(1ull << ak));
+    if (k < 0) c = std::conj(c);
+    return enqueue_phase(s, c, qubits, nq);
+  });
+}
+
+int rbk_phase_shift2(rbk_state* s, double phase1, double phase2, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    // phase_shift.hpp:660-709: a0' = (a0 - c2 a1)/sqrt2, a1' = r c1 (c2 a1 + a0)
+    const cplx c1 = exp_i(phase1), c2 = exp_i(phase2);
+    const cplx mc1 = kOneDivRootTwo * c1;
+    double m[8];
+    put(m, 0, {kOneDivRootTwo, 0.0});
+    put(m, 1, -(kOneDivRootTwo * c2));
+    put(m, 2, mc1);
+    put(m, 3, mc1 * c2);
+    return enqueue_target(s, rbk::OPK_MAT, target, controls, nc, m);
+  });
+}
+
+int rbk_phase_shift3(rbk_state* s, double phase1, double phase2, double phase3, uint32_t target,
+                     const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    // phase_shift.hpp:1200-1254: a0' = cos a0 - (sin c3) a1, a1' = ((cos c3) a1 + sin a0) c2
+    const double sine = std::sin(0.5 * phase1), cosine = std::cos(0.5 * phase1);
+    const cplx c2 = exp_i(phase2), c3 = exp_i(phase3);
+    double m[8];
+    put(m, 0, {cosine, 0.0});
+    put(m, 1, -(sine * c3));
+    put(m, 2, sine * c2);
+    put(m, 3, (cosine * c3) * c2);
+    return enqueue_target(s, rbk::OPK_MAT, target, controls, nc, m);
+  });
+}
+
+int rbk_exponential_pauli_x(rbk_state* s, double phase, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    // exp(i theta X) = cos I + i sin X
+    const cplx c = exp_i(phase);
+    double m[8];
+    put(m, 0, {c.real(), 0.0}); put(m, 1, {0.0, c.imag()});
+    put(m, 2, {0.0, c.imag()}); put(m, 3, {c.real(), 0.0});
+    return enqueue_target(s, rbk::OPK_MAT, target, controls, nc, m);
+  });
+}
+
+int rbk_exponential_pauli_y(rbk_state* s, double phase, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    // exponential_pauli_y.hpp:40-85: a0' = cos a0 + sin a1, a1' = cos a1 - sin a0
+    const cplx c = exp_i(phase);
+    double m[8];
+    put(m, 0, {c.real(), 0.0}); put(m, 1, {c.imag(), 0.0});
+    put(m, 2, {-c.imag(), 0.0}); put(m, 3, {c.real(), 0.0});
+    return enqueue_target(s, rbk::OPK_MAT, target, controls, nc, m);
+  });
+}
+
+int rbk_exponential_pauli_z(rbk_state* s, double phase, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    // exponential_pauli_z.hpp:40-78: a0 *= e^{i theta}, a1 *= e^{-i theta}
+    const cplx c = exp_i(phase);
+    double d[8] = {};
+    put(d, 0, c);
+    put(d, 1, std::conj(c));
+    return enqueue_target(s, rbk::OPK_DIAG, target, controls, nc, d, 0);
+  });
+}
+
+int rbk_swap(rbk_state* s, uint32_t q1, uint32_t q2, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    uint64_t cm = 0;
+    if (int rc = check_qubits(s, controls, nc, &cm)) return rc;
+    if (q1 >= static_cast<uint32_t>(s->n) || q2 >= static_cast<uint32_t>(s->n))
+      return fail(RBK_ERR_INVALID, "qubit index out of range");
+    if (q1 == q2) return fail(RBK_ERR_INVALID, "repeated qubit");
+    if (cm & ((1ull << q1) | (1ull << q2))) return fail(RBK_ERR_INVALID, "swap qubit is also a control qubit");
+    if (nc == 0) {
+      hgate g{};
+      g.kind = rbk::HK_SWAP;
+      g.target = static_cast<int8_t>(q1);
+      g.target2 = static_cast<int8_t>(q2);
+      return enqueue(s, g);
+    }
+    // Controlled swap = X(q1 <- q2) . C..C X(q2 <- q1) . X(q1 <- q2), all exact permutations.
+    const uint32_t c2[1] = {q2};
+    if (int rc = enqueue_target(s, rbk::OPK_X, q1, c2, 1, nullptr)) return rc;
+    std::vector<uint32_t> cc(controls, controls + nc);
+    cc.push_back(q1);
+    if (int rc = enqueue_target(s, rbk::OPK_X, q2, cc.data(), static_cast<int>(cc.size()), nullptr)) return rc;
+    return enqueue_target(s, rbk::OPK_X, q1, c2, 1, nullptr);
+  });
+}
+
+int rbk_apply_matrix2(rbk_state* s, const double* m, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    if (!m) return fail(RBK_ERR_INVALID, "null matrix");
+    return enqueue_target(s, rbk::OPK_MAT, target, controls, nc, m);
+  });
+}
+
+int rbk_apply_diagonal2(rbk_state* s, const double* d, uint32_t target, const uint32_t* controls, int nc)
+{
+  return guarded([&]() -> int {
+    if (!d) return fail(RBK_ERR_INVALID, "null diagonal");
+    double m[8] = {d[0], d[1], d[2], d[3], 0, 0, 0, 0};
+    const uint8_t one = (d[0] == 1.0 && d[1] == 0.0) ? 1 : 0;
+    return enqueue_target(s, rbk::OPK_DIAG, target, controls, nc, m, one);
+  });
+}
+
+// ---- observables -------------------------------------------------------------
+
+int rbk_norm2(rbk_state* s, double* out)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+    rbk::pauli_terms t{};
+    t.count = 1;
+    t.w[0][0] = 1.0;
+    double r[2];
+    if (int rc = pauli_group(s, 0, t, r)) return rc;
+    *out = r[0];
+    return RBK_OK;
+  });
+}
+
+int rbk_probabilities(rbk_state* s, double* host_out, uint64_t offset, uint64_t count)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    const uint64_t size = 1ull << s->n;
+    if (!host_out && count) return fail(RBK_ERR_INVALID, "null output pointer");
+    if (offset > size || count > size - offset) return fail(RBK_ERR_INVALID, "range out of bounds");
+    if (int rc = canonicalize(s)) return rc;
+    device_guard g(s->device);
+    const uint64_t chunk = std::min<uint64_t>(count, 1ull << 24);
+    double* dbuf = nullptr;
+    if (chunk) RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&dbuf), chunk * sizeof(double)));
+    int rc = RBK_OK;
+    for (uint64_t done = 0; done < count && rc == RBK_OK; done += chunk) {
+      const uint64_t c = std::min(chunk, count - done);
+      const cudaError_t e = s->precision == RBK_C128 ? rbk::launch_probs<double>(s->amps, offset + done, c, dbuf, s->stream)
+                                                    : rbk::launch_probs<float>(s->amps, offset + done, c, dbuf, s->stream);
+      if (e != cudaSuccess) { rc = cuda_fail(e, "probabilities"); break; }
+      ++s->stats.kernel_launches;
+      const cudaError_t e2 = cudaMemcpyAsync(host_out + done, dbuf, c * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+      if (e2 != cudaSuccess) { rc = cuda_fail(e2, "probabilities copy"); break; }
+      rc = bounded_sync(s);
+    }
+    if (dbuf) cudaFree(dbuf);
+    return rc;
+  });
+}
+
+int rbk_spin_expectation_values(rbk_state* s, double* out)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+    // <S_z>: one pass of Z sums over all physical bits.
+    int rc = launch_reduction(s, [&] {
+      return s->precision == RBK_C128 ? rbk::launch_zsum<double>(s->amps, s->n, s->d_partials, s->d_out, s->stream)
+                                      : rbk::launch_zsum<float>(s->amps, s->n, s->d_partials, s->d_out, s->stream);
+    });
+    if (rc) return rc;
+    if ((rc = read_out(s, s->n + 1))) return rc;
+    const double total = s->h_out[0];
+    std::vector<double> ones(s->n);
+    for (int p = 0; p < s->n; ++p) ones[p] = s->h_out[1 + p];
+    for (int q = 0; q < s->n; ++q) {
+      const double one = ones[s->perm[q]];
+      out[3 * q + 2] = 0.5 * ((total - one) - one);
+    }
+    // <S_x> + i <S_y> = sum over pairs with the qubit clear of conj(a0) a1.
+    for (int q = 0; q < s->n; ++q) {
+      rbk::pauli_terms t{};
+      t.count = 1;
+      t.w[0][0] = 1.0;
+      t.one_sided = 1;
+      const uint64_t flip = 1ull << s->perm[q];
+      double r[2];
+      if ((rc = pauli_group(s, flip, t, r))) return rc;
+      out[3 * q + 0] = r[0];
+      out[3 * q + 1] = r[1];
+    }
+    return RBK_OK;
+  });
+}
+
+int rbk_expectation_pauli(rbk_state* s, int num_terms, const char* strings, const double* coeffs, double* out)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (num_terms < 0 || (num_terms > 0 && (!strings || !coeffs)) || !out)
+      return fail(RBK_ERR_INVALID, "bad Pauli term arguments");
+    struct term { uint64_t flip, sign; cplx w; };
+    std::vector<term> terms;
+    for (int t = 0; t < num_terms; ++t) {
+      uint64_t x = 0, y = 0, z = 0;
+      for (int k = 0; k < s->n; ++k) {
+        const char c = strings[static_cast<size_t>(t) * s->n + k];
+        const uint64_t b = 1ull << s->perm[k];
+        if (c == 'X') x |= b;
+        else if (c == 'Y') y |= b;
+        else if (c == 'Z') z |= b;
+        else if (c != 'I') return fail(RBK_ERR_INVALID, "Pauli strings use the characters I, X, Y, Z");
+      }
+      // (P psi)(i) = (-i)^{#Y} (-1)^{popcount(i & (Y|Z))} psi(i ^ (X|Y))  (pauli_index_coeff.hpp:17-59)
+      static const cplx pow_mi[4] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}};
+      const cplx w = cplx{coeffs[2 * t], coeffs[2 * t + 1]} * pow_mi[__builtin_popcountll(y) & 3];
+      terms.push_back({x | y, y | z, w});
+    }
+    std::vector<char> done(terms.size(), 0);
+    double acc_re = 0, acc_im = 0;
+    for (size_t i = 0; i < terms.size(); ++i) {
+      if (done[i]) continue;
+      rbk::pauli_terms pt{};
+      for (size_t j = i; j < terms.size() && pt.count < rbk::kMaxPauliTerms; ++j) {
+        if (done[j] || terms[j].flip != terms[i].flip) continue;
+        pt.sign[pt.count] = terms[j].sign;
+        pt.w[pt.count][0] = terms[j].w.real();
+        pt.w[pt.count][1] = terms[j].w.imag();
+        ++pt.count;
+        done[j] = 1;
+      }
+      double r[2];
+      if (int rc = pauli_group(s, terms[i].flip, pt, r)) return rc;
+      acc_re += r[0];
+      acc_im += r[1];
+    }
+    out[0] = acc_re;
+    out[1] = acc_im;
+    return RBK_OK;
+  });
+}
+
+int rbk_inner_product(rbk_state* a, rbk_state* b, double* out)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(a)) return rc;
+    if (int rc = check_state(b)) return rc;
+    if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+    if (a->n != b->n || a->precision != b->precision) return fail(RBK_ERR_INVALID, "states differ in size or precision");
+    if (a->device != b->device) return fail(RBK_ERR_UNSUPPORTED, "states live on different devices");
+    if (a->perm != b->perm) {
+      if (int rc = canonicalize(a)) return rc;
+      if (int rc = canonicalize(b)) return rc;
+    }
+    if (int rc = flush(b)) return rc;
+    {
+      device_guard g(b->device);
+      if (int rc = bounded_sync(b)) return rc;
+    }
+    int rc = launch_reduction(a, [&] {
+      return a->precision == RBK_C128 ? rbk::launch_inner<double>(a->amps, b->amps, a->n, a->d_partials, a->d_out, a->stream)
+                                      : rbk::launch_inner<float>(a->amps, b->amps, a->n, a->d_partials, a->d_out, a->stream);
+    });
+    if (rc) return rc;
+    if ((rc = read_out(a, 2))) return rc;
+    out[0] = a->h_out[0];
+    out[1] = a->h_out[1];
+    return RBK_OK;
+  });
+}
+
+int rbk_fidelity(rbk_state* a, rbk_state* b, double* out)
+{
+  if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+  double ip[2];
+  if (int rc = rbk_inner_product(a, b, ip)) return rc;
+  *out = ip[0] * ip[0] + ip[1] * ip[1];
+  return RBK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,406 @@
+// rbk_plan.cpp -- host-side fusion planner.
+//
+// The reference applies each gate as one sweep over the state
+// (ket/include/ket/gate/*.hpp) or, inside BEGIN/END FUSION, replays a recorded
+// gate list on every 2^k chunk of the fused qubits
+// (bra/src/nompi_state.cpp:1285-1357).  Here the whole queue of gates is cut
+// into tile passes instead:
+//
+//  * A pass owns a set of K physical bits (the tile bits).  The low LOW
+//    physical bits are always tile bits, so that every tile is made of
+//    contiguous 512-byte runs in HBM (coalesced 16-byte accesses).
+//  * Walking the queue in order, a gate is taken into the pass when its
+//    non-diagonal target fits in the tile and it commutes with every earlier
+//    gate that was left behind (on each shared qubit both act diagonally:
+//    control, phase or Z-type).  Controls and diagonal qubits need not be
+//    tile bits: outside the tile they are a per-tile predicate.
+//  * Inside the pass, gates are grouped into register phases: R tile bits are
+//    held in each thread's registers, and a gate can run once its target is
+//    one of them.  Changing phase costs one shared-memory exchange.
+//  * At the end of a pass the tile bits are relabelled: the logical qubits
+//    that the queue needs next are written into the low physical bits.  This
+//    is the layout map of ket::mpi::qubit_permutation
+//    (ket/include/ket/mpi/qubit_permutation.hpp:242-252 `permutate`) with the
+//    swap of swap_permutated_local_qubits
+//    (ket/include/ket/mpi/utility/detail/swap_permutated_local_qubits.hpp:26-81)
+//    folded into a pass that moves the data anyway.
+//  * Uncontrolled SWAP gates only change the layout map.
+#include "rbk_plan.h"
+
+#include <algorithm>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+
+namespace rbk {
+namespace {
+
+inline uint64_t bit(int q) { return 1ull << q; }
+inline int popc(uint64_t v) { return __builtin_popcountll(v); }
+
+uint64_t map_mask(uint64_t logical, const std::vector<int>& perm)
+{
+  uint64_t r = 0;
+  while (logical) {
+    const int q = __builtin_ctzll(logical);
+    logical &= logical - 1;
+    r |= bit(perm[q]);
+  }
+  return r;
+}
+
+// A selected gate in physical bits.
+struct pop {
+  uint8_t kind;
+  uint8_t diag_one;
+  int target;       // physical; -1 for NEG
+  uint64_t cmask;   // physical
+  double m[8];
+};
+
+bool is_target_kind(uint8_t k) { return k == OPK_MAT || k == OPK_X || k == OPK_Y; }
+
+// Tracks register phases while gates are added (same greedy as build_pass).
+struct phase_tracker {
+  int R;
+  std::vector<int> cur;  // physical bits held in registers in the current phase
+  int phases = 1;
+
+  bool would_fit(int t, int max_phases) const
+  {
+    if (std::find(cur.begin(), cur.end(), t) != cur.end()) return true;
+    if (static_cast<int>(cur.size()) < R) return true;
+    return phases + 1 <= max_phases;
+  }
+  void add(int t)
+  {
+    if (std::find(cur.begin(), cur.end(), t) != cur.end()) return;
+    if (static_cast<int>(cur.size()) < R) { cur.push_back(t); return; }
+    cur.assign(1, t);
+    ++phases;
+  }
+};
+
+// Orders the thread bits of a phase so that the lowest lanes fall on tile bits
+// that map to distinct shared-memory bank groups (see smem_slot in
+// rbk_kernels.cu: vector-index bit b contributes to slot bit b mod 3).
+void order_thread_bits(std::vector<int>& thr, int vbits)
+{
+  std::vector<int> out;
+  std::vector<int> rest(thr);
+  auto take = [&](int b) {
+    out.push_back(b);
+    rest.erase(std::find(rest.begin(), rest.end(), b));
+  };
+  if (vbits == 1 && std::find(rest.begin(), rest.end(), 0) != rest.end()) take(0);
+  bool used[3] = {false, false, false};
+  for (int pass = 0; pass < 3; ++pass) {
+    for (int b : std::vector<int>(rest)) {
+      if (b < vbits) continue;
+      const int res = (b - vbits) % 3;
+      if (!used[res]) { used[res] = true; take(b); break; }
+    }
+  }
+  std::sort(rest.begin(), rest.end());
+  out.insert(out.end(), rest.begin(), rest.end());
+  thr = out;
+}
+
+void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>& ops,
+                const int* relabel_to, const int* tile_phys, dev_pass& out)
+{
+  std::memset(&out, 0, sizeof(out));
+  const int K = p.K, R = p.R, T = K - R;
+  int tile_of_phys[64];
+  for (int i = 0; i < 64; ++i) tile_of_phys[i] = -1;
+  for (int b = 0; b < K; ++b) {
+    out.tile_phys[b] = static_cast<uint8_t>(tile_phys[b]);
+    tile_of_phys[tile_phys[b]] = b;
+  }
+  int nn = 0;
+  for (int q = 0; q < p.n; ++q)
+    if (!(tile_mask & bit(q))) out.nontile_phys[nn++] = static_cast<uint8_t>(q);
+  out.num_nontile = static_cast<uint8_t>(nn);
+
+  // Group ops into phases by register set.
+  struct phase_build { std::vector<int> reg; std::vector<int> ops; };
+  std::vector<phase_build> phases(1);
+  for (int i = 0; i < static_cast<int>(ops.size()); ++i) {
+    const pop& o = ops[i];
+    if (is_target_kind(o.kind)) {
+      const int tb = tile_of_phys[o.target];
+      auto& cur = phases.back().reg;
+      if (std::find(cur.begin(), cur.end(), tb) == cur.end()) {
+        if (static_cast<int>(cur.size()) < R) cur.push_back(tb);
+        else { phases.emplace_back(); phases.back().reg.push_back(tb); }
+      }
+    }
+    phases.back().ops.push_back(i);
+  }
+  if (static_cast<int>(phases.size()) > kMaxPhases) throw std::logic_error("planner: too many phases");
+
+  int op_index = 0;
+  for (size_t ph = 0; ph < phases.size(); ++ph) {
+    auto& pb = phases[ph];
+    // Fill the register set from the highest tile bits (the low ones make good lanes).
+    for (int b = K - 1; b >= 0 && static_cast<int>(pb.reg.size()) < R; --b)
+      if (std::find(pb.reg.begin(), pb.reg.end(), b) == pb.reg.end()) pb.reg.push_back(b);
+    std::vector<int> thr;
+    for (int b = 0; b < K; ++b)
+      if (std::find(pb.reg.begin(), pb.reg.end(), b) == pb.reg.end()) thr.push_back(b);
+    order_thread_bits(thr, p.vbits);
+
+    dev_phase& dp = out.phases[ph];
+    int reg_index[64], thr_index[64];
+    for (int i = 0; i < 64; ++i) reg_index[i] = thr_index[i] = -1;
+    for (int b = 0; b < R; ++b) { dp.reg_pos[b] = static_cast<uint8_t>(pb.reg[b]); reg_index[pb.reg[b]] = b; }
+    for (int b = 0; b < T; ++b) { dp.thr_pos[b] = static_cast<uint8_t>(thr[b]); thr_index[thr[b]] = b; }
+    const bool last = ph + 1 == phases.size();
+    for (int b = 0; b < R; ++b) dp.wreg_pos[b] = static_cast<uint8_t>(last ? relabel_to[pb.reg[b]] : pb.reg[b]);
+    for (int b = 0; b < T; ++b) dp.wthr_pos[b] = static_cast<uint8_t>(last ? relabel_to[thr[b]] : thr[b]);
+
+    dp.op_begin = static_cast<uint16_t>(op_index);
+    for (int oi : pb.ops) {
+      const pop& o = ops[oi];
+      dev_op& d = out.ops[op_index++];
+      d.kind = o.kind;
+      d.diag_one = o.diag_one;
+      std::memcpy(d.m, o.m, sizeof(d.m));
+      auto classify = [&](uint64_t phys_mask, uint32_t& reg, uint32_t& thrm, uint64_t& outm) {
+        while (phys_mask) {
+          const int q = __builtin_ctzll(phys_mask);
+          phys_mask &= phys_mask - 1;
+          const int tb = tile_of_phys[q];
+          if (tb < 0) outm |= bit(q);
+          else if (reg_index[tb] >= 0) reg |= 1u << reg_index[tb];
+          else thrm |= 1u << thr_index[tb];
+        }
+      };
+      classify(o.cmask, d.creg, d.cthr, d.cout);
+      if (is_target_kind(o.kind)) {
+        const int tb = tile_of_phys[o.target];
+        if (tb < 0 || reg_index[tb] < 0) throw std::logic_error("planner: target not in registers");
+        d.treg = static_cast<uint8_t>(reg_index[tb]);
+      } else if (o.kind == OPK_DIAG) {
+        classify(bit(o.target), d.dreg, d.dthr, d.dout);
+      }
+    }
+    dp.op_end = static_cast<uint16_t>(op_index);
+  }
+  out.num_phases = static_cast<uint8_t>(phases.size());
+}
+
+// Tile bit order: physical bits 0..LOW-1 first, then the others ascending.
+void tile_order(const plan_params& p, uint64_t tile_mask, int* tile_phys)
+{
+  int k = 0;
+  for (int q = 0; q < p.LOW; ++q) tile_phys[k++] = q;
+  for (int q = p.LOW; q < p.n; ++q)
+    if (tile_mask & bit(q)) tile_phys[k++] = q;
+}
+
+// Applies a physical relabelling new_phys_of_old (for tile bits) to perm/inv
+// and returns it as tile-bit -> tile-bit.
+void apply_relabel(const plan_params& p, const int* tile_phys, const int* new_phys_of_tile_bit,
+                   std::vector<int>& perm, std::vector<int>& inv, int* relabel_to)
+{
+  int tile_of_phys[64];
+  for (int i = 0; i < 64; ++i) tile_of_phys[i] = -1;
+  for (int b = 0; b < p.K; ++b) tile_of_phys[tile_phys[b]] = b;
+  std::vector<int> moved_logical(p.K);
+  for (int b = 0; b < p.K; ++b) moved_logical[b] = inv[tile_phys[b]];
+  for (int b = 0; b < p.K; ++b) {
+    const int np = new_phys_of_tile_bit[b];
+    relabel_to[b] = tile_of_phys[np];
+    perm[moved_logical[b]] = np;
+    inv[np] = moved_logical[b];
+  }
+}
+
+}  // namespace
+
+gate_rec to_physical(const hgate& g, const std::vector<int>& perm)
+{
+  gate_rec r{};
+  r.kind = g.kind;
+  r.diag_one = g.diag_one;
+  r.target = static_cast<uint8_t>(g.target >= 0 ? perm[g.target] : 0);
+  r.cmask = map_mask(g.cmask, perm);
+  std::memcpy(r.m, g.m, sizeof(r.m));
+  return r;
+}
+
+void plan_passes(const plan_params& p, const std::vector<hgate>& gates, std::vector<int>& perm,
+                 std::vector<int>& inv, std::vector<dev_pass>& out)
+{
+  const uint64_t all = p.n >= 64 ? ~0ull : bit(p.n) - 1;
+  const uint64_t low_mask = bit(p.LOW) - 1;
+  std::vector<char> taken(gates.size(), 0);
+  size_t first = 0;
+  const int budget = p.dense_budget > 0 ? p.dense_budget : 1;
+
+  while (true) {
+    while (first < gates.size() && taken[first]) ++first;
+    if (first >= gates.size()) break;
+
+    uint64_t tile = low_mask;
+    uint64_t blockN = 0, blockZ = 0;
+    std::vector<pop> ops;
+    int dense = 0;
+    phase_tracker tracker{p.R};
+
+    for (size_t i = first; i < gates.size(); ++i) {
+      if (taken[i]) continue;
+      const hgate& g = gates[i];
+      if (g.kind == HK_SWAP) {
+        const uint64_t m = bit(g.target) | bit(g.target2);
+        if ((blockN | blockZ) & m) { blockN |= m; continue; }
+        const int pa = perm[g.target], pb = perm[g.target2];
+        perm[g.target] = pb; perm[g.target2] = pa;
+        inv[pa] = g.target2; inv[pb] = g.target;
+        taken[i] = 1;
+        continue;
+      }
+      const uint64_t Nq = is_target_kind(g.kind) ? bit(g.target) : 0;
+      const uint64_t Zq = g.cmask | (g.kind == OPK_DIAG ? bit(g.target) : 0);
+      if ((Nq & (blockN | blockZ)) || (Zq & blockN)) {
+        blockN |= Nq; blockZ |= Zq;
+        if (((blockN | blockZ) & all) == all) break;
+        continue;
+      }
+      bool ok = static_cast<int>(ops.size()) < kMaxPassOps;
+      const int t = Nq ? perm[g.target] : -1;
+      if (ok && t >= 0 && !(tile & bit(t)) && popc(tile) >= p.K) ok = false;
+      if (ok && is_dense(g) && dense >= budget) ok = false;
+      if (ok && t >= 0 && !tracker.would_fit(t, kMaxPhases)) ok = false;
+      if (!ok) {
+        blockN |= Nq; blockZ |= Zq;
+        if (((blockN | blockZ) & all) == all) break;
+        continue;
+      }
+      if (t >= 0) { tile |= bit(t); tracker.add(t); }
+      pop o{};
+      o.kind = g.kind;
+      o.diag_one = g.diag_one;
+      o.target = g.target >= 0 ? perm[g.target] : -1;
+      o.cmask = map_mask(g.cmask, perm);
+      std::memcpy(o.m, g.m, sizeof(o.m));
+      ops.push_back(o);
+      taken[i] = 1;
+      dense += is_dense(g) ? 1 : 0;
+    }
+    if (ops.empty()) continue;  // only swaps were taken: layout map updated, no data moved
+
+    // Next use (queue position) of each logical qubit as a non-diagonal target.
+    const int INF = std::numeric_limits<int>::max();
+    std::vector<int> next_use(p.n, INF);
+    bool remaining = false;
+    for (size_t i = first; i < gates.size(); ++i) {
+      if (taken[i]) continue;
+      remaining = true;
+      const hgate& g = gates[i];
+      if (g.kind == HK_SWAP) {
+        next_use[g.target] = std::min(next_use[g.target], static_cast<int>(i));
+        next_use[g.target2] = std::min(next_use[g.target2], static_cast<int>(i));
+      } else if (is_target_kind(g.kind)) {
+        next_use[g.target] = std::min(next_use[g.target], static_cast<int>(i));
+      }
+    }
+    // Fill the tile to K bits with the qubits needed soonest.
+    while (popc(tile) < p.K) {
+      int best = -1;
+      for (int q = 0; q < p.n; ++q) {
+        if (tile & bit(perm[q])) continue;
+        if (best < 0 || next_use[q] < next_use[best] ||
+            (next_use[q] == next_use[best] && perm[q] < perm[best])) best = q;
+      }
+      tile |= bit(perm[best]);
+    }
+    int tile_phys[16];
+    tile_order(p, tile, tile_phys);
+
+    // Relabel: the soonest-needed logical qubits go to the low physical bits;
+    // with nothing left in the queue, qubits go home where the tile allows.
+    int new_phys[16];
+    {
+      std::vector<int> logical(p.K);
+      for (int b = 0; b < p.K; ++b) logical[b] = inv[tile_phys[b]];
+      std::vector<int> assign(p.K, -1);  // tile bit -> new physical bit
+      std::vector<char> phys_used(64, 0);
+      if (remaining) {
+        std::vector<int> order(p.K);
+        for (int b = 0; b < p.K; ++b) order[b] = b;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b2) {
+          return next_use[logical[a]] < next_use[logical[b2]];
+        });
+        for (int r = 0; r < p.LOW; ++r) {
+          if (next_use[logical[order[r]]] == INF) break;
+          assign[order[r]] = r;
+          phys_used[r] = 1;
+        }
+        // Others keep their position when it is free.
+        for (int b = 0; b < p.K; ++b)
+          if (assign[b] < 0 && !phys_used[tile_phys[b]]) { assign[b] = tile_phys[b]; phys_used[tile_phys[b]] = 1; }
+      } else {
+        for (int b = 0; b < p.K; ++b) {
+          const int home = logical[b];
+          if ((tile & bit(home)) && !phys_used[home]) { assign[b] = home; phys_used[home] = 1; }
+        }
+        for (int b = 0; b < p.K; ++b)
+          if (assign[b] < 0 && !phys_used[tile_phys[b]]) { assign[b] = tile_phys[b]; phys_used[tile_phys[b]] = 1; }
+      }
+      for (int b = 0; b < p.K; ++b) {
+        if (assign[b] >= 0) continue;
+        for (int c = 0; c < p.K; ++c)
+          if (!phys_used[tile_phys[c]]) { assign[b] = tile_phys[c]; phys_used[tile_phys[c]] = 1; break; }
+      }
+      for (int b = 0; b < p.K; ++b) new_phys[b] = assign[b];
+    }
+    int relabel_to[16];
+    apply_relabel(p, tile_phys, new_phys, perm, inv, relabel_to);
+    out.emplace_back();
+    build_pass(p, tile, ops, relabel_to, tile_phys, out.back());
+  }
+}
+
+void plan_canonicalize(const plan_params& p, std::vector<int>& perm, std::vector<int>& inv,
+                       std::vector<dev_pass>& out)
+{
+  const uint64_t low_mask = bit(p.LOW) - 1;
+  for (int guard = 0; guard < 4 * p.n + 4; ++guard) {
+    bool identity = true;
+    for (int q = 0; q < p.n; ++q) if (perm[q] != q) { identity = false; break; }
+    if (identity) return;
+
+    uint64_t tile = low_mask;
+    for (int q = 0; q < p.n; ++q) {
+      if (perm[q] == q) continue;
+      const uint64_t need = bit(perm[q]) | bit(q);
+      if (popc(tile | need) <= p.K) tile |= need;
+    }
+    for (int q = 0; q < p.n && popc(tile) < p.K; ++q) tile |= bit(q);
+    int tile_phys[16];
+    tile_order(p, tile, tile_phys);
+
+    int new_phys[16];
+    std::vector<char> used(64, 0);
+    std::vector<int> assign(p.K, -1);
+    for (int b = 0; b < p.K; ++b) {
+      const int home = inv[tile_phys[b]];
+      if ((tile & bit(home)) && !used[home]) { assign[b] = home; used[home] = 1; }
+    }
+    for (int b = 0; b < p.K; ++b) {
+      if (assign[b] >= 0) continue;
+      for (int c = 0; c < p.K; ++c)
+        if (!used[tile_phys[c]]) { assign[b] = tile_phys[c]; used[tile_phys[c]] = 1; break; }
+    }
+    for (int b = 0; b < p.K; ++b) new_phys[b] = assign[b];
+    int relabel_to[16];
+    apply_relabel(p, tile_phys, new_phys, perm, inv, relabel_to);
+    out.emplace_back();
+    build_pass(p, tile, std::vector<pop>{}, relabel_to, tile_phys, out.back());
+  }
+  throw std::logic_error("planner: canonicalize did not converge");
+}
+
+}  // namespace rbk
