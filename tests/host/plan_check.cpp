@@ -1,0 +1,181 @@
+// plan_check.cpp -- CPU check of the host-side fusion planner (no GPU).
+//
+// Plans random gate queues with rbk::plan_passes / rbk::plan_canonicalize and
+// executes the resulting pass programs with a plain C++ model of what
+// tile_pass_kernel does with a dev_pass (load the tile, per phase gather the
+// registers, apply the ops with their register / thread / outside-tile
+// predicates, scatter back with the write positions, store).  The result,
+// read back through the final layout map, must equal the gates applied one by
+// one in logical order.  Test code only; built and run by tests/test_planner.py.
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "rbk_internal.h"
+#include "rbk_plan.h"
+
+using cplx = std::complex<double>;
+using namespace rbk;
+
+static void apply_direct(std::vector<cplx>& a, const hgate& g)
+{
+  const uint64_t N = a.size();
+  if (g.kind == HK_SWAP) {
+    const uint64_t m1 = 1ull << g.target, m2 = 1ull << g.target2;
+    for (uint64_t i = 0; i < N; ++i)
+      if ((i & m1) && !(i & m2)) std::swap(a[i], a[(i & ~m1) | m2]);
+    return;
+  }
+  const cplx m00{g.m[0], g.m[1]}, m01{g.m[2], g.m[3]}, m10{g.m[4], g.m[5]}, m11{g.m[6], g.m[7]};
+  for (uint64_t i = 0; i < N; ++i) {
+    if ((i & g.cmask) != g.cmask) continue;
+    if (g.kind == OPK_NEG) { a[i] = -a[i]; continue; }
+    const uint64_t tm = 1ull << g.target;
+    if (g.kind == OPK_DIAG) { a[i] *= (i & tm) ? m01 : m00; continue; }
+    if (i & tm) continue;
+    const cplx a0 = a[i], a1 = a[i | tm];
+    if (g.kind == OPK_X) { a[i] = a1; a[i | tm] = a0; }
+    else if (g.kind == OPK_Y) { a[i] = cplx{0, -1} * a1; a[i | tm] = cplx{0, 1} * a0; }
+    else { a[i] = m00 * a0 + m01 * a1; a[i | tm] = m10 * a0 + m11 * a1; }
+  }
+}
+
+// Model of tile_pass_kernel for one pass.
+static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass& P)
+{
+  const int K = p.K, R = p.R, T = K - R, NR = 1 << R, NT = 1 << T;
+  const uint64_t blocks = 1ull << (p.n - K);
+  std::vector<cplx> tile(1u << K), next(1u << K);
+  std::vector<cplx> regs(size_t(NT) * NR);
+  for (uint64_t b = 0; b < blocks; ++b) {
+    uint64_t base = 0;
+    for (int k = 0; k < P.num_nontile; ++k) base |= ((b >> k) & 1ull) << P.nontile_phys[k];
+    auto phys_of = [&](uint32_t j) {
+      uint64_t ph = base;
+      for (int t = 0; t < K; ++t) if ((j >> t) & 1) ph |= 1ull << P.tile_phys[t];
+      return ph;
+    };
+    for (uint32_t j = 0; j < (1u << K); ++j) tile[j] = st[phys_of(j)];
+    for (int ph = 0; ph < P.num_phases; ++ph) {
+      const dev_phase& D = P.phases[ph];
+      for (int tid = 0; tid < NT; ++tid) {
+        uint32_t toff = 0;
+        for (int x = 0; x < T; ++x) toff |= ((tid >> x) & 1u) << D.thr_pos[x];
+        cplx* a = &regs[size_t(tid) * NR];
+        for (int i = 0; i < NR; ++i) {
+          uint32_t j = toff;
+          for (int x = 0; x < R; ++x) if (i & (1 << x)) j |= 1u << D.reg_pos[x];
+          a[i] = tile[j];
+        }
+        for (int o = D.op_begin; o < D.op_end; ++o) {
+          const dev_op& op = P.ops[o];
+          if ((uint32_t(tid) & op.cthr) != op.cthr || (base & op.cout) != op.cout) continue;
+          const cplx m00{op.m[0], op.m[1]}, m01{op.m[2], op.m[3]}, m10{op.m[4], op.m[5]}, m11{op.m[6], op.m[7]};
+          for (int i = 0; i < NR; ++i) {
+            if ((uint32_t(i) & op.creg) != op.creg) continue;
+            if (op.kind == OPK_NEG) { a[i] = -a[i]; continue; }
+            if (op.kind == OPK_DIAG) {
+              const bool bit = (uint32_t(tid) & op.dthr) || (base & op.dout) || (uint32_t(i) & op.dreg);
+              if (bit) a[i] *= m01; else if (!op.diag_one) a[i] *= m00;
+              continue;
+            }
+            const int tb = 1 << op.treg;
+            if (i & tb) continue;
+            const cplx a0 = a[i], a1 = a[i | tb];
+            if (op.kind == OPK_X) { a[i] = a1; a[i | tb] = a0; }
+            else if (op.kind == OPK_Y) { a[i] = cplx{0, -1} * a1; a[i | tb] = cplx{0, 1} * a0; }
+            else { a[i] = m00 * a0 + m01 * a1; a[i | tb] = m10 * a0 + m11 * a1; }
+          }
+        }
+      }
+      std::vector<char> written(1u << K, 0);
+      for (int tid = 0; tid < NT; ++tid) {
+        uint32_t woff = 0;
+        for (int x = 0; x < T; ++x) woff |= ((tid >> x) & 1u) << D.wthr_pos[x];
+        for (int i = 0; i < NR; ++i) {
+          uint32_t j = woff;
+          for (int x = 0; x < R; ++x) if (i & (1 << x)) j |= 1u << D.wreg_pos[x];
+          if (j >= (1u << K) || written[j]) { std::fprintf(stderr, "bad write position\n"); std::exit(3); }
+          written[j] = 1;
+          next[j] = regs[size_t(tid) * NR + i];
+        }
+      }
+      tile.swap(next);
+    }
+    for (uint32_t j = 0; j < (1u << K); ++j) st[phys_of(j)] = tile[j];
+  }
+}
+
+static hgate random_gate(std::mt19937_64& rng, int n)
+{
+  hgate g{};
+  g.target2 = -1;
+  std::uniform_int_distribution<int> kind(0, 9), q(0, n - 1), nc(0, 2);
+  std::uniform_real_distribution<double> u(-1, 1);
+  const int k = kind(rng);
+  g.target = static_cast<int8_t>(q(rng));
+  const int ncontrols = nc(rng) == 2 ? 1 + (rng() % 2) : 0;
+  for (int c = 0; c < ncontrols; ++c) {
+    const int cq = q(rng);
+    if (cq != g.target) g.cmask |= 1ull << cq;
+  }
+  for (double& x : g.m) x = u(rng);
+  if (k <= 3) g.kind = OPK_MAT;
+  else if (k == 4) g.kind = OPK_X;
+  else if (k == 5) g.kind = OPK_Y;
+  else if (k == 6) { g.kind = OPK_DIAG; g.diag_one = rng() % 2; if (g.diag_one) { g.m[0] = 1; g.m[1] = 0; } }
+  else if (k == 7) { g.kind = OPK_NEG; g.cmask |= 1ull << g.target; g.target = -1; }
+  else {
+    g.kind = HK_SWAP;
+    g.cmask = 0;
+    do g.target2 = static_cast<int8_t>(q(rng)); while (g.target2 == g.target);
+  }
+  return g;
+}
+
+int main(int argc, char** argv)
+{
+  const int seeds = argc > 1 ? std::atoi(argv[1]) : 20;
+  int failures = 0;
+  for (int prec = 0; prec < 2; ++prec) {
+    plan_params p{};
+    if (prec == 0) { p.K = 12; p.R = 4; p.LOW = 5; p.vbits = 0; }
+    else { p.K = 13; p.R = 5; p.LOW = 6; p.vbits = 1; }
+    for (int seed = 0; seed < seeds; ++seed) {
+      std::mt19937_64 rng(1000 * prec + seed);
+      p.n = p.K + static_cast<int>(rng() % 4);
+      p.dense_budget = 1 + static_cast<int>(rng() % 16);
+      const uint64_t N = 1ull << p.n;
+      std::vector<cplx> init(N);
+      std::normal_distribution<double> nd;
+      for (auto& x : init) x = cplx{nd(rng), nd(rng)};
+      std::vector<hgate> gates;
+      const int count = 50 + static_cast<int>(rng() % 300);
+      for (int i = 0; i < count; ++i) gates.push_back(random_gate(rng, p.n));
+
+      std::vector<cplx> want = init;
+      for (const auto& g : gates) apply_direct(want, g);
+
+      std::vector<int> perm(p.n), inv(p.n);
+      for (int i = 0; i < p.n; ++i) perm[i] = inv[i] = i;
+      std::vector<dev_pass> passes;
+      plan_passes(p, gates, perm, inv, passes);
+      std::vector<cplx> st = init;
+      for (const auto& P : passes) run_pass(st, p, P);
+      std::vector<dev_pass> canon;
+      plan_canonicalize(p, perm, inv, canon);
+      for (const auto& P : canon) run_pass(st, p, P);
+      for (int i = 0; i < p.n; ++i) if (perm[i] != i) { std::printf("layout not canonical\n"); ++failures; break; }
+      double err = 0;
+      for (uint64_t i = 0; i < N; ++i) err = std::max(err, std::abs(st[i] - want[i]));
+      std::printf("prec=%d seed=%d n=%d gates=%d budget=%d passes=%zu canon=%zu err=%.3e\n", prec, seed, p.n, count,
+                  p.dense_budget, passes.size(), canon.size(), err);
+      if (!(err < 1e-9)) ++failures;
+    }
+  }
+  std::printf(failures ? "FAILED %d\n" : "ALL OK\n", failures);
+  return failures ? 1 : 0;
+}
