@@ -1,0 +1,352 @@
+"""Benchmark: HBM GB/s per state pass on the 30-qubit complex<double> brick
+circuit (H layer + 20 layers of U3 on every qubit and CNOT pairs, seeded
+angles, written with BEGIN/END FUSION blocks of <= 5 qubits), on one B200.
+
+A step applies the whole circuit to the state held in HBM.  value = state
+passes executed x bytes per pass (2 * 2^30 * 16 B = 34.36 GB) / step time,
+summed over ranks; the time is taken with CUDA events on the library's own
+stream (rbk_state_device_ms), max over ranks.  `e2e` repeats the measurement
+through the C ABI as a bra run sees it: reset to |0...0>, the gate calls,
+DO MEASUREMENT (all spins) and its read-back, all inside the timed region.
+
+--impl reference times the reference's own CPU code (ket + bra fused gates,
+release flags -Ofast -fopenmp, all host cores) on a bounded sample of the
+same circuit: the first fusion blocks of the 30-qubit run.
+
+Multi-GPU: the path does not shard in this tier, so --gpus N runs N
+independent replicas (one process per GPU, launched by torchrun).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QUBITS = 30
+DEPTH = 20
+FUSE_K = 5
+SEED = 1
+METRIC = "HBM GB/s per state pass (30q c128 brick, depth 20, fusion k<=5)"
+WORKLOAD = "brick circuit: 30 qubits, complex<double>, H layer + 20 layers of U3 (seeded) and CNOT pairs, BEGIN/END FUSION blocks of <= 5 qubits"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """dram bytes per launch of the pass kernel, from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def host_mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except Exception:
+        pass
+    return 0
+
+
+def reference_blocks(ops):
+    """Splits the instruction list into the reference's state passes: one per
+    fusion block, one per gate outside a block."""
+    blocks, cur, inside = [], [], False
+    for op in ops:
+        if op[0] == "BEGIN FUSION":
+            inside, cur = True, [op]
+        elif op[0] == "END FUSION":
+            cur.append(op)
+            blocks.append(cur)
+            inside, cur = False, []
+        elif inside:
+            cur.append(op)
+        else:
+            blocks.append([op])
+    return blocks
+
+
+class CpuReference:
+    """The reference's own ket/bra code, release build (oracle/_ref/libketref_fast.so)."""
+
+    def __init__(self, n, threads):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        self.kind = "reference"
+        self.state = oracle.KetRef(n, threads=threads, fast=True)
+        self.n, self.threads = n, threads
+
+    def run_blocks(self, blocks):
+        t = 0.0
+        for b in blocks:
+            t += self.state.apply_timed(b)
+        return t
+
+
+def cpu_sample(ops, threads, budget_s, n=N_QUBITS):
+    """Times reference passes of the workload on the host until budget_s of CPU
+    time is spent.  Returns (passes, seconds, description)."""
+    need = (16 << n) * 1.1
+    if host_mem_available() < need:
+        return None, None, f"host has {host_mem_available() / 2**30:.0f} GiB free, a {n}-qubit state needs {need / 2**30:.0f} GiB"
+    ref = CpuReference(n, threads)
+    blocks = reference_blocks(ops)
+    done, secs = 0, 0.0
+    while done < len(blocks) and secs < budget_s:
+        secs += ref.run_blocks([blocks[done]])
+        done += 1
+    desc = f"first {done} of {len(blocks)} reference passes (fusion blocks) of the {n}-qubit circuit"
+    return done, secs, desc
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world == 1:
+        return world, rank, local, None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local, dist
+
+
+def dist_max(dist, value, local):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, local):
+    if dist is not None:
+        import torch
+        dist.barrier(device_ids=[local])
+        torch.cuda.synchronize(local)
+
+
+def run_gpu(args):
+    world, rank, local, dist = dist_setup()
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    C = pkg.circuits
+    ops = C.brick(N_QUBITS, DEPTH, seed=SEED, fuse_k=FUSE_K)
+    ref_passes = C.reference_passes(ops)
+    bytes_pass = 2 * (1 << N_QUBITS) * 16
+
+    s = pkg.State(N_QUBITS, pkg.C128, device=local)
+    for _ in range(args.warmup):
+        s.apply(ops)
+        s.synchronize()
+
+    # ---- device-resident throughput: the circuit applied K times to the state in HBM
+    barrier(dist, local)
+    s.synchronize()
+    s.reset_stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.steps):
+        s.apply(ops)
+    ms = s.device_ms()  # CUDA events on the library's stream, first launch .. last completion
+    clk = clocks.stop()
+    st = s.stats()
+    ms_max = dist_max(dist, ms, local)
+    passes_per_step = st["passes"] / args.steps
+    value = world * st["passes"] * bytes_pass / (ms_max * 1e-3) / 1e9
+    launch_ms = ms / max(1, st["passes"])
+    achieved = bytes_pass / (launch_ms * 1e-3) / 1e9
+    peak, peak_kind = load_peaks()
+
+    # ---- end to end through the C ABI: reset, gate calls, DO MEASUREMENT, read-back
+    barrier(dist, local)
+    s.synchronize()
+    s.reset_stats()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.reset(0)
+        s.apply(ops)
+        spins = s.spins()  # flush + reduction passes + device->host copy of 3n doubles
+    e2e_s = time.perf_counter() - t0
+    e2e_max = dist_max(dist, e2e_s, local)
+    st_e = s.stats()
+    e2e_passes = st_e["passes"] / args.steps
+    e2e_value = world * args.steps * e2e_passes * bytes_pass / e2e_max / 1e9
+    assert math.isfinite(float(spins.sum()))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        done, secs, desc = cpu_sample(ops, threads, budget_s=args.cpu_budget)
+        if done:
+            cpu = {"value": done * bytes_pass / secs / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
+                   "sample": desc + f", {secs:.1f} s, reference release build (-Ofast -fopenmp)"}
+        else:
+            cpu = {"value": None, "unit": "GB/s", "cores": threads, "kind": "reference", "sample": desc}
+
+    traffic = load_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "depth": DEPTH, "fusion_k": FUSE_K, "seed": SEED,
+                   "passes_per_step": passes_per_step, "reference_passes_per_step": ref_passes,
+                   "bytes_per_pass": bytes_pass, "l2": "inputs larger than L2 (16 GiB state)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind,
+                     "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                     "kernel": "rbk::tile_pass_kernel<double>"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": int(e2e_passes * 12544),
+                "d2h_bytes_per_step": 8 * 3 * N_QUBITS,
+                "step": "reset |0..0>, gate calls through the C ABI, DO MEASUREMENT (all spins), read-back"},
+        "gpu_launches": st["kernel_launches"],
+        "clocks": clk,
+    }
+    s.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier(device_ids=[local])
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from __graft_entry__ import load_package
+    C = load_package().circuits
+    ops = C.brick(N_QUBITS, DEPTH, seed=SEED, fuse_k=FUSE_K)
+    bytes_pass = 2 * (1 << N_QUBITS) * 16
+    threads = os.cpu_count() or 1
+    need = (16 << N_QUBITS) * 1.1
+    if host_mem_available() < need:
+        print(json.dumps({"impl": "reference", "unavailable": f"host RAM: {host_mem_available() / 2**30:.0f} GiB free, "
+                                                             f"the 30-qubit state needs {need / 2**30:.0f} GiB"}))
+        return
+    ref = CpuReference(N_QUBITS, threads)
+    blocks = reference_blocks(ops)
+    per_step = max(1, args.ref_blocks_per_step)
+    pos = 0
+
+    def step():
+        nonlocal pos
+        chunk = [blocks[(pos + i) % len(blocks)] for i in range(per_step)]
+        pos += per_step
+        return ref.run_blocks(chunk)
+
+    for _ in range(args.warmup):
+        step()
+    secs = sum(step() for _ in range(args.steps))
+    value = args.steps * per_step * bytes_pass / secs / 1e9
+    sample = (f"{per_step} reference pass(es) (fusion blocks, in circuit order) of the 30-qubit circuit per step; "
+              f"reference release build (-Ofast -fopenmp), {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "depth": DEPTH, "fusion_k": FUSE_K, "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="rbk", choices=["rbk", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU reference work for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-blocks-per-step", type=int, default=1)
+    ap.add_argument("--qubits", type=int, default=N_QUBITS, help="smaller cases for profiling only")
+    ap.add_argument("--depth", type=int, default=DEPTH)
+    args = ap.parse_args()
+    globals()["N_QUBITS"], globals()["DEPTH"] = args.qubits, args.depth
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()
