@@ -252,7 +252,7 @@ def run_gpu(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        done, secs, desc = cpu_sample(ops, threads, budget_s=args.cpu_budget)
+        done, secs, desc = cpu_sample(ops, threads, budget_s=args.cpu_budget, n=N_QUBITS)
         if done:
             cpu = {"value": done * bytes_pass / secs / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
                    "sample": desc + f", {secs:.1f} s, reference release build (-Ofast -fopenmp)"}

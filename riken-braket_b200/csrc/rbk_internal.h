@@ -46,7 +46,7 @@ struct alignas(8) dev_op {
   uint8_t kind;
   uint8_t treg;       // MAT/X/Y: target register bit
   uint8_t diag_one;   // DIAG: d0 == 1 exactly (phase-shift form: only the one-half is touched)
-  uint8_t pad0;
+  uint8_t real;       // MAT: all four entries are real (H, exp(i theta Y), ...)
   uint32_t creg;      // controls inside the register bits
   uint32_t cthr;      // controls inside the thread bits
   uint32_t dreg;      // DIAG target bit among the register bits (mask), 0 if elsewhere
@@ -75,7 +75,9 @@ struct dev_pass {
   uint8_t nontile_phys[kMaxQubits];  // physical bits outside the tile, ascending
   uint8_t num_nontile;
   uint8_t num_phases;
-  uint8_t pad[6];
+  uint8_t direct_load;   // phase 0's layout reads HBM coalesced: load straight into registers
+  uint8_t direct_store;  // the last phase's write layout is coalesced: store straight from registers
+  uint8_t pad[4];
   dev_phase phases[kMaxPhases];
   dev_op ops[kMaxPassOps];
 };

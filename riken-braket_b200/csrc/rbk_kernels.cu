@@ -1,11 +1,6 @@
 // rbk_kernels.cu -- sm_100a kernels of the state-vector engine.
 //
-//   tile_pass_kernel   one fused pass: stage a 2^K-amplitude tile in shared
-//                      memory, apply a gate program in registers, write back
-//                      (optionally with the tile bits relabelled).  Replaces
-//                      ket's per-gate loops (ket/include/ket/gate/*.hpp, e.g.
-//                      hadamard.hpp:52-71, phase_shift.hpp:1235-1253) and bra's
-//                      fused replay (bra/src/nompi_state.cpp:1285-1357).
+//   (the fused tile pass lives in rbk_tile.cu)
 //   gate_kernel        one unfused gate straight on HBM (states smaller than a
 //                      tile, and the unfused execution mode).
 //   reductions         norm, probabilities, Z / pair sums for spins and Pauli
@@ -15,255 +10,15 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "rbk_device.cuh"
 #include "rbk_internal.h"
 #include "rbk_kernels.h"
 
 namespace rbk {
 
-template <typename Real> struct ctype;
-template <> struct ctype<double> { using c = double2; using v16 = double2; };
-template <> struct ctype<float> { using c = float2; using v16 = float4; };
-
-template <typename C>
-__device__ __forceinline__ C cmul(C a, C b) { return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
-template <typename C, typename Real>
-__device__ __forceinline__ C cmac2(C a0, C a1, Real m0r, Real m0i, Real m1r, Real m1i)
-{
-  // m0 * a0 + m1 * a1
-  C r;
-  r.x = m0r * a0.x - m0i * a0.y + m1r * a1.x - m1i * a1.y;
-  r.y = m0r * a0.y + m0i * a0.x + m1r * a1.y + m1i * a1.x;
-  return r;
-}
-
-// Shared-memory slot of tile index j: XOR-fold of the 16-byte-vector index so
-// that register layouts whose lanes sit on arbitrary tile bits still spread
-// over the banks.  Bijective (only bits >= 3 of the vector index feed the fold).
-template <int VEC>
-__device__ __forceinline__ uint32_t smem_slot(uint32_t j)
-{
-  constexpr int v = VEC == 2 ? 1 : 0;
-  uint32_t u = j >> v;
-  uint32_t f = (u >> 3) ^ (u >> 6) ^ (u >> 9) ^ (u >> 12);
-  u ^= f & 7u;
-  return (u << v) | (j & (VEC - 1));
-}
-
-// ---------------------------------------------------------------------------
-// Fused tile pass
-// ---------------------------------------------------------------------------
-template <typename Real>
-struct mat2 { Real m00r, m00i, m01r, m01i, m10r, m10i, m11r, m11i; };
-
-template <typename Real, int B, int NR>
-__device__ __forceinline__ void apply_mat(typename ctype<Real>::c* a, uint32_t creg, const mat2<Real> M)
-{
-  const Real m00r = M.m00r, m00i = M.m00i, m01r = M.m01r, m01i = M.m01i;
-  const Real m10r = M.m10r, m10i = M.m10i, m11r = M.m11r, m11i = M.m11i;
-#pragma unroll
-  for (int i = 0; i < NR; ++i) {
-    if (i & (1 << B)) continue;
-    if ((uint32_t(i) & creg) != creg) continue;
-    auto a0 = a[i], a1 = a[i | (1 << B)];
-    a[i] = cmac2(a0, a1, m00r, m00i, m01r, m01i);
-    a[i | (1 << B)] = cmac2(a0, a1, m10r, m10i, m11r, m11i);
-  }
-}
-
-template <typename Real, int B, int NR>
-__device__ __forceinline__ void apply_x(typename ctype<Real>::c* a, uint32_t creg)
-{
-#pragma unroll
-  for (int i = 0; i < NR; ++i) {
-    if (i & (1 << B)) continue;
-    if ((uint32_t(i) & creg) != creg) continue;
-    auto t = a[i]; a[i] = a[i | (1 << B)]; a[i | (1 << B)] = t;
-  }
-}
-
-template <typename Real, int B, int NR>
-__device__ __forceinline__ void apply_y(typename ctype<Real>::c* a, uint32_t creg)
-{
-#pragma unroll
-  for (int i = 0; i < NR; ++i) {
-    if (i & (1 << B)) continue;
-    if ((uint32_t(i) & creg) != creg) continue;
-    auto a0 = a[i], a1 = a[i | (1 << B)];
-    a[i] = typename ctype<Real>::c{a1.y, -a1.x};          // -i * a1
-    a[i | (1 << B)] = typename ctype<Real>::c{-a0.y, a0.x}; //  i * a0
-  }
-}
-
-// Runs F on register bit b (0 <= b < R); the bit must be a compile-time index
-// so that the register array stays in registers.
-#define RBK_DISPATCH_BIT(b, CALL)                                   \
-  switch (b) {                                                      \
-    case 0: { constexpr int BB = 0; CALL; } break;                  \
-    case 1: { constexpr int BB = 1; CALL; } break;                  \
-    case 2: { constexpr int BB = 2; CALL; } break;                  \
-    case 3: { constexpr int BB = 3; CALL; } break;                  \
-    case 4: if constexpr (R > 4) { constexpr int BB = 4; CALL; } break; \
-    default: break;                                                 \
-  }
-
-template <typename Real>
-__global__ void __launch_bounds__(1 << tiling<Real>::T, 2)
-tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_constant__ dev_pass P)
-{
-  using C = typename ctype<Real>::c;
-  using V = typename ctype<Real>::v16;
-  using TL = tiling<Real>;
-  constexpr int K = TL::K, R = TL::R, NR = 1 << R, NT = 1 << TL::T, VEC = TL::VEC;
-  constexpr int vbits = VEC == 2 ? 1 : 0;
-  constexpr int ITER = (1 << K) / VEC / NT;
-  constexpr int ITBITS = K - vbits - TL::T;
-  static_assert((1 << ITBITS) == ITER, "tile copy iterations");
-
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tile = reinterpret_cast<C*>(smem_raw);
-
-  const uint32_t tid = threadIdx.x;
-
-  // Tile base: deposit the block index into the physical bits outside the tile.
-  uint64_t base = 0;
-  {
-    uint64_t b = blockIdx.x;
-    for (int k = 0; k < P.num_nontile; ++k)
-      base |= ((b >> k) & 1ull) << P.nontile_phys[k];
-  }
-  // Physical offsets for the coalesced copy: tile index j = (it * NT + tid) * VEC.
-  uint64_t thr_phys = 0;
-#pragma unroll
-  for (int b = 0; b < TL::T; ++b) thr_phys |= uint64_t((tid >> b) & 1u) << P.tile_phys[vbits + b];
-  uint64_t it_bit_phys[ITBITS];
-#pragma unroll
-  for (int b = 0; b < ITBITS; ++b) it_bit_phys[b] = 1ull << P.tile_phys[vbits + TL::T + b];
-
-  const V* gsrc = reinterpret_cast<const V*>(state);
-#pragma unroll
-  for (int it = 0; it < ITER; ++it) {
-    uint64_t phys = base | thr_phys;
-#pragma unroll
-    for (int b = 0; b < ITBITS; ++b) if (it & (1 << b)) phys |= it_bit_phys[b];
-    const uint32_t j = uint32_t((it * NT + tid) * VEC);
-    V v = __ldcs(gsrc + (phys >> vbits));
-    *reinterpret_cast<V*>(&tile[smem_slot<VEC>(j)]) = v;
-  }
-  __syncthreads();
-
-  C a[NR];
-  for (int p = 0; p < P.num_phases; ++p) {
-    const dev_phase& ph = P.phases[p];
-    uint32_t toff = 0;
-#pragma unroll
-    for (int b = 0; b < TL::T; ++b) toff |= ((tid >> b) & 1u) << ph.thr_pos[b];
-    uint32_t rbit[R];
-#pragma unroll
-    for (int b = 0; b < R; ++b) rbit[b] = 1u << ph.reg_pos[b];
-#pragma unroll
-    for (int i = 0; i < NR; ++i) {
-      uint32_t j = toff;
-#pragma unroll
-      for (int b = 0; b < R; ++b) if (i & (1 << b)) j |= rbit[b];
-      a[i] = tile[smem_slot<VEC>(j)];
-    }
-
-    for (int o = ph.op_begin; o < ph.op_end; ++o) {
-      const dev_op& op = P.ops[o];
-      if ((tid & op.cthr) != op.cthr || (base & op.cout) != op.cout) continue;
-      switch (op.kind) {
-        case OPK_MAT: {
-          const mat2<Real> M{(Real)op.m[0], (Real)op.m[1], (Real)op.m[2], (Real)op.m[3],
-                             (Real)op.m[4], (Real)op.m[5], (Real)op.m[6], (Real)op.m[7]};
-          const uint32_t creg = op.creg;
-          RBK_DISPATCH_BIT(op.treg, (apply_mat<Real, BB, NR>(a, creg, M)));
-          break;
-        }
-        case OPK_X: { const uint32_t creg = op.creg; RBK_DISPATCH_BIT(op.treg, (apply_x<Real, BB, NR>(a, creg))); break; }
-        case OPK_Y: { const uint32_t creg = op.creg; RBK_DISPATCH_BIT(op.treg, (apply_y<Real, BB, NR>(a, creg))); break; }
-        case OPK_NEG: {
-#pragma unroll
-          for (int i = 0; i < NR; ++i)
-            if ((uint32_t(i) & op.creg) == op.creg) { a[i].x = -a[i].x; a[i].y = -a[i].y; }
-          break;
-        }
-        case OPK_DIAG: {
-          const bool tb = ((tid & op.dthr) != 0) || ((base & op.dout) != 0);
-          const C d0{(Real)op.m[0], (Real)op.m[1]}, d1{(Real)op.m[2], (Real)op.m[3]};
-#pragma unroll
-          for (int i = 0; i < NR; ++i) {
-            if ((uint32_t(i) & op.creg) != op.creg) continue;
-            const bool bit = tb || (uint32_t(i) & op.dreg);
-            if (bit) a[i] = cmul(a[i], d1);
-            else if (!op.diag_one) a[i] = cmul(a[i], d0);
-          }
-          break;
-        }
-        default: break;
-      }
-    }
-    __syncthreads();
-    uint32_t woff = 0;
-#pragma unroll
-    for (int b = 0; b < TL::T; ++b) woff |= ((tid >> b) & 1u) << ph.wthr_pos[b];
-#pragma unroll
-    for (int b = 0; b < R; ++b) rbit[b] = 1u << ph.wreg_pos[b];
-#pragma unroll
-    for (int i = 0; i < NR; ++i) {
-      uint32_t j = woff;
-#pragma unroll
-      for (int b = 0; b < R; ++b) if (i & (1 << b)) j |= rbit[b];
-      tile[smem_slot<VEC>(j)] = a[i];
-    }
-    __syncthreads();
-  }
-
-  V* gdst = reinterpret_cast<V*>(state);
-#pragma unroll
-  for (int it = 0; it < ITER; ++it) {
-    uint64_t phys = base | thr_phys;
-#pragma unroll
-    for (int b = 0; b < ITBITS; ++b) if (it & (1 << b)) phys |= it_bit_phys[b];
-    const uint32_t j = uint32_t((it * NT + tid) * VEC);
-    V v = *reinterpret_cast<const V*>(&tile[smem_slot<VEC>(j)]);
-    __stcs(gdst + (phys >> vbits), v);
-  }
-}
-
-template <typename Real>
-size_t tile_pass_smem_bytes() { return sizeof(typename ctype<Real>::c) << tiling<Real>::K; }
-
-template <typename Real>
-cudaError_t launch_tile_pass(void* state, int n, const dev_pass& pass, cudaStream_t stream)
-{
-  const size_t smem = tile_pass_smem_bytes<Real>();
-  static bool configured[64] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (!configured[dev]) {
-    e = cudaFuncSetAttribute(tile_pass_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured[dev] = true;
-  }
-  const uint64_t blocks = 1ull << (n - tiling<Real>::K);
-  tile_pass_kernel<Real><<<(unsigned)blocks, 1 << tiling<Real>::T, smem, stream>>>(
-    static_cast<typename ctype<Real>::c*>(state), pass);
-  return cudaGetLastError();
-}
-
-template cudaError_t launch_tile_pass<double>(void*, int, const dev_pass&, cudaStream_t);
-template cudaError_t launch_tile_pass<float>(void*, int, const dev_pass&, cudaStream_t);
-
 // ---------------------------------------------------------------------------
 // Unfused gate straight on HBM
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t insert_zero(uint64_t v, int q)
-{
-  const uint64_t low = (1ull << q) - 1;
-  return ((v & ~low) << 1) | (v & low);
-}
 
 template <typename Real>
 __global__ void gate_kernel(typename ctype<Real>::c* __restrict__ a, uint64_t size, const gate_rec g)

@@ -106,6 +106,80 @@ void order_thread_bits(std::vector<int>& thr, int vbits)
   thr = out;
 }
 
+// Qubits an op acts on non-diagonally (the target of MAT/X/Y) and diagonally
+// (controls, DIAG target, NEG bits), as physical masks.
+inline uint64_t n_mask(const pop& o) { return is_target_kind(o.kind) ? bit(o.target) : 0; }
+inline uint64_t z_mask(const pop& o) { return o.cmask | (o.kind == OPK_DIAG ? bit(o.target) : 0); }
+inline bool conflict(const pop& a, const pop& b)
+{
+  return (n_mask(a) & (n_mask(b) | z_mask(b))) || (z_mask(a) & n_mask(b));
+}
+
+struct phase_build { std::vector<int> reg; std::vector<int> ops; };
+
+// Register phases in program order: a new phase whenever a target misses the
+// current register set (the same rule as phase_tracker).
+std::vector<phase_build> phases_in_order(const std::vector<pop>& ops, const int* tile_of_phys, int R)
+{
+  std::vector<phase_build> phases(1);
+  for (int i = 0; i < static_cast<int>(ops.size()); ++i) {
+    const pop& o = ops[i];
+    if (is_target_kind(o.kind)) {
+      const int tb = tile_of_phys[o.target];
+      auto& cur = phases.back().reg;
+      if (std::find(cur.begin(), cur.end(), tb) == cur.end()) {
+        if (static_cast<int>(cur.size()) < R) cur.push_back(tb);
+        else { phases.emplace_back(); phases.back().reg.push_back(tb); }
+      }
+    }
+    phases.back().ops.push_back(i);
+  }
+  return phases;
+}
+
+// Register phases over the dependency graph of the pass: each phase sweeps
+// the ops in order and takes every op whose predecessors are done and whose
+// target is (or can still join) the phase's register set.  Gates that commute
+// are thereby gathered per register set (a light cone inside the registers).
+std::vector<phase_build> phases_by_dag(const std::vector<pop>& ops, const int* tile_of_phys, int R)
+{
+  const int m = static_cast<int>(ops.size());
+  std::vector<std::vector<int>> preds(m);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < j; ++i)
+      if (conflict(ops[i], ops[j])) preds[j].push_back(i);
+  std::vector<char> done(m, 0);
+  int remaining = m;
+  std::vector<phase_build> phases;
+  while (remaining > 0) {
+    phase_build pb;
+    bool progress = true;
+    while (progress) {
+      progress = false;
+      for (int j = 0; j < m; ++j) {
+        if (done[j]) continue;
+        bool ready = true;
+        for (int i : preds[j]) if (!done[i]) { ready = false; break; }
+        if (!ready) continue;
+        if (is_target_kind(ops[j].kind)) {
+          const int tb = tile_of_phys[ops[j].target];
+          if (std::find(pb.reg.begin(), pb.reg.end(), tb) == pb.reg.end()) {
+            if (static_cast<int>(pb.reg.size()) >= R) continue;
+            pb.reg.push_back(tb);
+          }
+        }
+        done[j] = 1;
+        --remaining;
+        pb.ops.push_back(j);
+        progress = true;
+      }
+    }
+    phases.push_back(pb);
+  }
+  if (phases.empty()) phases.emplace_back();
+  return phases;
+}
+
 void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>& ops,
                 const int* relabel_to, const int* tile_phys, dev_pass& out)
 {
@@ -122,40 +196,77 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     if (!(tile_mask & bit(q))) out.nontile_phys[nn++] = static_cast<uint8_t>(q);
   out.num_nontile = static_cast<uint8_t>(nn);
 
-  // Group ops into phases by register set.
-  struct phase_build { std::vector<int> reg; std::vector<int> ops; };
-  std::vector<phase_build> phases(1);
-  for (int i = 0; i < static_cast<int>(ops.size()); ++i) {
-    const pop& o = ops[i];
-    if (is_target_kind(o.kind)) {
-      const int tb = tile_of_phys[o.target];
-      auto& cur = phases.back().reg;
-      if (std::find(cur.begin(), cur.end(), tb) == cur.end()) {
-        if (static_cast<int>(cur.size()) < R) cur.push_back(tb);
-        else { phases.emplace_back(); phases.back().reg.push_back(tb); }
-      }
-    }
-    phases.back().ops.push_back(i);
-  }
+  std::vector<phase_build> phases = phases_by_dag(ops, tile_of_phys, R);
+  if (static_cast<int>(phases.size()) > kMaxPhases) phases = phases_in_order(ops, tile_of_phys, R);
   if (static_cast<int>(phases.size()) > kMaxPhases) throw std::logic_error("planner: too many phases");
+
+  // Tile bits lane0 .. lane0+4 are contiguous in HBM (512-byte runs); for c64
+  // tile bit 0 is the amplitude pair inside one 16-byte vector.
+  const int lane0 = p.vbits;
+  int relabel_from[16];
+  for (int b = 0; b < K; ++b) relabel_from[relabel_to[b]] = b;
+  auto contains = [](const std::vector<int>& v, int x) { return std::find(v.begin(), v.end(), x) != v.end(); };
 
   int op_index = 0;
   for (size_t ph = 0; ph < phases.size(); ++ph) {
     auto& pb = phases[ph];
-    // Fill the register set from the highest tile bits (the low ones make good lanes).
+    const bool first = ph == 0, last = ph + 1 == phases.size();
+    // Bits the fill should keep out of (or bring into) the registers so that
+    // the first phase can load and the last phase can store straight from HBM.
+    std::vector<int> keep_out, bring_in;
+    if (first) {
+      for (int l = 0; l < 5; ++l) keep_out.push_back(lane0 + l);
+      if (p.vbits) bring_in.push_back(0);
+    }
+    if (last) {
+      for (int l = 0; l < 5; ++l) keep_out.push_back(relabel_from[lane0 + l]);
+      if (p.vbits) bring_in.push_back(relabel_from[0]);
+    }
+    for (int b : bring_in)
+      if (!contains(pb.reg, b) && !contains(keep_out, b) && static_cast<int>(pb.reg.size()) < R) pb.reg.push_back(b);
     for (int b = K - 1; b >= 0 && static_cast<int>(pb.reg.size()) < R; --b)
-      if (std::find(pb.reg.begin(), pb.reg.end(), b) == pb.reg.end()) pb.reg.push_back(b);
+      if (!contains(pb.reg, b) && !contains(keep_out, b)) pb.reg.push_back(b);
+    for (int b = K - 1; b >= 0 && static_cast<int>(pb.reg.size()) < R; --b)
+      if (!contains(pb.reg, b)) pb.reg.push_back(b);
+
+    bool dl = false, ds = false;
+    if (first) {
+      dl = !p.vbits || contains(pb.reg, 0);
+      for (int l = 0; l < 5; ++l) dl = dl && !contains(pb.reg, lane0 + l);
+    }
+    if (last) {
+      ds = !p.vbits || contains(pb.reg, relabel_from[0]);
+      for (int l = 0; l < 5; ++l) ds = ds && !contains(pb.reg, relabel_from[lane0 + l]);
+      if (dl && ds) {  // one layout must serve both: only when the lanes (and the c64 pair bit) keep their place
+        for (int l = 0; l < 5; ++l) ds = ds && relabel_from[lane0 + l] == lane0 + l;
+        if (p.vbits) ds = ds && relabel_from[0] == 0;
+      }
+    }
     std::vector<int> thr;
-    for (int b = 0; b < K; ++b)
-      if (std::find(pb.reg.begin(), pb.reg.end(), b) == pb.reg.end()) thr.push_back(b);
-    order_thread_bits(thr, p.vbits);
+    for (int b = 0; b < K; ++b) if (!contains(pb.reg, b)) thr.push_back(b);
+    auto lanes_first = [&](const std::vector<int>& lanes) {
+      std::vector<int> o(lanes);
+      for (int b : thr) if (!contains(lanes, b)) o.push_back(b);
+      thr = o;
+    };
+    if (dl) lanes_first({lane0, lane0 + 1, lane0 + 2, lane0 + 3, lane0 + 4});
+    else if (ds) lanes_first({relabel_from[lane0], relabel_from[lane0 + 1], relabel_from[lane0 + 2],
+                              relabel_from[lane0 + 3], relabel_from[lane0 + 4]});
+    else order_thread_bits(thr, p.vbits);
+    // c64 vectors: register index bit 0 must be the amplitude pair bit.
+    if (p.vbits && (dl || ds)) {
+      const int want = dl ? 0 : relabel_from[0];
+      auto it = std::find(pb.reg.begin(), pb.reg.end(), want);
+      std::iter_swap(pb.reg.begin(), it);
+    }
+    if (first) out.direct_load = dl ? 1 : 0;
+    if (last) out.direct_store = ds ? 1 : 0;
 
     dev_phase& dp = out.phases[ph];
     int reg_index[64], thr_index[64];
     for (int i = 0; i < 64; ++i) reg_index[i] = thr_index[i] = -1;
     for (int b = 0; b < R; ++b) { dp.reg_pos[b] = static_cast<uint8_t>(pb.reg[b]); reg_index[pb.reg[b]] = b; }
     for (int b = 0; b < T; ++b) { dp.thr_pos[b] = static_cast<uint8_t>(thr[b]); thr_index[thr[b]] = b; }
-    const bool last = ph + 1 == phases.size();
     for (int b = 0; b < R; ++b) dp.wreg_pos[b] = static_cast<uint8_t>(last ? relabel_to[pb.reg[b]] : pb.reg[b]);
     for (int b = 0; b < T; ++b) dp.wthr_pos[b] = static_cast<uint8_t>(last ? relabel_to[thr[b]] : thr[b]);
 
@@ -166,6 +277,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
       d.kind = o.kind;
       d.diag_one = o.diag_one;
       std::memcpy(d.m, o.m, sizeof(d.m));
+      d.real = (o.kind == OPK_MAT && o.m[1] == 0.0 && o.m[3] == 0.0 && o.m[5] == 0.0 && o.m[7] == 0.0) ? 1 : 0;
       auto classify = [&](uint64_t phys_mask, uint32_t& reg, uint32_t& thrm, uint64_t& outm) {
         while (phys_mask) {
           const int q = __builtin_ctzll(phys_mask);

@@ -1,0 +1,314 @@
+// rbk_tile.cu -- the fused tile pass, the hot kernel of the engine.
+//
+// One pass reads and writes every amplitude once.  CTA b owns the tile of 2^K
+// amplitudes whose physical bits outside the pass's tile bits spell b.  The
+// tile moves through a sequence of register layouts ("phases"): in each phase
+// every thread holds 2^R amplitudes of the tile in registers, indexed by R
+// tile bits, and applies the phase's gates -- 2x2 matrices on a register bit,
+// with controls anywhere (register bits are checked per amplitude pair,
+// thread bits per thread, bits outside the tile per CTA).  Between phases the
+// tile is exchanged through shared memory.  The first phase loads straight
+// from HBM and the last phase stores straight to HBM when their layouts put
+// the lanes on the contiguous low tile bits; otherwise the tile is staged
+// through shared memory with coalesced 16-byte accesses.
+//
+// Replaces ket's per-gate sweeps (ket/include/ket/gate/hadamard.hpp:52-71,
+// phase_shift.hpp:1235-1253, pauli_x.hpp:120-165, ...) and bra's fused replay
+// of a BEGIN/END FUSION block on every 2^k chunk (bra/src/nompi_state.cpp:1285-1357).
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "rbk_device.cuh"
+#include "rbk_internal.h"
+#include "rbk_kernels.h"
+
+namespace rbk {
+namespace {
+
+template <typename Real>
+struct mat2 { Real m00r, m00i, m01r, m01i, m10r, m10i, m11r, m11i; };
+
+// Complex 2x2 on register bit B; CTRL: also require the register-bit controls.
+template <typename Real, int B, int NR, bool CTRL>
+__device__ __forceinline__ void apply_mat(typename ctype<Real>::c* a, uint32_t creg, const mat2<Real>& M)
+{
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    if (i & (1 << B)) continue;
+    if (CTRL && (uint32_t(i) & creg) != creg) continue;
+    const auto a0 = a[i], a1 = a[i | (1 << B)];
+    a[i] = cmac2(a0, a1, M.m00r, M.m00i, M.m01r, M.m01i);
+    a[i | (1 << B)] = cmac2(a0, a1, M.m10r, M.m10i, M.m11r, M.m11i);
+  }
+}
+
+// Real 2x2 (H, exp(i theta Y), ...): half the multiply-adds.
+template <typename Real, int B, int NR, bool CTRL>
+__device__ __forceinline__ void apply_real(typename ctype<Real>::c* a, uint32_t creg, Real m00, Real m01, Real m10, Real m11)
+{
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    if (i & (1 << B)) continue;
+    if (CTRL && (uint32_t(i) & creg) != creg) continue;
+    const auto a0 = a[i], a1 = a[i | (1 << B)];
+    a[i].x = m00 * a0.x + m01 * a1.x;
+    a[i].y = m00 * a0.y + m01 * a1.y;
+    a[i | (1 << B)].x = m10 * a0.x + m11 * a1.x;
+    a[i | (1 << B)].y = m10 * a0.y + m11 * a1.y;
+  }
+}
+
+template <typename Real, int B, int NR>
+__device__ __forceinline__ void apply_x(typename ctype<Real>::c* a, uint32_t creg)
+{
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    if (i & (1 << B)) continue;
+    if ((uint32_t(i) & creg) != creg) continue;
+    const auto t = a[i];
+    a[i] = a[i | (1 << B)];
+    a[i | (1 << B)] = t;
+  }
+}
+
+template <typename Real, int B, int NR>
+__device__ __forceinline__ void apply_y(typename ctype<Real>::c* a, uint32_t creg)
+{
+  using C = typename ctype<Real>::c;
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    if (i & (1 << B)) continue;
+    if ((uint32_t(i) & creg) != creg) continue;
+    const auto a0 = a[i], a1 = a[i | (1 << B)];
+    a[i] = C{a1.y, -a1.x};          // -i * a1
+    a[i | (1 << B)] = C{-a0.y, a0.x}; //  i * a0
+  }
+}
+
+// Runs CALL with the register bit b as the compile-time constant BB, so that
+// the register array is only ever indexed with constants.
+#define RBK_DISPATCH_BIT(b, CALL)                                       \
+  switch (b) {                                                          \
+    case 0: { constexpr int BB = 0; CALL; } break;                      \
+    case 1: { constexpr int BB = 1; CALL; } break;                      \
+    case 2: { constexpr int BB = 2; CALL; } break;                      \
+    case 3: { constexpr int BB = 3; CALL; } break;                      \
+    case 4: if constexpr (R > 4) { constexpr int BB = 4; CALL; } break; \
+    default: break;                                                     \
+  }
+
+template <typename Real, int R>
+__device__ __forceinline__ void apply_op(typename ctype<Real>::c* a, const dev_op& op, uint32_t tid, uint64_t base)
+{
+  using C = typename ctype<Real>::c;
+  constexpr int NR = 1 << R;
+  if ((tid & op.cthr) != op.cthr || (base & op.cout) != op.cout) return;
+  const uint32_t creg = op.creg;
+  switch (op.kind) {
+    case OPK_MAT:
+      if (op.real) {
+        const Real m00 = (Real)op.m[0], m01 = (Real)op.m[2], m10 = (Real)op.m[4], m11 = (Real)op.m[6];
+        if (creg == 0) { RBK_DISPATCH_BIT(op.treg, (apply_real<Real, BB, NR, false>(a, 0u, m00, m01, m10, m11))); }
+        else { RBK_DISPATCH_BIT(op.treg, (apply_real<Real, BB, NR, true>(a, creg, m00, m01, m10, m11))); }
+      } else {
+        const mat2<Real> M{(Real)op.m[0], (Real)op.m[1], (Real)op.m[2], (Real)op.m[3],
+                           (Real)op.m[4], (Real)op.m[5], (Real)op.m[6], (Real)op.m[7]};
+        if (creg == 0) { RBK_DISPATCH_BIT(op.treg, (apply_mat<Real, BB, NR, false>(a, 0u, M))); }
+        else { RBK_DISPATCH_BIT(op.treg, (apply_mat<Real, BB, NR, true>(a, creg, M))); }
+      }
+      break;
+    case OPK_X: RBK_DISPATCH_BIT(op.treg, (apply_x<Real, BB, NR>(a, creg))); break;
+    case OPK_Y: RBK_DISPATCH_BIT(op.treg, (apply_y<Real, BB, NR>(a, creg))); break;
+    case OPK_NEG:
+#pragma unroll
+      for (int i = 0; i < NR; ++i)
+        if ((uint32_t(i) & creg) == creg) { a[i].x = -a[i].x; a[i].y = -a[i].y; }
+      break;
+    case OPK_DIAG: {
+      const bool tb = ((tid & op.dthr) != 0) || ((base & op.dout) != 0);
+      const C d0{(Real)op.m[0], (Real)op.m[1]}, d1{(Real)op.m[2], (Real)op.m[3]};
+      const uint32_t dreg = op.dreg;
+      const bool one = op.diag_one;
+#pragma unroll
+      for (int i = 0; i < NR; ++i) {
+        if ((uint32_t(i) & creg) != creg) continue;
+        const bool bit = tb || (uint32_t(i) & dreg);
+        if (bit) a[i] = cmul(a[i], d1);
+        else if (!one) a[i] = cmul(a[i], d0);
+      }
+      break;
+    }
+    default: break;
+  }
+}
+
+}  // namespace
+
+namespace {
+
+// 16-byte vectors <-> register amplitudes (1 amplitude for c128, 2 for c64).
+template <typename Real> struct vec_io;
+template <> struct vec_io<double> {
+  static __device__ __forceinline__ void unpack(double2 v, double2* a) { a[0] = v; }
+  static __device__ __forceinline__ double2 pack(const double2* a) { return a[0]; }
+};
+template <> struct vec_io<float> {
+  static __device__ __forceinline__ void unpack(float4 v, float2* a) { a[0] = float2{v.x, v.y}; a[1] = float2{v.z, v.w}; }
+  static __device__ __forceinline__ float4 pack(const float2* a) { return float4{a[0].x, a[0].y, a[1].x, a[1].y}; }
+};
+
+}  // namespace
+
+template <typename Real>
+__global__ void __launch_bounds__(1 << tiling<Real>::T, 2)
+tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_constant__ dev_pass P)
+{
+  using C = typename ctype<Real>::c;
+  using V = typename ctype<Real>::v16;
+  using TL = tiling<Real>;
+  constexpr int K = TL::K, R = TL::R, NR = 1 << R, T = TL::T, NT = 1 << T, VEC = TL::VEC;
+  constexpr int VB = VEC == 2 ? 1 : 0;
+  constexpr int ITER = (1 << K) / VEC / NT;
+  constexpr int ITBITS = K - VB - T;
+  static_assert((1 << ITBITS) == ITER, "tile copy iterations");
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  const V* gsrc = reinterpret_cast<const V*>(state);
+  V* gdst = reinterpret_cast<V*>(state);
+  const uint32_t tid = threadIdx.x;
+
+  // Tile base: the block index deposited into the physical bits outside the tile.
+  uint64_t base = 0;
+  {
+    const uint64_t b = blockIdx.x;
+    for (int k = 0; k < P.num_nontile; ++k) base |= ((b >> k) & 1ull) << P.nontile_phys[k];
+  }
+
+  // Coalesced staging copy: vector u = it * NT + tid holds tile index u << VB;
+  // consecutive threads read consecutive 16-byte vectors of a contiguous run.
+  auto staged_copy = [&](bool to_smem) {
+    uint64_t thr_phys = base;
+#pragma unroll
+    for (int b = 0; b < T; ++b) thr_phys |= uint64_t((tid >> b) & 1u) << P.tile_phys[VB + b];
+    const uint32_t thr_slot = smem_slot<VB>(tid << VB);
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+      uint64_t phys = thr_phys;
+#pragma unroll
+      for (int b = 0; b < ITBITS; ++b)
+        if (it & (1 << b)) phys |= 1ull << P.tile_phys[VB + T + b];
+      V* s = reinterpret_cast<V*>(&tile[thr_slot ^ smem_slot<VB>(uint32_t(it * NT) << VB)]);
+      if (to_smem) *s = __ldcs(gsrc + (phys >> VB));
+      else __stcs(gdst + (phys >> VB), *s);
+    }
+  };
+
+  if (!P.direct_load) {
+    staged_copy(true);
+    __syncthreads();
+  }
+
+  C a[NR];
+  const int nph = P.num_phases;
+  for (int p = 0; p < nph; ++p) {
+    const dev_phase& ph = P.phases[p];
+    if (p == 0 && P.direct_load) {
+      uint64_t tphys = base;
+#pragma unroll
+      for (int b = 0; b < T; ++b) tphys |= uint64_t((tid >> b) & 1u) << P.tile_phys[ph.thr_pos[b]];
+      uint64_t rphys[R];
+#pragma unroll
+      for (int b = 0; b < R; ++b) rphys[b] = 1ull << P.tile_phys[ph.reg_pos[b]];
+#pragma unroll
+      for (int i = 0; i < NR; i += VEC) {
+        uint64_t phys = tphys;
+#pragma unroll
+        for (int b = VB; b < R; ++b) if (i & (1 << b)) phys |= rphys[b];
+        vec_io<Real>::unpack(__ldcs(gsrc + (phys >> VB)), &a[i]);
+      }
+    } else {
+      uint32_t toff = 0;
+#pragma unroll
+      for (int b = 0; b < T; ++b) toff |= ((tid >> b) & 1u) << ph.thr_pos[b];
+      const uint32_t ts = smem_slot<VB>(toff);
+      uint32_t rs[R];
+#pragma unroll
+      for (int b = 0; b < R; ++b) rs[b] = smem_slot<VB>(1u << ph.reg_pos[b]);
+#pragma unroll
+      for (int i = 0; i < NR; ++i) {
+        uint32_t sidx = ts;
+#pragma unroll
+        for (int b = 0; b < R; ++b) if (i & (1 << b)) sidx ^= rs[b];
+        a[i] = tile[sidx];
+      }
+    }
+
+    for (int o = ph.op_begin; o < ph.op_end; ++o) apply_op<Real, R>(a, P.ops[o], tid, base);
+
+    if (p + 1 == nph && P.direct_store) {
+      uint64_t tphys = base;
+#pragma unroll
+      for (int b = 0; b < T; ++b) tphys |= uint64_t((tid >> b) & 1u) << P.tile_phys[ph.wthr_pos[b]];
+      uint64_t rphys[R];
+#pragma unroll
+      for (int b = 0; b < R; ++b) rphys[b] = 1ull << P.tile_phys[ph.wreg_pos[b]];
+#pragma unroll
+      for (int i = 0; i < NR; i += VEC) {
+        uint64_t phys = tphys;
+#pragma unroll
+        for (int b = VB; b < R; ++b) if (i & (1 << b)) phys |= rphys[b];
+        __stcs(gdst + (phys >> VB), vec_io<Real>::pack(&a[i]));
+      }
+    } else {
+      __syncthreads();  // every thread has read this phase's layout
+      uint32_t woff = 0;
+#pragma unroll
+      for (int b = 0; b < T; ++b) woff |= ((tid >> b) & 1u) << ph.wthr_pos[b];
+      const uint32_t ts = smem_slot<VB>(woff);
+      uint32_t rs[R];
+#pragma unroll
+      for (int b = 0; b < R; ++b) rs[b] = smem_slot<VB>(1u << ph.wreg_pos[b]);
+#pragma unroll
+      for (int i = 0; i < NR; ++i) {
+        uint32_t sidx = ts;
+#pragma unroll
+        for (int b = 0; b < R; ++b) if (i & (1 << b)) sidx ^= rs[b];
+        tile[sidx] = a[i];
+      }
+      __syncthreads();
+    }
+  }
+
+  if (!P.direct_store) staged_copy(false);
+}
+
+template <typename Real>
+size_t tile_pass_smem_bytes() { return sizeof(typename ctype<Real>::c) << tiling<Real>::K; }
+
+template <typename Real>
+cudaError_t launch_tile_pass(void* state, int n, const dev_pass& pass, cudaStream_t stream)
+{
+  const size_t smem = tile_pass_smem_bytes<Real>();
+  static bool configured[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!configured[dev]) {
+    e = cudaFuncSetAttribute(tile_pass_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured[dev] = true;
+  }
+  const uint64_t blocks = 1ull << (n - tiling<Real>::K);
+  tile_pass_kernel<Real><<<(unsigned)blocks, 1 << tiling<Real>::T, smem, stream>>>(
+    static_cast<typename ctype<Real>::c*>(state), pass);
+  return cudaGetLastError();
+}
+
+template size_t tile_pass_smem_bytes<double>();
+template size_t tile_pass_smem_bytes<float>();
+template cudaError_t launch_tile_pass<double>(void*, int, const dev_pass&, cudaStream_t);
+template cudaError_t launch_tile_pass<float>(void*, int, const dev_pass&, cudaStream_t);
+
+}  // namespace rbk
