@@ -87,6 +87,10 @@ int rbk_flush(rbk_state* s);
 int rbk_state_set_deferred(rbk_state* s, int deferred);
 /* Upper bound on dense 2x2 gates per fused pass (0 = built-in default). */
 int rbk_state_set_pass_budget(rbk_state* s, int max_dense_gates_per_pass);
+/* Tile shape of the fused passes: 0 = 2^12 amplitudes (c128; 2^13 for c64)
+ * with 16 per thread, 1 = the same tile with 8 per thread, 2 = 2^11 (c128;
+ * 2^12 for c64) with 16 per thread (the default).  Results do not depend on it. */
+int rbk_state_set_tile_shape(rbk_state* s, int shape);
 int rbk_state_get_stats(const rbk_state* s, rbk_stats* out);
 int rbk_state_reset_stats(rbk_state* s);
 /* Milliseconds of device time spent in this state's kernels since the last

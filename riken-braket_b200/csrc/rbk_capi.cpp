@@ -34,6 +34,7 @@ struct rbk_state {
   bool deferred = true;
   bool in_fusion = false;
   int dense_budget = 0;
+  int shape = 2;
   rbk_stats stats{};
   cudaEvent_t ev_first = nullptr, ev_last = nullptr, ev_sync = nullptr;
   bool timing_started = false;
@@ -102,16 +103,19 @@ rbk::plan_params params_of(const rbk_state* s)
 {
   rbk::plan_params p{};
   p.n = s->n;
-  if (s->precision == RBK_C128) {
-    p.K = rbk::tiling<double>::K; p.R = rbk::tiling<double>::R; p.LOW = rbk::tiling<double>::LOW; p.vbits = 0;
-  } else {
-    p.K = rbk::tiling<float>::K; p.R = rbk::tiling<float>::R; p.LOW = rbk::tiling<float>::LOW; p.vbits = 1;
-  }
+  rbk::shape_bits(s->precision, s->shape, &p.K, &p.R);
+  p.LOW = s->precision == RBK_C128 ? rbk::precision_traits<double>::LOW : rbk::precision_traits<float>::LOW;
+  p.vbits = s->precision == RBK_C128 ? 0 : 1;
   p.dense_budget = s->dense_budget > 0 ? s->dense_budget : (s->precision == RBK_C128 ? 12 : 16);
   return p;
 }
 
-int tile_bits(const rbk_state* s) { return s->precision == RBK_C128 ? rbk::tiling<double>::K : rbk::tiling<float>::K; }
+int tile_bits(const rbk_state* s)
+{
+  int K = 0, R = 0;
+  rbk::shape_bits(s->precision, s->shape, &K, &R);
+  return K;
+}
 
 int mark_launch_start(rbk_state* s)
 {
@@ -126,8 +130,8 @@ int run_passes(rbk_state* s, const std::vector<rbk::dev_pass>& passes)
 {
   for (const auto& pass : passes) {
     const cudaError_t e = s->precision == RBK_C128
-      ? rbk::launch_tile_pass<double>(s->amps, s->n, pass, s->stream)
-      : rbk::launch_tile_pass<float>(s->amps, s->n, pass, s->stream);
+      ? rbk::launch_tile_pass<double>(s->amps, s->n, pass, s->shape, s->stream)
+      : rbk::launch_tile_pass<float>(s->amps, s->n, pass, s->shape, s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "tile pass launch");
     ++s->stats.kernel_launches;
   }
@@ -519,6 +523,15 @@ int rbk_state_set_pass_budget(rbk_state* s, int max_dense)
   if (int rc = check_state(s)) return rc;
   if (max_dense < 0) return fail(RBK_ERR_INVALID, "negative budget");
   s->dense_budget = max_dense;
+  return RBK_OK;
+}
+
+int rbk_state_set_tile_shape(rbk_state* s, int shape)
+{
+  if (int rc = check_state(s)) return rc;
+  if (shape < 0 || shape >= rbk::kNumShapes) return fail(RBK_ERR_INVALID, "unknown tile shape");
+  if (int rc = guarded([&] { return canonicalize(s); })) return rc;
+  s->shape = shape;
   return RBK_OK;
 }
 

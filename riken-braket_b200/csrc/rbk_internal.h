@@ -16,18 +16,33 @@
 
 namespace rbk {
 
-// Register tiling per precision.
-//   c128 (complex<double>, 16 B): K = 12 tile bits, R = 4 register bits,
-//        256 threads, 64 KiB of shared memory per tile.
-//   c64  (complex<float>,  8 B):  K = 13 tile bits, R = 5 register bits,
-//        256 threads, 64 KiB of shared memory per tile.
-template <typename Real> struct tiling;
-template <> struct tiling<double> {
-  static constexpr int K = 12, R = 4, T = K - R, VEC = 1, LOW = 5, SWZ = 3;
-};
-template <> struct tiling<float> {
-  static constexpr int K = 13, R = 5, T = K - R, VEC = 2, LOW = 6, SWZ = 4;
-};
+// Tile shapes.  A shape fixes the tile bits K (2^K amplitudes per CTA) and
+// the register bits R (2^R amplitudes per thread, 2^(K-R) threads); LOW low
+// physical bits are always tile bits (512-byte contiguous runs in HBM).
+//   shape 0: K = 12 (c128) / 13 (c64), 256 threads, 2 CTAs per SM
+//   shape 1: same tile, half the registers per thread, 512 threads
+//   shape 2: K = 11 (c128) / 12 (c64), 128 threads, 4 CTAs per SM
+constexpr int kNumShapes = 3;
+template <typename Real> struct precision_traits;
+template <> struct precision_traits<double> { static constexpr int VEC = 1, VB = 0, LOW = 5; };
+template <> struct precision_traits<float> { static constexpr int VEC = 2, VB = 1, LOW = 6; };
+
+template <typename Real, int SHAPE> struct tile_shape;
+template <> struct tile_shape<double, 0> { static constexpr int K = 12, R = 4, CTAS = 2; };
+template <> struct tile_shape<double, 1> { static constexpr int K = 12, R = 3, CTAS = 2; };
+template <> struct tile_shape<double, 2> { static constexpr int K = 11, R = 4, CTAS = 4; };
+template <> struct tile_shape<float, 0> { static constexpr int K = 13, R = 5, CTAS = 2; };
+template <> struct tile_shape<float, 1> { static constexpr int K = 13, R = 4, CTAS = 2; };
+template <> struct tile_shape<float, 2> { static constexpr int K = 12, R = 5, CTAS = 4; };
+
+// Host view of a tile shape: tile bits, register bits (precision 0 = c128, 1 = c64).
+inline void shape_bits(int precision, int shape, int* K, int* R)
+{
+  static const int k128[kNumShapes] = {12, 12, 11}, r128[kNumShapes] = {4, 3, 4};
+  static const int k64[kNumShapes] = {13, 13, 12}, r64[kNumShapes] = {5, 4, 5};
+  *K = precision == 0 ? k128[shape] : k64[shape];
+  *R = precision == 0 ? r128[shape] : r64[shape];
+}
 
 constexpr int kMaxPassOps = 112;
 constexpr int kMaxPhases = 16;
@@ -61,8 +76,16 @@ struct alignas(8) dev_op {
 // register slot i of thread t:  j = sum_b bit_b(i) << reg_pos[b]  |  sum_b bit_b(t) << thr_pos[b].
 // After the phase's gates the registers are written back at positions given by
 // wreg_pos / wthr_pos (equal to reg_pos / thr_pos except in the last phase,
-// where they carry the pass's relabelling of tile bits).
+// where they carry the pass's relabelling of tile bits).  The host also
+// precomputes the shared-memory slots of these positions: rslot[b] for
+// register bit b, and tslot_lo[t & 15] ^ tslot_hi[t >> 4] for thread t (up to
+// 9 thread bits; the
+// slot map is linear, so a thread XORs them together).
 struct dev_phase {
+  uint16_t rslot[8];
+  uint16_t wslot[8];
+  uint16_t tslot_lo[16], tslot_hi[32];
+  uint16_t wtslot_lo[16], wtslot_hi[32];
   uint8_t reg_pos[8];
   uint8_t thr_pos[16];
   uint8_t wreg_pos[8];
@@ -70,14 +93,24 @@ struct dev_phase {
   uint16_t op_begin, op_end;
 };
 
+// Physical offsets of a register layout for direct HBM access: register bit b
+// adds rphys[b]; thread t adds tphys_lo[t & 15] | tphys_hi[t >> 4].
+struct dev_hbm_layout {
+  uint64_t rphys[8];
+  uint64_t tphys_lo[16], tphys_hi[32];
+};
+
 struct dev_pass {
   uint8_t tile_phys[16];      // physical bit of tile bit b
-  uint8_t nontile_phys[kMaxQubits];  // physical bits outside the tile, ascending
-  uint8_t num_nontile;
+  uint8_t num_runs;           // the block index is deposited into the non-tile bits run by run:
+  uint8_t run_src[16];        //   base |= ((block >> run_src) & mask(run_len)) << run_dst
+  uint8_t run_len[16];
+  uint8_t run_dst[16];
   uint8_t num_phases;
   uint8_t direct_load;   // phase 0's layout reads HBM coalesced: load straight into registers
   uint8_t direct_store;  // the last phase's write layout is coalesced: store straight from registers
   uint8_t pad[4];
+  dev_hbm_layout load, store;
   dev_phase phases[kMaxPhases];
   dev_op ops[kMaxPassOps];
 };

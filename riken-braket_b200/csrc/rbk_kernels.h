@@ -20,8 +20,8 @@ struct pauli_terms {
   double w[kMaxPauliTerms][2];
 };
 
-template <typename Real> size_t tile_pass_smem_bytes();
-template <typename Real> cudaError_t launch_tile_pass(void* state, int n, const dev_pass& pass, cudaStream_t stream);
+// One fused pass with tile shape `shape` (see tile_shape in rbk_internal.h).
+template <typename Real> cudaError_t launch_tile_pass(void* state, int n, const dev_pass& pass, int shape, cudaStream_t stream);
 template <typename Real> cudaError_t launch_gate(void* state, int n, const gate_rec& g, cudaStream_t stream);
 template <typename Real> cudaError_t launch_set_basis(void* state, int n, uint64_t index, cudaStream_t stream);
 

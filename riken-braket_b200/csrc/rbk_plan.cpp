@@ -106,6 +106,15 @@ void order_thread_bits(std::vector<int>& thr, int vbits)
   thr = out;
 }
 
+// Host copy of smem_slot in rbk_device.cuh (shared-memory slot of tile index j).
+uint32_t smem_slot_host(uint32_t j, int vbits)
+{
+  uint32_t u = j >> vbits;
+  const uint32_t f = (u >> 3) ^ (u >> 6) ^ (u >> 9) ^ (u >> 12);
+  u ^= f & 7u;
+  return (u << vbits) | (j & ((1u << vbits) - 1));
+}
+
 // Qubits an op acts on non-diagonally (the target of MAT/X/Y) and diagonally
 // (controls, DIAG target, NEG bits), as physical masks.
 inline uint64_t n_mask(const pop& o) { return is_target_kind(o.kind) ? bit(o.target) : 0; }
@@ -191,10 +200,22 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     out.tile_phys[b] = static_cast<uint8_t>(tile_phys[b]);
     tile_of_phys[tile_phys[b]] = b;
   }
-  int nn = 0;
-  for (int q = 0; q < p.n; ++q)
-    if (!(tile_mask & bit(q))) out.nontile_phys[nn++] = static_cast<uint8_t>(q);
-  out.num_nontile = static_cast<uint8_t>(nn);
+  // Non-tile physical bits as runs of consecutive bits.
+  {
+    int runs = 0, src = 0;
+    for (int q = 0; q < p.n;) {
+      if (tile_mask & bit(q)) { ++q; continue; }
+      int len = 0;
+      while (q + len < p.n && !(tile_mask & bit(q + len))) ++len;
+      out.run_src[runs] = static_cast<uint8_t>(src);
+      out.run_len[runs] = static_cast<uint8_t>(len);
+      out.run_dst[runs] = static_cast<uint8_t>(q);
+      ++runs;
+      src += len;
+      q += len;
+    }
+    out.num_runs = static_cast<uint8_t>(runs);
+  }
 
   std::vector<phase_build> phases = phases_by_dag(ops, tile_of_phys, R);
   if (static_cast<int>(phases.size()) > kMaxPhases) phases = phases_in_order(ops, tile_of_phys, R);
@@ -269,6 +290,42 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     for (int b = 0; b < T; ++b) { dp.thr_pos[b] = static_cast<uint8_t>(thr[b]); thr_index[thr[b]] = b; }
     for (int b = 0; b < R; ++b) dp.wreg_pos[b] = static_cast<uint8_t>(last ? relabel_to[pb.reg[b]] : pb.reg[b]);
     for (int b = 0; b < T; ++b) dp.wthr_pos[b] = static_cast<uint8_t>(last ? relabel_to[thr[b]] : thr[b]);
+
+    // Precomputed shared-memory slots (the slot map is linear) and HBM offsets.
+    if (T < 5 || T > 9) throw std::logic_error("planner: layout tables hold 5 to 9 thread bits");
+    for (int b = 0; b < R; ++b) {
+      dp.rslot[b] = static_cast<uint16_t>(smem_slot_host(1u << dp.reg_pos[b], p.vbits));
+      dp.wslot[b] = static_cast<uint16_t>(smem_slot_host(1u << dp.wreg_pos[b], p.vbits));
+    }
+    for (int x = 0; x < 32; ++x) {
+      uint32_t lo = 0, hi = 0, wlo = 0, whi = 0;
+      for (int k = 0; k < 5; ++k) {
+        if (!((x >> k) & 1)) continue;
+        if (k < 4) { lo |= 1u << dp.thr_pos[k]; wlo |= 1u << dp.wthr_pos[k]; }
+        if (4 + k < T) { hi |= 1u << dp.thr_pos[4 + k]; whi |= 1u << dp.wthr_pos[4 + k]; }
+      }
+      if (x < 16) {
+        dp.tslot_lo[x] = static_cast<uint16_t>(smem_slot_host(lo, p.vbits));
+        dp.wtslot_lo[x] = static_cast<uint16_t>(smem_slot_host(wlo, p.vbits));
+      }
+      dp.tslot_hi[x] = static_cast<uint16_t>(smem_slot_host(hi, p.vbits));
+      dp.wtslot_hi[x] = static_cast<uint16_t>(smem_slot_host(whi, p.vbits));
+    }
+    auto hbm = [&](dev_hbm_layout& L, const uint8_t* rpos, const uint8_t* tpos) {
+      for (int b = 0; b < R; ++b) L.rphys[b] = bit(tile_phys[rpos[b]]);
+      for (int x = 0; x < 32; ++x) {
+        uint64_t lo = 0, hi = 0;
+        for (int k = 0; k < 5; ++k) {
+          if (!((x >> k) & 1)) continue;
+          if (k < 4) lo |= bit(tile_phys[tpos[k]]);
+          if (4 + k < T) hi |= bit(tile_phys[tpos[4 + k]]);
+        }
+        if (x < 16) L.tphys_lo[x] = lo;
+        L.tphys_hi[x] = hi;
+      }
+    };
+    if (first && dl) hbm(out.load, dp.reg_pos, dp.thr_pos);
+    if (last && ds) hbm(out.store, dp.wreg_pos, dp.wthr_pos);
 
     dp.op_begin = static_cast<uint16_t>(op_index);
     for (int oi : pb.ops) {

@@ -159,18 +159,19 @@ template <> struct vec_io<float> {
 
 }  // namespace
 
-template <typename Real>
-__global__ void __launch_bounds__(1 << tiling<Real>::T, 2)
+template <typename Real, int SHAPE>
+__global__ void __launch_bounds__(1 << (tile_shape<Real, SHAPE>::K - tile_shape<Real, SHAPE>::R), tile_shape<Real, SHAPE>::CTAS)
 tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_constant__ dev_pass P)
 {
   using C = typename ctype<Real>::c;
   using V = typename ctype<Real>::v16;
-  using TL = tiling<Real>;
-  constexpr int K = TL::K, R = TL::R, NR = 1 << R, T = TL::T, NT = 1 << T, VEC = TL::VEC;
-  constexpr int VB = VEC == 2 ? 1 : 0;
+  using SH = tile_shape<Real, SHAPE>;
+  using PT = precision_traits<Real>;
+  constexpr int K = SH::K, R = SH::R, NR = 1 << R, T = K - R, NT = 1 << T, VEC = PT::VEC, VB = PT::VB;
   constexpr int ITER = (1 << K) / VEC / NT;
   constexpr int ITBITS = K - VB - T;
   static_assert((1 << ITBITS) == ITER, "tile copy iterations");
+  static_assert(T >= 5 && T <= 9, "the layout tables split the thread index into 4 + up to 5 bits");
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tile = reinterpret_cast<C*>(smem_raw);
@@ -182,7 +183,8 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
   uint64_t base = 0;
   {
     const uint64_t b = blockIdx.x;
-    for (int k = 0; k < P.num_nontile; ++k) base |= ((b >> k) & 1ull) << P.nontile_phys[k];
+    for (int r = 0; r < P.num_runs; ++r)
+      base |= ((b >> P.run_src[r]) & ((1ull << P.run_len[r]) - 1)) << P.run_dst[r];
   }
 
   // Coalesced staging copy: vector u = it * NT + tid holds tile index u << VB;
@@ -214,12 +216,10 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
   for (int p = 0; p < nph; ++p) {
     const dev_phase& ph = P.phases[p];
     if (p == 0 && P.direct_load) {
-      uint64_t tphys = base;
-#pragma unroll
-      for (int b = 0; b < T; ++b) tphys |= uint64_t((tid >> b) & 1u) << P.tile_phys[ph.thr_pos[b]];
+      const uint64_t tphys = base | P.load.tphys_lo[tid & 15] | P.load.tphys_hi[tid >> 4];
       uint64_t rphys[R];
 #pragma unroll
-      for (int b = 0; b < R; ++b) rphys[b] = 1ull << P.tile_phys[ph.reg_pos[b]];
+      for (int b = 0; b < R; ++b) rphys[b] = P.load.rphys[b];
 #pragma unroll
       for (int i = 0; i < NR; i += VEC) {
         uint64_t phys = tphys;
@@ -228,13 +228,10 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
         vec_io<Real>::unpack(__ldcs(gsrc + (phys >> VB)), &a[i]);
       }
     } else {
-      uint32_t toff = 0;
-#pragma unroll
-      for (int b = 0; b < T; ++b) toff |= ((tid >> b) & 1u) << ph.thr_pos[b];
-      const uint32_t ts = smem_slot<VB>(toff);
+      const uint32_t ts = ph.tslot_lo[tid & 15] ^ ph.tslot_hi[tid >> 4];
       uint32_t rs[R];
 #pragma unroll
-      for (int b = 0; b < R; ++b) rs[b] = smem_slot<VB>(1u << ph.reg_pos[b]);
+      for (int b = 0; b < R; ++b) rs[b] = ph.rslot[b];
 #pragma unroll
       for (int i = 0; i < NR; ++i) {
         uint32_t sidx = ts;
@@ -247,12 +244,14 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
     for (int o = ph.op_begin; o < ph.op_end; ++o) apply_op<Real, R>(a, P.ops[o], tid, base);
 
     if (p + 1 == nph && P.direct_store) {
-      uint64_t tphys = base;
-#pragma unroll
-      for (int b = 0; b < T; ++b) tphys |= uint64_t((tid >> b) & 1u) << P.tile_phys[ph.wthr_pos[b]];
+      // A one-phase pass that also loaded straight from HBM: every warp of the
+      // CTA must have read its amplitudes before any warp overwrites the tile
+      // in its relabelled order.
+      if (p == 0 && P.direct_load) __syncthreads();
+      const uint64_t tphys = base | P.store.tphys_lo[tid & 15] | P.store.tphys_hi[tid >> 4];
       uint64_t rphys[R];
 #pragma unroll
-      for (int b = 0; b < R; ++b) rphys[b] = 1ull << P.tile_phys[ph.wreg_pos[b]];
+      for (int b = 0; b < R; ++b) rphys[b] = P.store.rphys[b];
 #pragma unroll
       for (int i = 0; i < NR; i += VEC) {
         uint64_t phys = tphys;
@@ -262,13 +261,10 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
       }
     } else {
       __syncthreads();  // every thread has read this phase's layout
-      uint32_t woff = 0;
-#pragma unroll
-      for (int b = 0; b < T; ++b) woff |= ((tid >> b) & 1u) << ph.wthr_pos[b];
-      const uint32_t ts = smem_slot<VB>(woff);
+      const uint32_t ts = ph.wtslot_lo[tid & 15] ^ ph.wtslot_hi[tid >> 4];
       uint32_t rs[R];
 #pragma unroll
-      for (int b = 0; b < R; ++b) rs[b] = smem_slot<VB>(1u << ph.wreg_pos[b]);
+      for (int b = 0; b < R; ++b) rs[b] = ph.wslot[b];
 #pragma unroll
       for (int i = 0; i < NR; ++i) {
         uint32_t sidx = ts;
@@ -283,32 +279,44 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
   if (!P.direct_store) staged_copy(false);
 }
 
-template <typename Real>
-size_t tile_pass_smem_bytes() { return sizeof(typename ctype<Real>::c) << tiling<Real>::K; }
+namespace {
 
-template <typename Real>
-cudaError_t launch_tile_pass(void* state, int n, const dev_pass& pass, cudaStream_t stream)
+template <typename Real, int SHAPE>
+cudaError_t launch_shape(void* state, int n, const dev_pass& pass, cudaStream_t stream)
 {
-  const size_t smem = tile_pass_smem_bytes<Real>();
+  using SH = tile_shape<Real, SHAPE>;
+  const size_t smem = sizeof(typename ctype<Real>::c) << SH::K;
   static bool configured[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   if (!configured[dev]) {
-    e = cudaFuncSetAttribute(tile_pass_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(tile_pass_kernel<Real, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  const uint64_t blocks = 1ull << (n - tiling<Real>::K);
-  tile_pass_kernel<Real><<<(unsigned)blocks, 1 << tiling<Real>::T, smem, stream>>>(
+  if (n < SH::K) return cudaErrorInvalidValue;
+  const uint64_t blocks = 1ull << (n - SH::K);
+  tile_pass_kernel<Real, SHAPE><<<(unsigned)blocks, 1 << (SH::K - SH::R), smem, stream>>>(
     static_cast<typename ctype<Real>::c*>(state), pass);
   return cudaGetLastError();
 }
 
-template size_t tile_pass_smem_bytes<double>();
-template size_t tile_pass_smem_bytes<float>();
-template cudaError_t launch_tile_pass<double>(void*, int, const dev_pass&, cudaStream_t);
-template cudaError_t launch_tile_pass<float>(void*, int, const dev_pass&, cudaStream_t);
+}  // namespace
+
+template <typename Real>
+cudaError_t launch_tile_pass(void* state, int n, const dev_pass& pass, int shape, cudaStream_t stream)
+{
+  switch (shape) {
+    case 0: return launch_shape<Real, 0>(state, n, pass, stream);
+    case 1: return launch_shape<Real, 1>(state, n, pass, stream);
+    case 2: return launch_shape<Real, 2>(state, n, pass, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template cudaError_t launch_tile_pass<double>(void*, int, const dev_pass&, int, cudaStream_t);
+template cudaError_t launch_tile_pass<float>(void*, int, const dev_pass&, int, cudaStream_t);
 
 }  // namespace rbk

@@ -54,6 +54,7 @@ _SIGNATURES = {
     "rbk_flush": ([_P], _I),
     "rbk_state_set_deferred": ([_P, _I], _I),
     "rbk_state_set_pass_budget": ([_P, _I], _I),
+    "rbk_state_set_tile_shape": ([_P, _I], _I),
     "rbk_state_get_stats": ([_P, ctypes.POINTER(Stats)], _I),
     "rbk_state_reset_stats": ([_P], _I),
     "rbk_state_device_ms": ([_P, ctypes.POINTER(_D)], _I),
@@ -166,6 +167,9 @@ class State:
 
     def set_pass_budget(self, budget):
         _check(lib().rbk_state_set_pass_budget(self.h, budget))
+
+    def set_tile_shape(self, shape):
+        _check(lib().rbk_state_set_tile_shape(self.h, shape))
 
     def stats(self):
         s = Stats()

@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <random>
+#include <set>
 #include <vector>
 
 #include "rbk_internal.h"
@@ -43,32 +44,56 @@ static void apply_direct(std::vector<cplx>& a, const hgate& g)
   }
 }
 
-// Model of tile_pass_kernel for one pass.
+static uint32_t slot_of(uint32_t j, int vbits)
+{
+  uint32_t u = j >> vbits;
+  const uint32_t f = (u >> 3) ^ (u >> 6) ^ (u >> 9) ^ (u >> 12);
+  u ^= f & 7u;
+  return (u << vbits) | (j & ((1u << vbits) - 1));
+}
+
+// Model of tile_pass_kernel for one pass: shared memory is indexed by slot and
+// every address comes from the precomputed tables, as in the kernel.  Each
+// phase completes all threads' reads before any write, which is what the
+// kernel's barriers guarantee (including the one before the direct store of a
+// one-phase pass that also loaded straight from HBM).
 static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass& P)
 {
   const int K = p.K, R = p.R, T = K - R, NR = 1 << R, NT = 1 << T;
   const uint64_t blocks = 1ull << (p.n - K);
-  std::vector<cplx> tile(1u << K), next(1u << K);
+  std::vector<cplx> smem(1u << K);
   std::vector<cplx> regs(size_t(NT) * NR);
   for (uint64_t b = 0; b < blocks; ++b) {
     uint64_t base = 0;
-    for (int k = 0; k < P.num_nontile; ++k) base |= ((b >> k) & 1ull) << P.nontile_phys[k];
+    for (int r = 0; r < P.num_runs; ++r)
+      base |= ((b >> P.run_src[r]) & ((1ull << P.run_len[r]) - 1)) << P.run_dst[r];
     auto phys_of = [&](uint32_t j) {
       uint64_t ph = base;
       for (int t = 0; t < K; ++t) if ((j >> t) & 1) ph |= 1ull << P.tile_phys[t];
       return ph;
     };
-    for (uint32_t j = 0; j < (1u << K); ++j) tile[j] = st[phys_of(j)];
+    std::set<uint64_t> touched, stored;  // direct HBM accesses of this tile
+    if (!P.direct_load)
+      for (uint32_t j = 0; j < (1u << K); ++j) smem[slot_of(j, p.vbits)] = st[phys_of(j)];
     for (int ph = 0; ph < P.num_phases; ++ph) {
       const dev_phase& D = P.phases[ph];
       for (int tid = 0; tid < NT; ++tid) {
-        uint32_t toff = 0;
-        for (int x = 0; x < T; ++x) toff |= ((tid >> x) & 1u) << D.thr_pos[x];
         cplx* a = &regs[size_t(tid) * NR];
-        for (int i = 0; i < NR; ++i) {
-          uint32_t j = toff;
-          for (int x = 0; x < R; ++x) if (i & (1 << x)) j |= 1u << D.reg_pos[x];
-          a[i] = tile[j];
+        if (ph == 0 && P.direct_load) {
+          const uint64_t tp = base | P.load.tphys_lo[tid & 15] | P.load.tphys_hi[tid >> 4];
+          for (int i = 0; i < NR; ++i) {
+            uint64_t phys = tp;
+            for (int x = 0; x < R; ++x) if (i & (1 << x)) phys |= P.load.rphys[x];
+            if (!touched.insert(phys).second) { std::fprintf(stderr, "direct load reads an amplitude twice\n"); std::exit(4); }
+            a[i] = st[phys];
+          }
+        } else {
+          const uint32_t ts = D.tslot_lo[tid & 15] ^ D.tslot_hi[tid >> 4];
+          for (int i = 0; i < NR; ++i) {
+            uint32_t sidx = ts;
+            for (int x = 0; x < R; ++x) if (i & (1 << x)) sidx ^= D.rslot[x];
+            a[i] = smem[sidx];
+          }
         }
         for (int o = D.op_begin; o < D.op_end; ++o) {
           const dev_op& op = P.ops[o];
@@ -91,21 +116,37 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
           }
         }
       }
+      const bool last = ph + 1 == P.num_phases;
       std::vector<char> written(1u << K, 0);
       for (int tid = 0; tid < NT; ++tid) {
-        uint32_t woff = 0;
-        for (int x = 0; x < T; ++x) woff |= ((tid >> x) & 1u) << D.wthr_pos[x];
+        const cplx* a = &regs[size_t(tid) * NR];
+        if (last && P.direct_store) {
+          const uint64_t tp = base | P.store.tphys_lo[tid & 15] | P.store.tphys_hi[tid >> 4];
+          for (int i = 0; i < NR; ++i) {
+            uint64_t phys = tp;
+            for (int x = 0; x < R; ++x) if (i & (1 << x)) phys |= P.store.rphys[x];
+            if (!stored.insert(phys).second) { std::fprintf(stderr, "direct store writes an amplitude twice\n"); std::exit(5); }
+            st[phys] = a[i];
+          }
+          continue;
+        }
+        const uint32_t ts = D.wtslot_lo[tid & 15] ^ D.wtslot_hi[tid >> 4];
         for (int i = 0; i < NR; ++i) {
-          uint32_t j = woff;
-          for (int x = 0; x < R; ++x) if (i & (1 << x)) j |= 1u << D.wreg_pos[x];
-          if (j >= (1u << K) || written[j]) { std::fprintf(stderr, "bad write position\n"); std::exit(3); }
-          written[j] = 1;
-          next[j] = regs[size_t(tid) * NR + i];
+          uint32_t sidx = ts;
+          for (int x = 0; x < R; ++x) if (i & (1 << x)) sidx ^= D.wslot[x];
+          if (sidx >= (1u << K) || written[sidx]) { std::fprintf(stderr, "bad write position\n"); std::exit(3); }
+          written[sidx] = 1;
+          smem[sidx] = a[i];
         }
       }
-      tile.swap(next);
     }
-    for (uint32_t j = 0; j < (1u << K); ++j) st[phys_of(j)] = tile[j];
+    if (!P.direct_store)
+      for (uint32_t j = 0; j < (1u << K); ++j) st[phys_of(j)] = smem[slot_of(j, p.vbits)];
+    if ((P.direct_load && touched.size() != (1u << K)) || (P.direct_store && stored.size() != (1u << K))) {
+      std::fprintf(stderr, "direct HBM access does not cover the tile\n");
+      std::exit(6);
+    }
+    for (uint64_t ph : stored) if ((ph & ~((1ull << p.n) - 1)) != 0) { std::fprintf(stderr, "store out of range\n"); std::exit(7); }
   }
 }
 
@@ -140,12 +181,14 @@ int main(int argc, char** argv)
 {
   const int seeds = argc > 1 ? std::atoi(argv[1]) : 20;
   int failures = 0;
-  for (int prec = 0; prec < 2; ++prec) {
+  for (int prec = 0; prec < 2; ++prec)
+  for (int shape = 0; shape < kNumShapes; ++shape) {
     plan_params p{};
-    if (prec == 0) { p.K = 12; p.R = 4; p.LOW = 5; p.vbits = 0; }
-    else { p.K = 13; p.R = 5; p.LOW = 6; p.vbits = 1; }
+    shape_bits(prec, shape, &p.K, &p.R);
+    p.LOW = prec == 0 ? 5 : 6;
+    p.vbits = prec;
     for (int seed = 0; seed < seeds; ++seed) {
-      std::mt19937_64 rng(1000 * prec + seed);
+      std::mt19937_64 rng(1000 * prec + 100 * shape + seed);
       p.n = p.K + static_cast<int>(rng() % 4);
       p.dense_budget = 1 + static_cast<int>(rng() % 16);
       const uint64_t N = 1ull << p.n;
@@ -171,7 +214,7 @@ int main(int argc, char** argv)
       for (int i = 0; i < p.n; ++i) if (perm[i] != i) { std::printf("layout not canonical\n"); ++failures; break; }
       double err = 0;
       for (uint64_t i = 0; i < N; ++i) err = std::max(err, std::abs(st[i] - want[i]));
-      std::printf("prec=%d seed=%d n=%d gates=%d budget=%d passes=%zu canon=%zu err=%.3e\n", prec, seed, p.n, count,
+      std::printf("prec=%d shape=%d seed=%d n=%d gates=%d budget=%d passes=%zu canon=%zu err=%.3e\n", prec, shape, seed, p.n, count,
                   p.dense_budget, passes.size(), canon.size(), err);
       if (!(err < 1e-9)) ++failures;
     }

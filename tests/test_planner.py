@@ -18,6 +18,6 @@ def test_planner_programs_are_exact(tmp_path):
     subprocess.run(["g++", "-std=c++17", "-O2", "-I", csrc, "-o", str(exe),
                     os.path.join(ROOT, "tests", "host", "plan_check.cpp"), os.path.join(csrc, "rbk_plan.cpp")],
                    check=True, env={**os.environ, "CXX": "g++"})
-    r = subprocess.run([str(exe), "12"], capture_output=True, text=True, timeout=300)
+    r = subprocess.run([str(exe), "6"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr
     assert "ALL OK" in r.stdout
