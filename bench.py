@@ -211,6 +211,10 @@ def run_gpu(args):
     bytes_pass = 2 * (1 << N_QUBITS) * 16
 
     s = pkg.State(N_QUBITS, pkg.C128, device=local)
+    if args.shape is not None:
+        s.set_tile_shape(args.shape)
+    if args.budget is not None:
+        s.set_pass_budget(args.budget)
     for _ in range(args.warmup):
         s.apply(ops)
         s.synchronize()
@@ -340,6 +344,8 @@ def main():
     ap.add_argument("--ref-blocks-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=N_QUBITS, help="smaller cases for profiling only")
     ap.add_argument("--depth", type=int, default=DEPTH)
+    ap.add_argument("--shape", type=int, default=None, help="tile shape (rbk_state_set_tile_shape)")
+    ap.add_argument("--budget", type=int, default=None, help="dense gates per pass (rbk_state_set_pass_budget)")
     args = ap.parse_args()
     globals()["N_QUBITS"], globals()["DEPTH"] = args.qubits, args.depth
     if args.impl == "reference":
