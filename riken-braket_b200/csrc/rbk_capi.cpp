@@ -862,6 +862,9 @@ int rbk_expectation_pauli(rbk_state* s, int num_terms, const char* strings, cons
     if (int rc = check_state(s)) return rc;
     if (num_terms < 0 || (num_terms > 0 && (!strings || !coeffs)) || !out)
       return fail(RBK_ERR_INVALID, "bad Pauli term arguments");
+    // The queued gates may move qubits (SWAPs, relabelling): map logical
+    // qubits to physical bits only after they have run.
+    if (int rc = flush(s)) return rc;
     struct term { uint64_t flip, sign; cplx w; };
     std::vector<term> terms;
     for (int t = 0; t < num_terms; ++t) {
@@ -911,6 +914,8 @@ int rbk_inner_product(rbk_state* a, rbk_state* b, double* out)
     if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
     if (a->n != b->n || a->precision != b->precision) return fail(RBK_ERR_INVALID, "states differ in size or precision");
     if (a->device != b->device) return fail(RBK_ERR_UNSUPPORTED, "states live on different devices");
+    if (int rc = flush(a)) return rc;  // layouts are final only after the queued gates ran
+    if (int rc = flush(b)) return rc;
     if (a->perm != b->perm) {
       if (int rc = canonicalize(a)) return rc;
       if (int rc = canonicalize(b)) return rc;

@@ -243,3 +243,22 @@ def test_errors_are_status_codes(pkg):
     s.end_fusion()
     s.hadamard(0)
     assert abs(s.norm2() - 1.0) < 1e-14
+
+
+def test_observables_right_after_queued_swaps(pkg):
+    """Reads issued straight after gates that move qubits (SWAPs, relabelling)
+    see the layout those gates leave behind."""
+    n = 16
+    ops = pkg.circuits.random_circuit(n, 200, seed=5)
+    terms = pkg.circuits.ansatz_hamiltonian(n) + [("XYZ" + "I" * (n - 3), 0.3 + 0.1j)]
+    o = oracle.COracle(n)
+    o.apply(ops)
+    s = pkg.State(n)
+    s.apply(ops)
+    assert abs(s.expectation(terms) - o.expectation(terms)) <= TOL64
+    a, b = pkg.State(n), pkg.State(n)
+    a.apply(ops)
+    b.apply(ops[:120])
+    ob = oracle.COracle(n)
+    ob.apply(ops[:120])
+    assert abs(a.inner_product(b) - o.inner_product(ob)) <= TOL64
