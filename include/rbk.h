@@ -175,6 +175,23 @@ int rbk_inner_product(rbk_state* a, rbk_state* b, double* out);
 /* ket::fidelity: |<b|a>|^2 (fidelity.hpp) */
 int rbk_fidelity(rbk_state* a, rbk_state* b, double* out);
 
+/* Pauli-string expectation value of a caller-owned device state, with no
+ * device memory allocated.  No counterpart in the reference: it exists for
+ * callers that cannot allocate when they need the value -- code in a CUDA
+ * host callback, a process whose HBM another allocator has already reserved,
+ * or a loop that must not take the device synchronisation of cudaMalloc /
+ * cudaFree.  Same meaning and arguments as rbk_expectation_pauli, except:
+ * device_amps points to 2^num_qubits amplitudes of the given precision in
+ * logical order (e.g. rbk_state_canonicalize + rbk_state_device_pointer);
+ * stream is a cudaStream_t (NULL: the default stream); out is a host pointer
+ * to (re, im).  Its scratch is one fixed device array of about 10 KB, held by
+ * every GPU that loads the library until exit and shared by all calls: calls
+ * that overlap on the GPU race.  At most 64 groups of strings with distinct
+ * X/Y positions (RBK_ERR_INVALID beyond).  The first call on a device looks up
+ * the array's device address; make that first call before any stream capture. */
+int rbk_expectation_pauli_noalloc(const void* device_amps, int num_qubits, int precision, int num_terms,
+                                  const char* strings, const double* coeffs, double* out, void* stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -356,6 +356,8 @@ int pauli_group(rbk_state* s, uint64_t flip, const rbk::pauli_terms& t, double* 
 
 }  // namespace
 
+int rbk::set_last_error(int code, const char* msg) { return fail(code, msg); }
+
 extern "C" {
 
 const char* rbk_last_error(void) { return g_error.c_str(); }

@@ -26,6 +26,9 @@ template <typename Real> cudaError_t launch_gate(void* state, int n, const gate_
 template <typename Real> cudaError_t launch_set_basis(void* state, int n, uint64_t index, cudaStream_t stream);
 
 int reduction_blocks();
+
+// Records msg as the calling thread's rbk_last_error() and returns code.
+int set_last_error(int code, const char* msg);
 // Scratch needed by the reductions below, in doubles.
 inline size_t reduction_scratch_doubles() { return size_t(1 << 12) * (1 + kMaxQubits) + 64; }
 
