@@ -61,7 +61,7 @@ struct alignas(8) dev_op {
   uint8_t kind;
   uint8_t treg;       // MAT/X/Y: target register bit
   uint8_t diag_one;   // DIAG: d0 == 1 exactly (phase-shift form: only the one-half is touched)
-  uint8_t real;       // MAT: all four entries are real (H, exp(i theta Y), ...)
+  uint8_t real;       // MAT: 1 = all four entries real (H, exp(i theta Y)); 2 = m00 real (U3, U2)
   uint32_t creg;      // controls inside the register bits
   uint32_t cthr;      // controls inside the thread bits
   uint32_t dreg;      // DIAG target bit among the register bits (mask), 0 if elsewhere

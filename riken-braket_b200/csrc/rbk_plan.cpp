@@ -334,7 +334,10 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
       d.kind = o.kind;
       d.diag_one = o.diag_one;
       std::memcpy(d.m, o.m, sizeof(d.m));
-      d.real = (o.kind == OPK_MAT && o.m[1] == 0.0 && o.m[3] == 0.0 && o.m[5] == 0.0 && o.m[7] == 0.0) ? 1 : 0;
+      // 1: all four entries real; 2: m00 real (U3, U2); 0: general.
+      if (o.kind == OPK_MAT && o.m[1] == 0.0 && o.m[3] == 0.0 && o.m[5] == 0.0 && o.m[7] == 0.0) d.real = 1;
+      else if (o.kind == OPK_MAT && o.m[1] == 0.0) d.real = 2;
+      else d.real = 0;
       auto classify = [&](uint64_t phys_mask, uint32_t& reg, uint32_t& thrm, uint64_t& outm) {
         while (phys_mask) {
           const int q = __builtin_ctzll(phys_mask);

@@ -42,6 +42,21 @@ __device__ __forceinline__ void apply_mat(typename ctype<Real>::c* a, uint32_t c
   }
 }
 
+// Complex 2x2 whose m00 is real (U3: cos(theta/2); U2: 1/sqrt 2): 14 multiply-adds per pair instead of 16.
+template <typename Real, int B, int NR, bool CTRL>
+__device__ __forceinline__ void apply_mat_r00(typename ctype<Real>::c* a, uint32_t creg, const mat2<Real>& M)
+{
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    if (i & (1 << B)) continue;
+    if (CTRL && (uint32_t(i) & creg) != creg) continue;
+    const auto a0 = a[i], a1 = a[i | (1 << B)];
+    a[i].x = M.m00r * a0.x + M.m01r * a1.x - M.m01i * a1.y;
+    a[i].y = M.m00r * a0.y + M.m01r * a1.y + M.m01i * a1.x;
+    a[i | (1 << B)] = cmac2(a0, a1, M.m10r, M.m10i, M.m11r, M.m11i);
+  }
+}
+
 // Real 2x2 (H, exp(i theta Y), ...): half the multiply-adds.
 template <typename Real, int B, int NR, bool CTRL>
 __device__ __forceinline__ void apply_real(typename ctype<Real>::c* a, uint32_t creg, Real m00, Real m01, Real m10, Real m11)
@@ -106,10 +121,15 @@ __device__ __forceinline__ void apply_op(typename ctype<Real>::c* a, const dev_o
   const uint32_t creg = op.creg;
   switch (op.kind) {
     case OPK_MAT:
-      if (op.real) {
+      if (op.real == 1) {
         const Real m00 = (Real)op.m[0], m01 = (Real)op.m[2], m10 = (Real)op.m[4], m11 = (Real)op.m[6];
         if (creg == 0) { RBK_DISPATCH_BIT(op.treg, (apply_real<Real, BB, NR, false>(a, 0u, m00, m01, m10, m11))); }
         else { RBK_DISPATCH_BIT(op.treg, (apply_real<Real, BB, NR, true>(a, creg, m00, m01, m10, m11))); }
+      } else if (op.real == 2) {
+        const mat2<Real> M{(Real)op.m[0], (Real)0, (Real)op.m[2], (Real)op.m[3],
+                           (Real)op.m[4], (Real)op.m[5], (Real)op.m[6], (Real)op.m[7]};
+        if (creg == 0) { RBK_DISPATCH_BIT(op.treg, (apply_mat_r00<Real, BB, NR, false>(a, 0u, M))); }
+        else { RBK_DISPATCH_BIT(op.treg, (apply_mat_r00<Real, BB, NR, true>(a, creg, M))); }
       } else {
         const mat2<Real> M{(Real)op.m[0], (Real)op.m[1], (Real)op.m[2], (Real)op.m[3],
                            (Real)op.m[4], (Real)op.m[5], (Real)op.m[6], (Real)op.m[7]};
