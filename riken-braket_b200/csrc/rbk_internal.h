@@ -56,6 +56,22 @@ enum op_kind : uint8_t {
   OPK_NEG = 5,   // amplitude *= -1 when the controls are all one (Z, CZ: exact)
 };
 
+// Dispatch key of a pass op: MAT ops are keyed by matrix form (0 general,
+// 1 real, 2 real m00), by whether register-bit controls exist and by the target
+// register bit; X and Y by the target bit; NEG and DIAG by kind alone.
+#ifdef __CUDACC__
+#define RBK_HOST_DEVICE __host__ __device__
+#else
+#define RBK_HOST_DEVICE
+#endif
+RBK_HOST_DEVICE constexpr uint32_t op_code(int kind, int form, bool controlled, int treg)
+{
+  return kind == OPK_MAT ? uint32_t((form * 2 + (controlled ? 1 : 0)) * 8 + treg)
+       : kind == OPK_X ? 48u + uint32_t(treg)
+       : kind == OPK_Y ? 56u + uint32_t(treg)
+       : kind == OPK_NEG ? 64u : 65u;
+}
+
 // One gate inside a pass, in the coordinates of the phase it belongs to.
 struct alignas(8) dev_op {
   uint8_t kind;
@@ -66,7 +82,7 @@ struct alignas(8) dev_op {
   uint32_t cthr;      // controls inside the thread bits
   uint32_t dreg;      // DIAG target bit among the register bits (mask), 0 if elsewhere
   uint32_t dthr;      // DIAG target bit among the thread bits (mask)
-  uint32_t pad1;
+  uint32_t code;      // op_code(kind, form, controlled, treg): the kernel's single dispatch key
   uint64_t cout;      // controls on physical bits outside the tile
   uint64_t dout;      // DIAG target on a physical bit outside the tile (mask)
   double m[8];        // MAT: m00 m01 m10 m11 as (re, im); DIAG: d0 d1

@@ -357,6 +357,12 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
         classify(bit(o.target), d.dreg, d.dthr, d.dout);
       }
     }
+    for (int k = dp.op_begin; k < op_index; ++k) {
+      dev_op& d = out.ops[k];
+      d.code = d.kind == OPK_MAT ? op_code(OPK_MAT, d.real, d.creg != 0, d.treg)
+             : (d.kind == OPK_X || d.kind == OPK_Y) ? op_code(d.kind, 0, true, d.treg)
+             : op_code(d.kind, 0, true, 0);
+    }
     dp.op_end = static_cast<uint16_t>(op_index);
   }
   out.num_phases = static_cast<uint8_t>(phases.size());

@@ -112,6 +112,8 @@ __device__ __forceinline__ void apply_y(typename ctype<Real>::c* a, uint32_t cre
     default: break;                                                     \
   }
 
+// One jump per op: the host encodes (kind, matrix form, controls, target bit)
+// into op.code (see op_code in rbk_internal.h).
 template <typename Real, int R>
 __device__ __forceinline__ void apply_op(typename ctype<Real>::c* a, const dev_op& op, uint32_t tid, uint64_t base)
 {
@@ -119,32 +121,40 @@ __device__ __forceinline__ void apply_op(typename ctype<Real>::c* a, const dev_o
   constexpr int NR = 1 << R;
   if ((tid & op.cthr) != op.cthr || (base & op.cout) != op.cout) return;
   const uint32_t creg = op.creg;
-  switch (op.kind) {
-    case OPK_MAT:
-      if (op.real == 1) {
-        const Real m00 = (Real)op.m[0], m01 = (Real)op.m[2], m10 = (Real)op.m[4], m11 = (Real)op.m[6];
-        if (creg == 0) { RBK_DISPATCH_BIT(op.treg, (apply_real<Real, BB, NR, false>(a, 0u, m00, m01, m10, m11))); }
-        else { RBK_DISPATCH_BIT(op.treg, (apply_real<Real, BB, NR, true>(a, creg, m00, m01, m10, m11))); }
-      } else if (op.real == 2) {
-        const mat2<Real> M{(Real)op.m[0], (Real)0, (Real)op.m[2], (Real)op.m[3],
-                           (Real)op.m[4], (Real)op.m[5], (Real)op.m[6], (Real)op.m[7]};
-        if (creg == 0) { RBK_DISPATCH_BIT(op.treg, (apply_mat_r00<Real, BB, NR, false>(a, 0u, M))); }
-        else { RBK_DISPATCH_BIT(op.treg, (apply_mat_r00<Real, BB, NR, true>(a, creg, M))); }
-      } else {
-        const mat2<Real> M{(Real)op.m[0], (Real)op.m[1], (Real)op.m[2], (Real)op.m[3],
-                           (Real)op.m[4], (Real)op.m[5], (Real)op.m[6], (Real)op.m[7]};
-        if (creg == 0) { RBK_DISPATCH_BIT(op.treg, (apply_mat<Real, BB, NR, false>(a, 0u, M))); }
-        else { RBK_DISPATCH_BIT(op.treg, (apply_mat<Real, BB, NR, true>(a, creg, M))); }
-      }
-      break;
-    case OPK_X: RBK_DISPATCH_BIT(op.treg, (apply_x<Real, BB, NR>(a, creg))); break;
-    case OPK_Y: RBK_DISPATCH_BIT(op.treg, (apply_y<Real, BB, NR>(a, creg))); break;
-    case OPK_NEG:
+#define RBK_MAT_CASES(FORM, CTRL, B)                                                                    \
+  case op_code(OPK_MAT, FORM, CTRL, B):                                                                 \
+    if constexpr (B < R) {                                                                              \
+      if constexpr (FORM == 1) {                                                                        \
+        apply_real<Real, B, NR, CTRL>(a, creg, (Real)op.m[0], (Real)op.m[2], (Real)op.m[4], (Real)op.m[6]); \
+      } else {                                                                                          \
+        const mat2<Real> M{(Real)op.m[0], FORM == 2 ? (Real)0 : (Real)op.m[1], (Real)op.m[2], (Real)op.m[3], \
+                           (Real)op.m[4], (Real)op.m[5], (Real)op.m[6], (Real)op.m[7]};                \
+        if constexpr (FORM == 2) apply_mat_r00<Real, B, NR, CTRL>(a, creg, M);                          \
+        else apply_mat<Real, B, NR, CTRL>(a, creg, M);                                                  \
+      }                                                                                                 \
+    }                                                                                                   \
+    break;
+#define RBK_MAT_BITS(FORM, CTRL) \
+  RBK_MAT_CASES(FORM, CTRL, 0) RBK_MAT_CASES(FORM, CTRL, 1) RBK_MAT_CASES(FORM, CTRL, 2) \
+  RBK_MAT_CASES(FORM, CTRL, 3) RBK_MAT_CASES(FORM, CTRL, 4)
+#define RBK_PERM_CASES(KIND, FN) \
+  case op_code(KIND, 0, true, 0): FN<Real, 0, NR>(a, creg); break; \
+  case op_code(KIND, 0, true, 1): FN<Real, 1, NR>(a, creg); break; \
+  case op_code(KIND, 0, true, 2): FN<Real, 2, NR>(a, creg); break; \
+  case op_code(KIND, 0, true, 3): FN<Real, 3, NR>(a, creg); break; \
+  case op_code(KIND, 0, true, 4): if constexpr (R > 4) { FN<Real, (R > 4 ? 4 : 0), NR>(a, creg); } break;
+  switch (op.code) {
+    RBK_MAT_BITS(0, false) RBK_MAT_BITS(0, true)
+    RBK_MAT_BITS(1, false) RBK_MAT_BITS(1, true)
+    RBK_MAT_BITS(2, false) RBK_MAT_BITS(2, true)
+    RBK_PERM_CASES(OPK_X, apply_x)
+    RBK_PERM_CASES(OPK_Y, apply_y)
+    case op_code(OPK_NEG, 0, true, 0):
 #pragma unroll
       for (int i = 0; i < NR; ++i)
         if ((uint32_t(i) & creg) == creg) { a[i].x = -a[i].x; a[i].y = -a[i].y; }
       break;
-    case OPK_DIAG: {
+    case op_code(OPK_DIAG, 0, true, 0): {
       const bool tb = ((tid & op.dthr) != 0) || ((base & op.dout) != 0);
       const C d0{(Real)op.m[0], (Real)op.m[1]}, d1{(Real)op.m[2], (Real)op.m[3]};
       const uint32_t dreg = op.dreg;
@@ -160,6 +170,9 @@ __device__ __forceinline__ void apply_op(typename ctype<Real>::c* a, const dev_o
     }
     default: break;
   }
+#undef RBK_PERM_CASES
+#undef RBK_MAT_BITS
+#undef RBK_MAT_CASES
 }
 
 }  // namespace
