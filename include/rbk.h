@@ -175,6 +175,39 @@ int rbk_inner_product(rbk_state* a, rbk_state* b, double* out);
 /* ket::fidelity: |<b|a>|^2 (fidelity.hpp) */
 int rbk_fidelity(rbk_state* a, rbk_state* b, double* out);
 
+/* ---- adjoint gradient (no counterpart in the reference) --------------------
+ * One gate of a parametrised circuit, in bra's terms.  qubits[0] is the target
+ * (CNOT: qubits[0] = control, qubits[1] = target, as in "CNOT c t"; CZ, SWAP and
+ * "U c1 c2 k" use both).  EX/EY/EZ apply exp(i phi P) with
+ * phi = scale * theta[param] + angles[0] (param = -1: a fixed angle); U1 takes
+ * angles[0]; U2 angles[0..1]; U3 angles[0..2]; U takes k in angles[0]. */
+typedef struct rbk_circuit_gate {
+  int32_t kind;
+  int32_t qubits[2];
+  int32_t param;
+  double scale;
+  double angles[3];
+} rbk_circuit_gate;
+
+enum {
+  RBK_GATE_H = 1, RBK_GATE_X = 2, RBK_GATE_Y = 3, RBK_GATE_Z = 4, RBK_GATE_U1 = 5, RBK_GATE_U2 = 6,
+  RBK_GATE_U3 = 7, RBK_GATE_CNOT = 8, RBK_GATE_CZ = 9, RBK_GATE_U = 10, RBK_GATE_EX = 11, RBK_GATE_EY = 12,
+  RBK_GATE_EZ = 13, RBK_GATE_SWAP = 14
+};
+
+/* Energy E = <psi|H|psi> of psi = U(theta)|0...0> and dE/dtheta for every
+ * parameter, from one forward pass and one reverse sweep that un-applies each
+ * gate on psi and on lambda = H psi (exact gate inverses; no stored
+ * intermediate states).  Only EX/EY/EZ gates take parameters (RY(t) = EY with
+ * scale -1/2).  H is given like rbk_expectation_pauli (strings over all
+ * num_qubits qubits, complex coeffs); at most 128 strings in 64 X/Y patterns.
+ * The reference has no differentiation support; the tests check these
+ * gradients against the parameter-shift rule evaluated with the reference
+ * ket code and against central finite differences. */
+int rbk_adjoint_gradient(int num_qubits, int precision, int device, const rbk_circuit_gate* gates, int num_gates,
+                         const double* theta, int num_params, int num_terms, const char* strings,
+                         const double* coeffs, double* energy, double* grad);
+
 /* Pauli-string expectation value of a caller-owned device state, with no
  * device memory allocated.  No counterpart in the reference: it exists for
  * callers that cannot allocate when they need the value -- code in a CUDA

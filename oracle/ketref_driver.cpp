@@ -17,7 +17,7 @@
 //   CZ     -> ket::gate::ranges::pauli_z on two controls
 //   U c1 c2 k -> ket::gate::ranges::phase_shift_coeff with the bra phase table
 //             (bra/src/state.cpp:148 generate_phase_coefficients; :2650-2669)
-//   EY/EZ  -> ket::gate::ranges::exponential_pauli_{y,z}
+//   EX/EY/EZ -> ket::gate::ranges::exponential_pauli_{x,y,z}
 //   BEGIN/END FUSION -> bra::fused_gate objects replayed per fused index by
 //             ket::gate::runtime::ranges::gate (bra/src/nompi_state.cpp:1285-1357,
 //             found-qubit bookkeeping of bra/include/bra/state.hpp:126-173)
@@ -75,6 +75,7 @@
 #include <bra/fused_gate/fused_controlled_not.hpp>
 #include <bra/fused_gate/fused_controlled_pauli_z.hpp>
 #include <bra/fused_gate/fused_controlled_phase_shift.hpp>
+#include <bra/fused_gate/fused_exponential_pauli_x.hpp>
 #include <bra/fused_gate/fused_exponential_pauli_y.hpp>
 #include <bra/fused_gate/fused_exponential_pauli_z.hpp>
 #include <bra/fused_gate/fused_swap.hpp>
@@ -254,6 +255,10 @@ void apply_one(ref_state& s, oracle_op const& op)
     else ket::gate::ranges::phase_shift_coeff(s.policy, s.data, coeff, cq(q0), cq(q1));
     break;
    }
+   case ORC_EX:
+    if (f) { mark(s, q0, found::target); push_fused<bra::fused_gate::fused_exponential_pauli_x>(s, op.p[0], qb(q0)); }
+    else ket::gate::ranges::exponential_pauli_x(s.policy, s.data, op.p[0], qb(q0));
+    break;
    case ORC_EY:
     if (f) { mark(s, q0, found::target); push_fused<bra::fused_gate::fused_exponential_pauli_y>(s, op.p[0], qb(q0)); }
     else ket::gate::ranges::exponential_pauli_y(s.policy, s.data, op.p[0], qb(q0));

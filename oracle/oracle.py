@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 ORC = {
     "H": 1, "X": 2, "Y": 3, "Z": 4, "U1": 5, "U2": 6, "U3": 7, "CNOT": 8, "CZ": 9,
-    "U": 10, "EY": 11, "EZ": 12, "SWAP": 13, "BEGIN FUSION": 14, "END FUSION": 15,
+    "U": 10, "EY": 11, "EZ": 12, "SWAP": 13, "BEGIN FUSION": 14, "END FUSION": 15, "EX": 16,
 }
 
 

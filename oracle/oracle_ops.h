@@ -25,7 +25,8 @@ enum oracle_code {
   ORC_EZ = 12,          /* EZ t theta                exp(i theta Z)                 */
   ORC_SWAP = 13,        /* SWAP t1 t2                                               */
   ORC_BEGIN_FUSION = 14,
-  ORC_END_FUSION = 15
+  ORC_END_FUSION = 15,
+  ORC_EX = 16           /* EX t theta                exp(i theta X), p[0]=theta     */
 };
 
 typedef struct oracle_op {

@@ -205,6 +205,25 @@ static void gate_ey(orc_state* s, int q, double theta)
   }
 }
 
+/* EX: exponential_pauli_x.hpp (coeff form): a0 = a0 cos + a1 (i sin), a1 = a1 cos + a0 (i sin) */
+static void gate_ex(orc_state* s, int q, double theta)
+{
+  cplx coeff = exp_i(theta);
+  double cs = coeff.re;
+  cplx isn = { 0.0 * coeff.im, 1.0 * coeff.im };
+  uint64_t half = s->size >> 1, m = UINT64_C(1) << q;
+  #pragma omp parallel for schedule(static)
+  for (uint64_t v = 0; v < half; ++v) {
+    uint64_t i0 = insert0(v, q), i1 = i0 | m;
+    cplx a0 = s->a[i0], a1 = s->a[i1];
+    cplx z = c_scale(a0, cs);
+    z = c_add(z, c_mul(a1, isn));
+    cplx o = c_scale(a1, cs);
+    o = c_add(o, c_mul(a0, isn));
+    s->a[i0] = z; s->a[i1] = o;
+  }
+}
+
 /* EZ: exponential_pauli_z.hpp:40-78 with coeff = exp_i(theta) (:369-377) */
 static void gate_ez(orc_state* s, int q, double theta)
 {
@@ -257,6 +276,7 @@ int orc_apply(orc_state* s, const oracle_op* ops, int num_ops)
       }
       case ORC_EY: gate_ey(s, q0, op->p[0]); break;
       case ORC_EZ: gate_ez(s, q0, op->p[0]); break;
+      case ORC_EX: gate_ex(s, q0, op->p[0]); break;
       case ORC_SWAP: gate_swap(s, q0, q1); break;
       case ORC_BEGIN_FUSION: case ORC_END_FUSION: break;
       default: return -1;

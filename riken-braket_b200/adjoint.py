@@ -1,0 +1,98 @@
+"""Adjoint (reverse-sweep) gradients through the C ABI (rbk_adjoint_gradient).
+
+The reference has no differentiation support; this is one of the engine's
+extensions.  ``adjoint_gradient`` returns E(theta) = <psi|H|psi> and dE/dtheta
+for a circuit whose EX/EY/EZ gates take parameters.  ``AnsatzEnergy`` wraps it
+in a torch.autograd.Function; it exists only as a gradient-check harness
+(torch.autograd.gradcheck), not as a compute path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import rbk
+
+GATE = {"H": 1, "X": 2, "Y": 3, "Z": 4, "U1": 5, "U2": 6, "U3": 7, "CNOT": 8, "CZ": 9, "U": 10,
+        "EX": 11, "EY": 12, "EZ": 13, "SWAP": 14}
+
+
+class CircuitGate(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("qubits", ctypes.c_int32 * 2), ("param", ctypes.c_int32),
+                ("scale", ctypes.c_double), ("angles", ctypes.c_double * 3)]
+
+
+def gate_array(spec):
+    """spec: list of (mnemonic, qubits, param_index or None, scale, angles)."""
+    arr = (CircuitGate * max(1, len(spec)))()
+    for i, (mnem, qubits, param, scale, angles) in enumerate(spec):
+        g = arr[i]
+        g.kind = GATE[mnem]
+        for j, q in enumerate(qubits[:2]):
+            g.qubits[j] = int(q)
+        g.param = -1 if param is None else int(param)
+        g.scale = float(scale)
+        for j, a in enumerate(angles[:3]):
+            g.angles[j] = float(a)
+    return arr, len(spec)
+
+
+def ansatz_spec(n, layers):
+    """The hardware-efficient ansatz of circuits.ansatz as a parametrised gate
+    list: RY(theta_k) = EY with scale -1/2, RZ(theta_k) = EZ with scale -1/2,
+    then the CZ ring; parameter k in the same order as circuits.ansatz."""
+    spec, k = [], 0
+    for _ in range(layers):
+        for q in range(n):
+            spec.append(("EY", (q,), k, -0.5, ()))
+            k += 1
+        for q in range(n):
+            spec.append(("EZ", (q,), k, -0.5, ()))
+            k += 1
+        for i in range(n):
+            spec.append(("CZ", (i, (i + 1) % n), None, 0.0, ()))
+    return spec, k
+
+
+def _bind():
+    lib = rbk.lib()
+    f = lib.rbk_adjoint_gradient
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                  ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    return f
+
+
+def adjoint_gradient(n, spec, theta, terms, precision=rbk.C128, device=0):
+    """Returns (energy, gradient) for the parametrised gate list `spec`."""
+    gates, count = gate_array(spec)
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    strings = b"".join(s.encode() for s, _ in terms)
+    coeffs = np.array([[complex(c).real, complex(c).imag] for _, c in terms], dtype=np.float64).ravel()
+    energy = ctypes.c_double()
+    grad = np.zeros(theta.size, dtype=np.float64)
+    rc = _bind()(n, precision, device, ctypes.cast(gates, ctypes.c_void_p), count, theta.ctypes.data, theta.size,
+                 len(terms), strings, coeffs.ctypes.data, ctypes.addressof(energy), grad.ctypes.data)
+    if rc != 0:
+        raise rbk.RbkError(rc, rbk.lib().rbk_last_error().decode())
+    return energy.value, grad
+
+
+def make_autograd_function():
+    """torch.autograd.Function over adjoint_gradient (gradient-check harness only)."""
+    import torch
+
+    class AnsatzEnergy(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, theta, n, spec, terms):
+            e, g = adjoint_gradient(n, spec, theta.detach().cpu().numpy(), terms)
+            ctx.save_for_backward(torch.from_numpy(g))
+            return theta.new_tensor(e)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            (g,) = ctx.saved_tensors
+            return grad_out * g.to(grad_out.dtype), None, None, None
+
+    return AnsatzEnergy

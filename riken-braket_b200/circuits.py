@@ -127,7 +127,7 @@ def ansatz_hamiltonian(n):
 def random_circuit(n, count, seed=1, kinds=None):
     """Random mix of the hot-path instructions (parity tests)."""
     rng = _rng(seed)
-    kinds = kinds or ["H", "X", "Y", "Z", "U1", "U2", "U3", "CNOT", "CZ", "U", "EY", "EZ", "SWAP"]
+    kinds = kinds or ["H", "X", "Y", "Z", "U1", "U2", "U3", "CNOT", "CZ", "U", "EX", "EY", "EZ", "SWAP"]
     ops = []
     for _ in range(count):
         k = kinds[int(rng.integers(len(kinds)))]
@@ -135,7 +135,7 @@ def random_circuit(n, count, seed=1, kinds=None):
         a = [float(x) for x in rng.uniform(0.0, TWO_PI, size=3)]
         if k in ("H", "X", "Y", "Z"):
             ops.append((k, (q[0],), ()))
-        elif k in ("U1", "EY", "EZ"):
+        elif k in ("U1", "EX", "EY", "EZ"):
             ops.append((k, (q[0],), (a[0],)))
         elif k == "U2":
             ops.append((k, (q[0],), (a[0], a[1])))

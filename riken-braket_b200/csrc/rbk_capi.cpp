@@ -38,6 +38,7 @@ struct rbk_state {
   rbk_stats stats{};
   cudaEvent_t ev_first = nullptr, ev_last = nullptr, ev_sync = nullptr;
   bool timing_started = false;
+  bool owns_stream = true;  // false when the stream is borrowed from another state
 };
 
 namespace {
@@ -421,7 +422,7 @@ int rbk_state_destroy(rbk_state* s)
   if (s->d_out) cudaFree(s->d_out);
   if (s->h_out) cudaFreeHost(s->h_out);
   for (cudaEvent_t ev : {s->ev_first, s->ev_last, s->ev_sync}) if (ev) cudaEventDestroy(ev);
-  if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
   delete s;
   return RBK_OK;
 }
@@ -949,3 +950,174 @@ int rbk_fidelity(rbk_state* a, rbk_state* b, double* out)
 }
 
 }  // extern "C"
+
+// ---- adjoint gradient ---------------------------------------------------------
+//
+// No counterpart in the reference (which has no differentiation support).
+// Forward: psi = U(theta)|0...0> through the fused passes.  Then lambda = H psi
+// and E = <psi|lambda>.  Reverse: for g = last..first, a rotation
+// exp(i phi P) with phi = scale * theta[k] + offset contributes
+//   dE/dtheta_k += 2 Re(i scale <lambda|P|psi>) = -2 scale Im <lambda|P|psi>
+// (psi, lambda taken after gate g), then U_g^dagger is applied to both states.
+// The gate inverses are exact (rotation angle negated, U3(t,p,l)^dagger =
+// U3(-t,-l,-p), self-inverse Paulis), so no intermediate state is stored.
+
+namespace {
+
+int apply_circuit_gate(rbk_state* s, const rbk_circuit_gate& g, const double* theta, bool inverse)
+{
+  const uint32_t q0 = static_cast<uint32_t>(g.qubits[0]), q1 = static_cast<uint32_t>(g.qubits[1]);
+  const double sign = inverse ? -1.0 : 1.0;
+  const double phase = (g.param >= 0 ? g.scale * theta[g.param] : 0.0) + g.angles[0];
+  switch (g.kind) {
+    case RBK_GATE_H: return rbk_hadamard(s, q0, nullptr, 0);
+    case RBK_GATE_X: return rbk_pauli_x(s, q0, nullptr, 0);
+    case RBK_GATE_Y: return rbk_pauli_y(s, q0, nullptr, 0);
+    case RBK_GATE_Z: return rbk_pauli_z(s, &q0, 1);
+    case RBK_GATE_U1: return rbk_phase_shift(s, sign * phase, &q0, 1);
+    case RBK_GATE_U2:
+      return inverse ? rbk_phase_shift3(s, -1.5707963267948966192, -g.angles[1], -g.angles[0], q0, nullptr, 0)
+                     : rbk_phase_shift2(s, g.angles[0], g.angles[1], q0, nullptr, 0);
+    case RBK_GATE_U3:
+      return inverse ? rbk_phase_shift3(s, -g.angles[0], -g.angles[2], -g.angles[1], q0, nullptr, 0)
+                     : rbk_phase_shift3(s, g.angles[0], g.angles[1], g.angles[2], q0, nullptr, 0);
+    case RBK_GATE_CNOT: return rbk_pauli_x(s, q1, &q0, 1);
+    case RBK_GATE_CZ: { const uint32_t qs[2] = {q0, q1}; return rbk_pauli_z(s, qs, 2); }
+    case RBK_GATE_U: {
+      const uint32_t qs[2] = {q0, q1};
+      const int k = static_cast<int>(g.angles[0]);
+      return rbk_controlled_phase_shift_k(s, inverse ? -k : k, qs, 2);
+    }
+    case RBK_GATE_EX: return rbk_exponential_pauli_x(s, sign * phase, q0, nullptr, 0);
+    case RBK_GATE_EY: return rbk_exponential_pauli_y(s, sign * phase, q0, nullptr, 0);
+    case RBK_GATE_EZ: return rbk_exponential_pauli_z(s, sign * phase, q0, nullptr, 0);
+    case RBK_GATE_SWAP: return rbk_swap(s, q0, q1, nullptr, 0);
+    default: return fail(RBK_ERR_INVALID, "unknown circuit gate kind");
+  }
+}
+
+struct state_guard {
+  rbk_state* s = nullptr;
+  ~state_guard() { if (s) rbk_state_destroy(s); }
+};
+
+struct device_buffer {
+  double* p = nullptr;
+  ~device_buffer() { if (p) cudaFree(p); }
+};
+
+}  // namespace
+
+extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, const rbk_circuit_gate* gates,
+                                    int num_gates, const double* theta, int num_params, int num_terms,
+                                    const char* strings, const double* coeffs, double* energy, double* grad)
+{
+  return guarded([&]() -> int {
+    if (num_gates < 0 || (num_gates > 0 && !gates) || num_params < 0 || (num_params > 0 && (!theta || !grad)) ||
+        num_terms < 1 || !strings || !coeffs || !energy)
+      return fail(RBK_ERR_INVALID, "bad adjoint-gradient arguments");
+    for (int i = 0; i < num_gates; ++i) {
+      const auto& g = gates[i];
+      if (g.param >= num_params) return fail(RBK_ERR_INVALID, "gate parameter index out of range");
+      if (g.param >= 0 && g.kind != RBK_GATE_EX && g.kind != RBK_GATE_EY && g.kind != RBK_GATE_EZ)
+        return fail(RBK_ERR_UNSUPPORTED, "only EX, EY and EZ gates take parameters");
+    }
+    // Observable as grouped Pauli sums (logical bits: both states are kept canonical).
+    rbk::pauli_sum H{};
+    {
+      struct term { uint64_t flip, sign; cplx w; };
+      std::vector<term> terms;
+      static const cplx pow_mi[4] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}};
+      for (int t = 0; t < num_terms; ++t) {
+        uint64_t x = 0, y = 0, z = 0;
+        for (int k = 0; k < num_qubits; ++k) {
+          const char c = strings[static_cast<size_t>(t) * num_qubits + k];
+          if (c == 'X') x |= 1ull << k;
+          else if (c == 'Y') y |= 1ull << k;
+          else if (c == 'Z') z |= 1ull << k;
+          else if (c != 'I') return fail(RBK_ERR_INVALID, "Pauli strings use the characters I, X, Y, Z");
+        }
+        terms.push_back({x | y, y | z, cplx{coeffs[2 * t], coeffs[2 * t + 1]} * pow_mi[__builtin_popcountll(y) & 3]});
+      }
+      std::vector<char> done(terms.size(), 0);
+      int nt = 0;
+      for (size_t i = 0; i < terms.size(); ++i) {
+        if (done[i]) continue;
+        if (H.num_groups >= rbk::kMaxSumGroups) return fail(RBK_ERR_INVALID, "more than 64 distinct X/Y patterns in the observable");
+        H.flip[H.num_groups] = terms[i].flip;
+        H.begin[H.num_groups] = nt;
+        for (size_t j = i; j < terms.size(); ++j) {
+          if (done[j] || terms[j].flip != terms[i].flip) continue;
+          if (nt >= rbk::kMaxSumTerms) return fail(RBK_ERR_INVALID, "more than 128 Pauli strings in the observable");
+          H.sign[nt] = terms[j].sign;
+          H.w[nt][0] = terms[j].w.real();
+          H.w[nt][1] = terms[j].w.imag();
+          ++nt;
+          done[j] = 1;
+        }
+        ++H.num_groups;
+      }
+      H.begin[H.num_groups] = nt;
+    }
+
+    state_guard psi, lam;
+    if (int rc = rbk_state_create(num_qubits, precision, 0, device, &psi.s)) return rc;
+    if (int rc = rbk_state_create(num_qubits, precision, 0, device, &lam.s)) return rc;
+    device_guard dg(device);
+    // One stream for both states: every kernel below is ordered without host waits.
+    cudaStreamSynchronize(lam.s->stream);
+    cudaStreamDestroy(lam.s->stream);
+    lam.s->stream = psi.s->stream;
+    lam.s->owns_stream = false;
+
+    int num_pg = 0;
+    for (int i = 0; i < num_gates; ++i) num_pg += gates[i].param >= 0 ? 1 : 0;
+    device_buffer ov;  // (re, im) of <lambda|P|psi> per parametrised gate, then E
+    RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&ov.p), sizeof(double) * 2 * (num_pg + 1)));
+
+    for (int i = 0; i < num_gates; ++i)
+      if (int rc = apply_circuit_gate(psi.s, gates[i], theta, false)) return rc;
+    if (int rc = canonicalize(psi.s)) return rc;
+    const bool c128 = precision == RBK_C128;
+    cudaError_t e = c128 ? rbk::launch_pauli_apply<double>(psi.s->amps, lam.s->amps, num_qubits, H, psi.s->stream)
+                         : rbk::launch_pauli_apply<float>(psi.s->amps, lam.s->amps, num_qubits, H, psi.s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "H psi");
+    // E = <psi|lambda>
+    e = c128 ? rbk::launch_inner<double>(lam.s->amps, psi.s->amps, num_qubits, psi.s->d_partials, ov.p + 2 * num_pg, psi.s->stream)
+             : rbk::launch_inner<float>(lam.s->amps, psi.s->amps, num_qubits, psi.s->d_partials, ov.p + 2 * num_pg, psi.s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "energy");
+
+    std::vector<int> slot_param(num_pg);
+    std::vector<double> slot_scale(num_pg);
+    int slot = num_pg;
+    for (int i = num_gates - 1; i >= 0; --i) {
+      const auto& g = gates[i];
+      if (g.param >= 0) {
+        if (int rc = flush(psi.s)) return rc;
+        if (int rc = flush(lam.s)) return rc;
+        if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
+        --slot;
+        slot_param[slot] = g.param;
+        slot_scale[slot] = g.scale;
+        const uint64_t t = 1ull << psi.s->perm[g.qubits[0]];
+        uint64_t flip = 0, sign = 0;
+        double wr = 1.0, wi = 0.0;
+        if (g.kind == RBK_GATE_EX) flip = t;
+        else if (g.kind == RBK_GATE_EY) { flip = t; sign = t; wr = 0.0; wi = -1.0; }
+        else sign = t;  // EZ
+        e = c128 ? rbk::launch_overlap<double>(lam.s->amps, psi.s->amps, num_qubits, flip, sign, wr, wi, psi.s->d_partials, ov.p + 2 * slot, psi.s->stream)
+                 : rbk::launch_overlap<float>(lam.s->amps, psi.s->amps, num_qubits, flip, sign, wr, wi, psi.s->d_partials, ov.p + 2 * slot, psi.s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "overlap");
+      }
+      if (int rc = apply_circuit_gate(psi.s, g, theta, true)) return rc;
+      if (int rc = apply_circuit_gate(lam.s, g, theta, true)) return rc;
+    }
+    std::vector<double> host(2 * (num_pg + 1));
+    RBK_CUDA(cudaMemcpyAsync(host.data(), ov.p, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, psi.s->stream));
+    if (int rc = bounded_sync(psi.s)) return rc;
+    *energy = host[2 * num_pg];
+    for (int k = 0; k < num_params; ++k) grad[k] = 0.0;
+    for (int j = 0; j < num_pg; ++j) grad[slot_param[j]] += -2.0 * slot_scale[j] * host[2 * j + 1];
+    return RBK_OK;
+  });
+}

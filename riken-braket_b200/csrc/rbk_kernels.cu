@@ -287,3 +287,84 @@ template cudaError_t launch_probs<double>(const void*, uint64_t, uint64_t, doubl
 template cudaError_t launch_probs<float>(const void*, uint64_t, uint64_t, double*, cudaStream_t);
 
 }  // namespace rbk
+
+namespace rbk {
+
+// ---------------------------------------------------------------------------
+// Adjoint-gradient helpers
+// ---------------------------------------------------------------------------
+
+// dst_i = sum_g sum_{t in g} w_t (-1)^popcount(i & sign_t) src_{i ^ flip_g}
+// (a Pauli-string sum applied to a state; pauli_index_coeff.hpp:17-59 form).
+template <typename Real>
+__global__ void pauli_apply_kernel(const typename ctype<Real>::c* __restrict__ src, typename ctype<Real>::c* __restrict__ dst,
+                                   uint64_t size, const pauli_sum P)
+{
+  using C = typename ctype<Real>::c;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += stride) {
+    double re = 0, im = 0;
+    for (int g = 0; g < P.num_groups; ++g) {
+      const C v = src[i ^ P.flip[g]];
+      double wr = 0, wi = 0;
+      for (int t = P.begin[g]; t < P.begin[g + 1]; ++t) {
+        const double s = (__popcll(i & P.sign[t]) & 1) ? -1.0 : 1.0;
+        wr += s * P.w[t][0];
+        wi += s * P.w[t][1];
+      }
+      re += wr * double(v.x) - wi * double(v.y);
+      im += wr * double(v.y) + wi * double(v.x);
+    }
+    dst[i] = C{(Real)re, (Real)im};
+  }
+}
+
+// sum_i conj(lam_i) w (-1)^popcount(i & sign) psi_{i ^ flip}: <lam| P |psi> for
+// one Pauli string P given as (flip, sign, w) -- the overlap of the adjoint sweep.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads)
+overlap_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename ctype<Real>::c* __restrict__ psi,
+               uint64_t size, uint64_t flip, uint64_t sign, double wr, double wi, double* partials)
+{
+  double re = 0, im = 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += stride) {
+    const auto l = lam[i], p = psi[i ^ flip];
+    const double s = (__popcll(i & sign) & 1) ? -1.0 : 1.0;
+    // conj(l) * p
+    const double cr = double(l.x) * double(p.x) + double(l.y) * double(p.y);
+    const double ci = double(l.x) * double(p.y) - double(l.y) * double(p.x);
+    re += s * (cr * wr - ci * wi);
+    im += s * (cr * wi + ci * wr);
+  }
+  double vals[2] = {re, im};
+  block_sum_store<2>(vals, 2, partials + size_t(blockIdx.x) * 2);
+}
+
+template <typename Real>
+cudaError_t launch_pauli_apply(const void* src, void* dst, int n, const pauli_sum& P, cudaStream_t stream)
+{
+  const uint64_t size = 1ull << n;
+  pauli_apply_kernel<Real><<<grid_for(size, 256), 256, 0, stream>>>(
+    static_cast<const typename ctype<Real>::c*>(src), static_cast<typename ctype<Real>::c*>(dst), size, P);
+  return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_overlap(const void* lam, const void* psi, int n, uint64_t flip, uint64_t sign, double wr, double wi,
+                           double* partials, double* out, cudaStream_t stream)
+{
+  const int blocks = reduction_blocks();
+  overlap_kernel<Real><<<blocks, kRedThreads, 0, stream>>>(static_cast<const typename ctype<Real>::c*>(lam),
+                                                           static_cast<const typename ctype<Real>::c*>(psi), 1ull << n,
+                                                           flip, sign, wr, wi, partials);
+  finish_partials_kernel<<<1, 32, 0, stream>>>(partials, blocks, 2, out);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_pauli_apply<double>(const void*, void*, int, const pauli_sum&, cudaStream_t);
+template cudaError_t launch_pauli_apply<float>(const void*, void*, int, const pauli_sum&, cudaStream_t);
+template cudaError_t launch_overlap<double>(const void*, const void*, int, uint64_t, uint64_t, double, double, double*, double*, cudaStream_t);
+template cudaError_t launch_overlap<float>(const void*, const void*, int, uint64_t, uint64_t, double, double, double*, double*, cudaStream_t);
+
+}  // namespace rbk

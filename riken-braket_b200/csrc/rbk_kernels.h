@@ -40,4 +40,23 @@ template <typename Real> cudaError_t launch_inner(const void* a, const void* b, 
 template <typename Real> cudaError_t launch_probs(const void* state, uint64_t offset, uint64_t count, double* out,
                                                   cudaStream_t stream);
 
+// A sum of Pauli strings grouped by flip mask, for applying H to a state:
+// group g holds terms [begin[g], begin[g+1]).
+constexpr int kMaxSumGroups = 64;
+constexpr int kMaxSumTerms = 128;
+struct pauli_sum {
+  int num_groups;
+  int pad;
+  uint64_t flip[kMaxSumGroups];
+  int begin[kMaxSumGroups + 1];
+  int pad2;
+  uint64_t sign[kMaxSumTerms];
+  double w[kMaxSumTerms][2];
+};
+
+template <typename Real> cudaError_t launch_pauli_apply(const void* src, void* dst, int n, const pauli_sum& P, cudaStream_t stream);
+// out (device, 2 doubles) = <lam| P |psi> with P = w (-1)^popcount(i & sign) X^flip
+template <typename Real> cudaError_t launch_overlap(const void* lam, const void* psi, int n, uint64_t flip, uint64_t sign,
+                                                    double wr, double wi, double* partials, double* out, cudaStream_t stream);
+
 }  // namespace rbk

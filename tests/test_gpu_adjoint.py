@@ -1,0 +1,119 @@
+"""Adjoint gradients (GPU, through the C ABI) against the parameter-shift rule
+evaluated with the reference's own ket code (oracle/_ref) where it is built,
+else with the C restatement, and against central finite differences.  The
+reference has no differentiation support, so these are the checks: energy to
+1e-12, parameter-shift gradients to 1e-9, finite differences (h = 1e-6) to 1e-6."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+REF_BUILT = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libketref.so"))
+
+
+def cpu_energy(pkg, n, layers, theta, terms, ref=False):
+    ops, _ = pkg.circuits.ansatz(n, layers, thetas=theta)
+    o = oracle.KetRef(n) if ref else oracle.COracle(n)
+    o.apply(ops)
+    return o.expectation(terms).real
+
+
+@pytest.mark.parametrize("n,layers", [(4, 2), (6, 3), (9, 2)])
+def test_adjoint_matches_parameter_shift_and_fd(pkg, n, layers):
+    C = pkg.circuits
+    terms = C.ansatz_hamiltonian(n)
+    _, theta = C.ansatz(n, layers, seed=n)
+    spec, nparams = pkg.adjoint.ansatz_spec(n, layers)
+    assert nparams == theta.size
+    e, g = pkg.adjoint.adjoint_gradient(n, spec, theta, terms)
+    assert abs(e - cpu_energy(pkg, n, layers, theta, terms, ref=REF_BUILT)) <= 1e-12
+    shift = np.empty_like(theta)
+    fd = np.empty_like(theta)
+    for k in range(theta.size):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += math.pi / 2
+        tm[k] -= math.pi / 2
+        shift[k] = 0.5 * (cpu_energy(pkg, n, layers, tp, terms, ref=REF_BUILT) - cpu_energy(pkg, n, layers, tm, terms, ref=REF_BUILT))
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += 1e-6
+        tm[k] -= 1e-6
+        fd[k] = (cpu_energy(pkg, n, layers, tp, terms) - cpu_energy(pkg, n, layers, tm, terms)) / 2e-6
+    assert np.abs(g - shift).max() <= 1e-9
+    assert np.abs(g - fd).max() <= 1e-6
+
+
+def test_adjoint_config4_20_qubits(pkg):
+    """20-qubit ansatz, 16 layers, 640 parameters: energy against the oracle and
+    a sample of gradients against the parameter-shift rule."""
+    C = pkg.circuits
+    n, layers = 20, 16
+    terms = C.ansatz_hamiltonian(n)
+    _, theta = C.ansatz(n, layers, seed=1)
+    spec, nparams = pkg.adjoint.ansatz_spec(n, layers)
+    assert nparams == 640
+    e, g = pkg.adjoint.adjoint_gradient(n, spec, theta, terms)
+    assert abs(e - cpu_energy(pkg, n, layers, theta, terms)) <= 1e-12
+    for k in (0, 19, 20, 333, 620, 639):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += math.pi / 2
+        tm[k] -= math.pi / 2
+        shift = 0.5 * (cpu_energy(pkg, n, layers, tp, terms) - cpu_energy(pkg, n, layers, tm, terms))
+        assert abs(g[k] - shift) <= 1e-9
+
+
+def test_adjoint_general_gates_and_c64(pkg):
+    """Fixed gates of every kind around the rotations (exact inverses in the
+    reverse sweep); complex<float> against the FP64 result."""
+    C = pkg.circuits
+    n = 7
+    rng = np.random.default_rng(3)
+    spec, k = [], 0
+    for _ in range(3):
+        for q in range(n):
+            spec.append(("U3", (q,), None, 0.0, tuple(rng.uniform(0, 6.28, 3))))
+            spec.append((["EX", "EY", "EZ"][q % 3], (q,), k, 0.7, (0.1,)))
+            k += 1
+        spec += [("CNOT", (0, 3), None, 0.0, ()), ("H", (2,), None, 0.0, ()), ("U", (1, 5), None, 0.0, (3,)),
+                 ("SWAP", (4, 6), None, 0.0, ()), ("U1", (6,), None, 0.0, (0.4,)), ("U2", (5,), None, 0.0, (0.3, 1.1)),
+                 ("Y", (3,), None, 0.0, ()), ("CZ", (2, 4), None, 0.0, ())]
+    theta = rng.uniform(-math.pi, math.pi, k)
+    terms = C.ansatz_hamiltonian(n) + [("XYZ" + "I" * (n - 3), 0.3)]
+    e, g = pkg.adjoint.adjoint_gradient(n, spec, theta, terms)
+
+    def energy(th):
+        ops = []
+        for mnem, qubits, param, scale, angles in spec:
+            if param is not None:
+                ops.append((mnem, qubits, (scale * th[param] + angles[0],)))
+            elif mnem == "U":
+                ops.append((mnem, qubits, (int(angles[0]),)))
+            else:
+                ops.append((mnem, qubits, tuple(angles)))
+        o = oracle.COracle(n)
+        o.apply(ops)
+        return o.expectation(terms).real
+
+    assert abs(e - energy(theta)) <= 1e-12
+    for j in range(k):
+        tp, tm = theta.copy(), theta.copy()
+        tp[j] += 1e-6
+        tm[j] -= 1e-6
+        assert abs(g[j] - (energy(tp) - energy(tm)) / 2e-6) <= 1e-6
+    e32, g32 = pkg.adjoint.adjoint_gradient(n, spec, theta, terms, precision=pkg.C64)
+    assert abs(e32 - e) <= 1e-5 and np.abs(g32 - g).max() <= 1e-4
+
+
+def test_autograd_harness_gradcheck(pkg):
+    torch = pytest.importorskip("torch")
+    n, layers = 4, 2
+    terms = pkg.circuits.ansatz_hamiltonian(n)
+    spec, nparams = pkg.adjoint.ansatz_spec(n, layers)
+    fn = pkg.adjoint.make_autograd_function()
+    theta = torch.tensor(np.random.default_rng(0).uniform(-3, 3, nparams), dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(lambda t: fn.apply(t, n, spec, terms), (theta,), eps=1e-6, atol=1e-6)
