@@ -333,6 +333,72 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_adjoint(args):
+    """Config 4: energy + adjoint gradient of the 20-qubit ansatz (16 layers of
+    RY, RZ and a CZ ring; 640 parameters; H = sum Z_i Z_i+1 + 0.5 sum X_i),
+    against per-parameter plain GPU evaluation (parameter shift, 2 energies per
+    parameter) and the reference's CPU code doing the same."""
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    C = pkg.circuits
+    n, layers = 20, 16
+    terms = C.ansatz_hamiltonian(n)
+    _, theta = C.ansatz(n, layers, seed=SEED)
+    spec, nparams = pkg.adjoint.ansatz_spec(n, layers)
+    for _ in range(args.warmup):
+        pkg.adjoint.adjoint_gradient(n, spec, theta, terms)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e, g = pkg.adjoint.adjoint_gradient(n, spec, theta, terms)
+    t_adj = (time.perf_counter() - t0) / args.steps
+
+    # Per-parameter plain GPU evaluation: E(theta +- pi/2 e_k) through the fused engine.
+    s = pkg.State(n, pkg.C128)
+    sample = list(range(0, nparams, max(1, nparams // 16)))[:16]
+
+    def energy_gpu(th):
+        s.reset(0)
+        s.apply(C.ansatz(n, layers, thetas=th)[0])
+        return s.expectation(terms).real
+
+    energy_gpu(theta)
+    t0 = time.perf_counter()
+    shift = []
+    for k in sample:
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += math.pi / 2
+        tm[k] -= math.pi / 2
+        shift.append(0.5 * (energy_gpu(tp) - energy_gpu(tm)))
+    t_shift = (time.perf_counter() - t0) / len(sample) * nparams
+    err = max(abs(a - g[k]) for a, k in zip(shift, sample))
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        threads = os.cpu_count() or 1
+        ops, _ = C.ansatz(n, layers, thetas=theta)
+        r = oracle.KetRef(n, threads=threads, fast=True)
+        secs = r.apply_timed(ops)
+        t1 = time.perf_counter()
+        r.expectation(terms)
+        secs += time.perf_counter() - t1
+        cpu = {"value": 1.0 / (secs * 2 * nparams), "unit": "gradients/s", "cores": threads, "kind": "reference",
+               "sample": f"one energy evaluation (ket forward + expectation, release build) = {secs:.3f} s, "
+                         f"times 2 x {nparams} parameter-shift evaluations"}
+    peak, peak_kind = load_peaks()
+    line = {
+        "metric": "adjoint gradients/s (20q ansatz, 640 parameters)", "value": 1.0 / t_adj, "unit": "gradients/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_adj * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "energy + adjoint gradient, 20-qubit hardware-efficient ansatz, 16 layers, 640 parameters",
+                   "per_parameter_gpu_ms": t_shift * 1e3, "speedup_vs_per_parameter_gpu": t_shift / t_adj,
+                   "max_abs_diff_vs_parameter_shift": err, "energy": e, "timing": "host wall clock per call (includes state set-up)"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,9 +412,13 @@ def main():
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--shape", type=int, default=None, help="tile shape (rbk_state_set_tile_shape)")
     ap.add_argument("--budget", type=int, default=None, help="dense gates per pass (rbk_state_set_pass_budget)")
+    ap.add_argument("--workload", default="brick", choices=["brick", "adjoint"],
+                    help="brick: the 30-qubit circuit (default); adjoint: energy + gradient of the 20-qubit ansatz")
     args = ap.parse_args()
     globals()["N_QUBITS"], globals()["DEPTH"] = args.qubits, args.depth
-    if args.impl == "reference":
+    if args.workload == "adjoint":
+        run_adjoint(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
