@@ -175,6 +175,24 @@ int rbk_inner_product(rbk_state* a, rbk_state* b, double* out);
 /* ket::fidelity: |<b|a>|^2 (fidelity.hpp) */
 int rbk_fidelity(rbk_state* a, rbk_state* b, double* out);
 
+/* ---- sampling and measurement -------------------------------------------
+ * Random numbers come from a std::mt19937_64 per state, seeded with 1 at
+ * creation (bra's random_number_generator_, bra/include/bra/state.hpp:459-479,
+ * fed by --seed). */
+int rbk_state_seed(rbk_state* s, uint64_t seed);
+/* GENERATE EVENTS: num_events basis-state indices drawn from |a_i|^2 as
+ * ket::generate_events does (ket/include/ket/generate_events.hpp:18-66):
+ * uniform_real_distribution(0, total) and upper_bound over the inclusive prefix
+ * sums.  seed < 0 uses (and advances) the state's generator; otherwise a fresh
+ * generator built from seed.  Unlike the reference, the state is left intact. */
+int rbk_generate_events(rbk_state* s, int num_events, int64_t seed, uint64_t* events);
+/* ket::measure (ket/include/ket/measure.hpp:16-46): sample one index with the
+ * state's generator; the state becomes that basis state. */
+int rbk_measure(rbk_state* s, uint64_t* outcome);
+/* M q: ket::gate::projective_measurement (ket/include/ket/gate/projective_measurement.hpp):
+ * outcome 0/1 with probabilities p0/p1, the kept half scaled by p^(-1/2). */
+int rbk_projective_measurement(rbk_state* s, uint32_t qubit, int* outcome);
+
 /* ---- adjoint gradient (no counterpart in the reference) --------------------
  * One gate of a parametrised circuit, in bra's terms.  qubits[0] is the target
  * (CNOT: qubits[0] = control, qubits[1] = target, as in "CNOT c t"; CZ, SWAP and

@@ -57,6 +57,10 @@
 #include <ket/gate/utility/index_with_qubits.hpp>
 #include <ket/gate/utility/pauli_index_coeff.hpp>
 #include <ket/all_spin_expectation_values.hpp>
+#include <ket/generate_events.hpp>
+#include <ket/measure.hpp>
+#include <ket/gate/projective_measurement.hpp>
+#include <random>
 #include <ket/expectation_value.hpp>
 #include <ket/inner_product.hpp>
 #include <ket/utility/generate_phase_coefficients.hpp>
@@ -107,6 +111,7 @@ struct ref_state
   std::vector<found> found_qubits;
   std::vector<std::unique_ptr<bra::fused_gate::fused_gate<plain_it>>> fused_plain;
   std::vector<std::unique_ptr<bra::fused_gate::fused_gate<cache_it>>> fused_cache;
+  std::mt19937_64 rng{1};  // bra::state's random_number_generator_ (bra/include/bra/state.hpp:459-479)
 
   ref_state(unsigned nq, unsigned threads, std::uint64_t initial)
     : n{nq}, policy{threads}, data(std::size_t{1} << nq), found_qubits(nq, found::none)
@@ -395,6 +400,38 @@ void ketref_inner_product(void* a, void* b, double* out)
   auto const v = ket::ranges::inner_product(sa.policy, sa.data, sb.data);
   out[0] = v.real();
   out[1] = v.imag();
+}
+
+void ketref_seed(void* h, std::uint64_t seed) { static_cast<ref_state*>(h)->rng.seed(seed); }
+
+// GENERATE EVENTS (bra/src/nompi_state.cpp:1143-1153): seed < 0 uses the
+// state's generator, else ket's seeded overload.  Like the reference, this
+// overwrites the amplitudes with the prefix sums.
+void ketref_generate_events(void* h, int num_events, long long seed, std::uint64_t* out)
+{
+  auto& s = *static_cast<ref_state*>(h);
+  std::vector<std::uint64_t> events;
+  if (seed < 0)
+    ket::ranges::generate_events(ket::utility::policy::make_sequential(), events, s.data, num_events, s.rng);
+  else
+    ket::ranges::generate_events(ket::utility::policy::make_sequential(), events, s.data, num_events, s.rng,
+                                 static_cast<std::mt19937_64::result_type>(seed));
+  for (int i = 0; i < num_events; ++i) out[i] = events[i];
+}
+
+// ket::ranges::measure with the state's generator (bra/src/nompi_state.cpp do_measure).
+std::uint64_t ketref_measure(void* h)
+{
+  auto& s = *static_cast<ref_state*>(h);
+  return static_cast<std::uint64_t>(ket::ranges::measure(ket::utility::policy::make_sequential(), s.data, s.rng));
+}
+
+// M q (bra/src/nompi_state.cpp:1102-1103).
+int ketref_projective_measurement(void* h, int qubit)
+{
+  auto& s = *static_cast<ref_state*>(h);
+  auto const r = ket::gate::ranges::projective_measurement(s.policy, s.data, s.rng, qb(qubit));
+  return r == ket::gate::outcome::one ? 1 : 0;
 }
 
 } // extern "C"

@@ -78,6 +78,11 @@ class KetRef:
         lib.ketref_expectation.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p,
                                            ctypes.c_void_p, ctypes.c_void_p]
         lib.ketref_inner_product.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ketref_seed.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        lib.ketref_generate_events.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p]
+        lib.ketref_measure.argtypes = [ctypes.c_void_p]
+        lib.ketref_measure.restype = ctypes.c_uint64
+        lib.ketref_projective_measurement.argtypes = [ctypes.c_void_p, ctypes.c_int]
         self.lib, self.n = lib, n
         self.h = lib.ketref_create(n, threads, initial_index)
         if not self.h:
@@ -127,6 +132,21 @@ class KetRef:
         self.lib.ketref_inner_product(self.h, other.h, out.ctypes.data)
         return complex(out[0], out[1])
 
+    def seed(self, seed):
+        self.lib.ketref_seed(self.h, seed)
+
+    def generate_events(self, num, seed=-1):
+        """Like the reference, this overwrites the amplitudes with prefix sums."""
+        out = np.empty(num, dtype=np.uint64)
+        self.lib.ketref_generate_events(self.h, num, seed, out.ctypes.data)
+        return out
+
+    def measure(self):
+        return int(self.lib.ketref_measure(self.h))
+
+    def projective_measurement(self, q):
+        return int(self.lib.ketref_projective_measurement(self.h, q))
+
 
 class COracle:
     """The project's C restatement (oracle/rbk_oracle.c)."""
@@ -145,6 +165,11 @@ class COracle:
         lib.orc_expectation.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p,
                                         ctypes.c_void_p, ctypes.c_void_p]
         lib.orc_inner_product.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.orc_seed.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        lib.orc_generate_events.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p]
+        lib.orc_projective_measurement.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.orc_measure.argtypes = [ctypes.c_void_p]
+        lib.orc_measure.restype = ctypes.c_uint64
         self.lib, self.n = lib, n
         self.h = lib.orc_create(n, initial_index)
         if not self.h:
@@ -191,3 +216,18 @@ class COracle:
         out = np.empty(2, dtype=np.float64)
         self.lib.orc_inner_product(self.h, other.h, out.ctypes.data)
         return complex(out[0], out[1])
+
+    def seed(self, seed):
+        self.lib.orc_seed(self.h, seed)
+
+    def generate_events(self, num, seed=-1):
+        out = np.empty(num, dtype=np.uint64)
+        if self.lib.orc_generate_events(self.h, num, seed, out.ctypes.data) != 0:
+            raise MemoryError("orc_generate_events")
+        return out
+
+    def projective_measurement(self, q):
+        return int(self.lib.orc_projective_measurement(self.h, q))
+
+    def measure(self):
+        return int(self.lib.orc_measure(self.h))

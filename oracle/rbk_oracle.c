@@ -22,11 +22,52 @@
 
 typedef struct { double re, im; } cplx;
 
+/* MT19937-64 (Matsumoto & Nishimura, 64-bit variant): the engine behind
+ * std::mt19937_64, which bra::state uses (bra/include/bra/state.hpp:459). */
+typedef struct mt64 { uint64_t x[312]; int i; } mt64;
+
+static void mt64_seed(mt64* g, uint64_t seed)
+{
+  g->x[0] = seed;
+  for (int k = 1; k < 312; ++k)
+    g->x[k] = UINT64_C(6364136223846793005) * (g->x[k - 1] ^ (g->x[k - 1] >> 62)) + (uint64_t)k;
+  g->i = 312;
+}
+
+static uint64_t mt64_next(mt64* g)
+{
+  if (g->i >= 312) {
+    for (int k = 0; k < 312; ++k) {
+      uint64_t y = (g->x[k] & UINT64_C(0xFFFFFFFF80000000)) | (g->x[(k + 1) % 312] & UINT64_C(0x7FFFFFFF));
+      uint64_t v = g->x[(k + 156) % 312] ^ (y >> 1);
+      if (y & 1) v ^= UINT64_C(0xB5026F5AA96619E9);
+      g->x[k] = v;
+    }
+    g->i = 0;
+  }
+  uint64_t z = g->x[g->i++];
+  z ^= (z >> 29) & UINT64_C(0x5555555555555555);
+  z ^= (z << 17) & UINT64_C(0x71D67FFFEDA60000);
+  z ^= (z << 37) & UINT64_C(0xFFF7EEE000000000);
+  z ^= z >> 43;
+  return z;
+}
+
+/* std::uniform_real_distribution<double>(0, maximum) over a 64-bit engine:
+ * one draw scaled to [0, 1) with 53 significant bits, times the width. */
+static double mt64_upto(mt64* g, double maximum)
+{
+  double u = (double)mt64_next(g) / 18446744073709551616.0;
+  if (u >= 1.0) u = nextafter(1.0, 0.0);
+  return u * maximum;
+}
+
 typedef struct orc_state {
   int n;
   uint64_t size;
   cplx* a;
   cplx phase_table[65];
+  mt64 rng;
 } orc_state;
 
 static inline cplx c_mul(cplx x, cplx y)
@@ -74,6 +115,7 @@ orc_state* orc_create(int n, uint64_t initial_index)
   s->a = (cplx*)calloc(s->size, sizeof(cplx));
   if (!s->a) { free(s); return NULL; }
   s->a[initial_index].re = 1.0;
+  mt64_seed(&s->rng, 1);
   /* ket::utility::generate_phase_coefficients (ket/include/ket/utility/generate_phase_coefficients.hpp:20-39),
    * called with num_qubits = n by bra (bra/src/state.cpp:148): entry k = exp_i(2 pi / 2^k). */
   for (int k = 0; k <= n && k < 65; ++k)
@@ -356,4 +398,68 @@ void orc_inner_product(const orc_state* a, const orc_state* b, double* out)
 void orc_probabilities(const orc_state* s, double* out)
 {
   for (uint64_t i = 0; i < s->size; ++i) out[i] = s->a[i].re * s->a[i].re + s->a[i].im * s->a[i].im;
+}
+
+/* std::norm of the reference's complex<double>: libstdc++ computes x*x + y*y
+ * for the builtin floating types (the product is not contracted: no FMA on
+ * the x86-64 baseline the reference is built for here). */
+static double ref_norm(cplx z) { return z.re * z.re + z.im * z.im; }
+
+void orc_seed(orc_state* s, uint64_t seed) { mt64_seed(&s->rng, seed); }
+
+/* ket::generate_events (generate_events.hpp:18-66): inclusive prefix sums of
+ * |a|^2, r = uniform(0, total), upper_bound.  seed < 0: the state's generator;
+ * else a fresh one.  The state itself is not modified here. */
+int orc_generate_events(orc_state* s, int num_events, long long seed, uint64_t* out)
+{
+  double* prefix = (double*)malloc(s->size * sizeof(double));
+  if (!prefix) return -1;
+  double run = 0;
+  for (uint64_t i = 0; i < s->size; ++i) { run = run + ref_norm(s->a[i]); prefix[i] = run; }
+  mt64 fresh;
+  mt64* g = &s->rng;
+  if (seed >= 0) { mt64_seed(&fresh, (uint64_t)seed); g = &fresh; }
+  for (int k = 0; k < num_events; ++k) {
+    double r = mt64_upto(g, prefix[s->size - 1]);
+    uint64_t lo = 0, hi = s->size;
+    while (lo < hi) { uint64_t mid = lo + ((hi - lo) >> 1); if (prefix[mid] > r) hi = mid; else lo = mid + 1; }
+    out[k] = lo;
+  }
+  free(prefix);
+  return 0;
+}
+
+/* ket::gate::projective_measurement (projective_measurement.hpp): long double
+ * sums of |a|^2 per outcome, r = uniform(0, p0 + p1) < p0 -> 0, the kept half
+ * scaled by pow(p, -1/2), the other half zeroed. */
+int orc_projective_measurement(orc_state* s, int q)
+{
+  long double z = 0, o = 0;
+  uint64_t half = s->size >> 1, m = UINT64_C(1) << q;
+  for (uint64_t v = 0; v < half; ++v) {
+    uint64_t i0 = insert0(v, q), i1 = i0 | m;
+    z += (long double)ref_norm(s->a[i0]);
+    o += (long double)ref_norm(s->a[i1]);
+  }
+  double p0 = (double)z, p1 = (double)o;
+  int one = !(mt64_upto(&s->rng, p0 + p1) < p0);
+  double mult = pow(one ? p1 : p0, -0.5);
+  for (uint64_t v = 0; v < half; ++v) {
+    uint64_t i0 = insert0(v, q), i1 = i0 | m;
+    uint64_t keep = one ? i1 : i0, drop = one ? i0 : i1;
+    s->a[keep] = c_scale(s->a[keep], mult);
+    s->a[drop].re = 0; s->a[drop].im = 0;
+  }
+  return one;
+}
+
+/* ket::measure (measure.hpp): one event from the state's generator, then the
+ * state becomes the basis vector of that index. */
+uint64_t orc_measure(orc_state* s)
+{
+  uint64_t idx = 0;
+  if (orc_generate_events(s, 1, -1, &idx) != 0) return UINT64_MAX;
+  memset(s->a, 0, s->size * sizeof(cplx));
+  s->a[idx].re = 1.0;
+  return idx;
 }

@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <random>
 #include <string>
 #include <thread>
 #include <vector>
@@ -39,6 +40,7 @@ struct rbk_state {
   cudaEvent_t ev_first = nullptr, ev_last = nullptr, ev_sync = nullptr;
   bool timing_started = false;
   bool owns_stream = true;  // false when the stream is borrowed from another state
+  std::mt19937_64 rng{1};   // bra::state's random_number_generator_ (bra/include/bra/state.hpp:459-479)
 };
 
 namespace {
@@ -1119,5 +1121,113 @@ extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, c
     for (int k = 0; k < num_params; ++k) grad[k] = 0.0;
     for (int j = 0; j < num_pg; ++j) grad[slot_param[j]] += -2.0 * slot_scale[j] * host[2 * j + 1];
     return RBK_OK;
+  });
+}
+
+// ---- sampling and measurement ------------------------------------------------
+
+namespace {
+
+// ket::utility::positive_random_value_upto (ket/include/ket/utility/positive_random_value_upto.hpp):
+// a uniform_real_distribution on [0, maximum).
+double random_upto(std::mt19937_64& g, double maximum)
+{
+  std::uniform_real_distribution<double> d{0.0, maximum};
+  return d(g);
+}
+
+// Inclusive prefix sums of |a_i|^2 in logical order, plus the total.
+int prob_prefix(rbk_state* s, device_buffer& prefix, device_buffer& scratch, double* total)
+{
+  if (int rc = canonicalize(s)) return rc;
+  device_guard g(s->device);
+  const uint64_t size = 1ull << s->n;
+  RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&prefix.p), sizeof(double) * size));
+  RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&scratch.p), sizeof(double) * rbk::scan_scratch_doubles(size)));
+  const cudaError_t e = s->precision == RBK_C128 ? rbk::launch_prob_scan<double>(s->amps, size, prefix.p, scratch.p, s->stream)
+                                                : rbk::launch_prob_scan<float>(s->amps, size, prefix.p, scratch.p, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "probability scan");
+  s->stats.kernel_launches += 2;
+  RBK_CUDA(cudaMemcpyAsync(s->h_out, prefix.p + (size - 1), sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  if (int rc = bounded_sync(s)) return rc;
+  *total = s->h_out[0];
+  return RBK_OK;
+}
+
+int sample_indices(rbk_state* s, std::mt19937_64& g, int num, uint64_t* out)
+{
+  device_buffer prefix, scratch, rbuf;
+  double total = 0;
+  if (int rc = prob_prefix(s, prefix, scratch, &total)) return rc;
+  std::vector<double> r(num);
+  for (auto& x : r) x = random_upto(g, total);
+  RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&rbuf.p), sizeof(double) * 2 * num));
+  uint64_t* ev = reinterpret_cast<uint64_t*>(rbuf.p + num);
+  RBK_CUDA(cudaMemcpyAsync(rbuf.p, r.data(), sizeof(double) * num, cudaMemcpyHostToDevice, s->stream));
+  RBK_CUDA(rbk::launch_upper_bound(prefix.p, 1ull << s->n, rbuf.p, num, ev, s->stream));
+  ++s->stats.kernel_launches;
+  RBK_CUDA(cudaMemcpyAsync(out, ev, sizeof(uint64_t) * num, cudaMemcpyDeviceToHost, s->stream));
+  if (int rc = bounded_sync(s)) return rc;
+  // upper_bound can land past the end only when r reaches the total (rounding); clamp like the last bin.
+  const uint64_t last = (1ull << s->n) - 1;
+  for (int k = 0; k < num; ++k) if (out[k] > last) out[k] = last;
+  return RBK_OK;
+}
+
+}  // namespace
+
+extern "C" int rbk_state_seed(rbk_state* s, uint64_t seed)
+{
+  if (int rc = check_state(s)) return rc;
+  s->rng.seed(seed);
+  return RBK_OK;
+}
+
+extern "C" int rbk_generate_events(rbk_state* s, int num_events, int64_t seed, uint64_t* events)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (num_events < 0 || (num_events > 0 && !events)) return fail(RBK_ERR_INVALID, "bad event arguments");
+    if (num_events == 0) return RBK_OK;
+    if (seed < 0) return sample_indices(s, s->rng, num_events, events);
+    std::mt19937_64 fresh(static_cast<uint64_t>(seed));  // generate_events.hpp: a generator built from the seed
+    return sample_indices(s, fresh, num_events, events);
+  });
+}
+
+extern "C" int rbk_measure(rbk_state* s, uint64_t* outcome)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!outcome) return fail(RBK_ERR_INVALID, "null output pointer");
+    uint64_t idx = 0;
+    if (int rc = sample_indices(s, s->rng, 1, &idx)) return rc;
+    *outcome = idx;
+    return rbk_state_reset(s, idx);  // measure.hpp: the state becomes |outcome>
+  });
+}
+
+extern "C" int rbk_projective_measurement(rbk_state* s, uint32_t qubit, int* outcome)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!outcome) return fail(RBK_ERR_INVALID, "null output pointer");
+    if (qubit >= static_cast<uint32_t>(s->n)) return fail(RBK_ERR_INVALID, "qubit index out of range");
+    int rc = launch_reduction(s, [&] {
+      return s->precision == RBK_C128 ? rbk::launch_zsum<double>(s->amps, s->n, s->d_partials, s->d_out, s->stream)
+                                      : rbk::launch_zsum<float>(s->amps, s->n, s->d_partials, s->d_out, s->stream);
+    });
+    if (rc) return rc;
+    if ((rc = read_out(s, s->n + 1))) return rc;
+    const double p1 = s->h_out[1 + s->perm[qubit]];
+    const double p0 = s->h_out[0] - p1;
+    const int one = random_upto(s->rng, p0 + p1) < p0 ? 0 : 1;
+    // projective_measurement.hpp: keep the measured half scaled by p^(-1/2), zero the other half.
+    double d[4] = {0, 0, 0, 0};
+    if (one) d[2] = std::pow(p1, -0.5);
+    else d[0] = std::pow(p0, -0.5);
+    *outcome = one;
+    if ((rc = rbk_apply_diagonal2(s, d, qubit, nullptr, 0))) return rc;
+    return flush(s);
   });
 }

@@ -368,3 +368,143 @@ template cudaError_t launch_overlap<double>(const void*, const void*, int, uint6
 template cudaError_t launch_overlap<float>(const void*, const void*, int, uint64_t, uint64_t, double, double, double*, double*, cudaStream_t);
 
 }  // namespace rbk
+
+namespace rbk {
+
+// ---------------------------------------------------------------------------
+// Sampling: inclusive prefix sums of |a_i|^2 and upper_bound searches
+// (the device form of ket::generate_events, ket/include/ket/generate_events.hpp:18-51)
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanPerThread = 16;
+constexpr int kScanChunk = kScanThreads * kScanPerThread;  // values per block
+
+// One block scans kScanChunk consecutive values: out[i] = sum_{j<=i in chunk} v[j],
+// and writes the chunk total to sums[block].  v = |a_i|^2 when amps != nullptr,
+// else v = in[i].
+template <typename Real>
+__global__ void __launch_bounds__(kScanThreads)
+chunk_scan_kernel(const typename ctype<Real>::c* __restrict__ amps, const double* __restrict__ in, uint64_t count,
+                  double* __restrict__ out, double* __restrict__ sums)
+{
+  __shared__ double warp_tot[kScanThreads / 32];
+  const uint64_t base = uint64_t(blockIdx.x) * kScanChunk + uint64_t(threadIdx.x) * kScanPerThread;
+  double v[kScanPerThread];
+  double run = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    const uint64_t i = base + k;
+    double x = 0;
+    if (i < count) {
+      if (amps) { const auto a = amps[i]; x = double(a.x) * double(a.x) + double(a.y) * double(a.y); }
+      else x = in[i];
+    }
+    run += x;
+    v[k] = run;
+  }
+  // exclusive scan of the per-thread totals over the block
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double incl = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  double warp_off = 0, block_tot = 0;
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    if (w < warp) warp_off += warp_tot[w];
+    block_tot += warp_tot[w];
+  }
+  const double off = warp_off + (incl - run);
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    const uint64_t i = base + k;
+    if (i < count) out[i] = v[k] + off;
+  }
+  if (threadIdx.x == 0 && sums) sums[blockIdx.x] = block_tot;
+}
+
+// out[i] += offsets[block of i - 1] (offsets = inclusive scan of the chunk totals)
+__global__ void add_offsets_kernel(double* __restrict__ out, uint64_t count, const double* __restrict__ offsets)
+{
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count; i += stride) {
+    const uint64_t chunk = i / kScanChunk;
+    if (chunk > 0) out[i] += offsets[chunk - 1];
+  }
+}
+
+// events[k] = first index i with prefix[i] > r[k]  (std::upper_bound)
+__global__ void upper_bound_kernel(const double* __restrict__ prefix, uint64_t count, const double* __restrict__ r,
+                                   int num, uint64_t* __restrict__ events)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= num) return;
+  const double x = r[k];
+  uint64_t lo = 0, hi = count;
+  while (lo < hi) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    if (prefix[mid] > x) hi = mid;
+    else lo = mid + 1;
+  }
+  events[k] = lo;
+}
+
+size_t scan_scratch_doubles(uint64_t count)
+{
+  size_t total = 0;
+  uint64_t m = count;
+  while (m > 1) {
+    m = (m + kScanChunk - 1) / kScanChunk;
+    total += m;
+  }
+  return total + 1;
+}
+
+// Inclusive scan of |a|^2 (level 0) with the chunk totals scanned recursively in `scratch`.
+template <typename Real>
+cudaError_t launch_prob_scan(const void* amps, uint64_t count, double* prefix, double* scratch, cudaStream_t stream)
+{
+  // level list: (values, count, out, sums)
+  const double* in = nullptr;
+  const void* a = amps;
+  double* out = prefix;
+  uint64_t m = count;
+  double* level_out[64];
+  uint64_t level_count[64];
+  int levels = 0;
+  double* s = scratch;
+  while (true) {
+    const uint64_t blocks = (m + kScanChunk - 1) / kScanChunk;
+    double* sums = blocks > 1 ? s : nullptr;
+    if (a) chunk_scan_kernel<Real><<<(unsigned)blocks, kScanThreads, 0, stream>>>(static_cast<const typename ctype<Real>::c*>(a), nullptr, m, out, sums);
+    else chunk_scan_kernel<double><<<(unsigned)blocks, kScanThreads, 0, stream>>>(nullptr, in, m, out, sums);
+    level_out[levels] = out;
+    level_count[levels] = m;
+    ++levels;
+    if (blocks <= 1) break;
+    // scan the chunk totals in place: next level reads `sums`, writes into the same array
+    in = sums;
+    a = nullptr;
+    out = sums;
+    m = blocks;
+    s += blocks;
+  }
+  for (int l = levels - 2; l >= 0; --l) {
+    add_offsets_kernel<<<grid_for(level_count[l], 256), 256, 0, stream>>>(level_out[l], level_count[l], level_out[l + 1]);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_upper_bound(const double* prefix, uint64_t count, const double* r, int num, uint64_t* events, cudaStream_t stream)
+{
+  upper_bound_kernel<<<(num + 255) / 256, 256, 0, stream>>>(prefix, count, r, num, events);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_prob_scan<double>(const void*, uint64_t, double*, double*, cudaStream_t);
+template cudaError_t launch_prob_scan<float>(const void*, uint64_t, double*, double*, cudaStream_t);
+
+}  // namespace rbk

@@ -59,4 +59,12 @@ template <typename Real> cudaError_t launch_pauli_apply(const void* src, void* d
 template <typename Real> cudaError_t launch_overlap(const void* lam, const void* psi, int n, uint64_t flip, uint64_t sign,
                                                     double wr, double wi, double* partials, double* out, cudaStream_t stream);
 
+// Sampling: prefix = inclusive scan of |a_i|^2 (scratch: scan_scratch_doubles(count)
+// doubles); events[k] = upper_bound(prefix, r[k]).
+size_t scan_scratch_doubles(uint64_t count);
+template <typename Real> cudaError_t launch_prob_scan(const void* amps, uint64_t count, double* prefix, double* scratch,
+                                                      cudaStream_t stream);
+cudaError_t launch_upper_bound(const double* prefix, uint64_t count, const double* r, int num, uint64_t* events,
+                               cudaStream_t stream);
+
 }  // namespace rbk

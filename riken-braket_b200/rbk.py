@@ -84,6 +84,10 @@ _SIGNATURES = {
     "rbk_expectation_pauli": ([_P, _I, ctypes.c_char_p, _P, _P], _I),
     "rbk_inner_product": ([_P, _P, _P], _I),
     "rbk_fidelity": ([_P, _P, ctypes.POINTER(_D)], _I),
+    "rbk_state_seed": ([_P, _U64], _I),
+    "rbk_generate_events": ([_P, _I, ctypes.c_int64, _P], _I),
+    "rbk_measure": ([_P, ctypes.POINTER(_U64)], _I),
+    "rbk_projective_measurement": ([_P, _U32, ctypes.POINTER(_I)], _I),
 }
 
 
@@ -340,4 +344,29 @@ class State:
     def fidelity(self, other):
         v = ctypes.c_double()
         _check(lib().rbk_fidelity(self.h, other.h, ctypes.byref(v)))
+        return v.value
+
+    # -- sampling and measurement ------------------------------------------------
+    def seed(self, seed):
+        """Re-seeds the state's std::mt19937_64 (bra's initial seed is 1)."""
+        _check(lib().rbk_state_seed(self.h, seed))
+
+    def generate_events(self, num, seed=-1):
+        """ket::generate_events: num basis indices drawn from |a|^2.  seed < 0
+        draws from the state's generator; otherwise a fresh one seeded `seed`.
+        The amplitudes are left unchanged."""
+        out = np.empty(num, dtype=np.uint64)
+        _check(lib().rbk_generate_events(self.h, num, seed, out.ctypes.data))
+        return out
+
+    def measure(self):
+        """ket::measure: one sampled basis index; the state collapses onto it."""
+        v = ctypes.c_uint64()
+        _check(lib().rbk_measure(self.h, ctypes.byref(v)))
+        return v.value
+
+    def projective_measurement(self, qubit):
+        """ket::gate::projective_measurement: outcome 0/1, state renormalised."""
+        v = ctypes.c_int()
+        _check(lib().rbk_projective_measurement(self.h, qubit, ctypes.byref(v)))
         return v.value

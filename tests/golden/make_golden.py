@@ -98,6 +98,24 @@ def main():
     arrays["brick20_spins"] = r.spins()
     meta["brick20"] = {"n": n20, "generator": "brick(20, 10, seed=1)"}
 
+    # 4. Sampling and measurement on random9 (bra's generator starts at seed 1;
+    #    ket::generate_events with a seed builds its own generator).
+    n9, ops9 = circuits["random9"]
+    r = oracle.KetRef(n9)
+    r.apply(ops9)
+    arrays["random9_events_seeded"] = r.generate_events(2000, 5)
+    r = oracle.KetRef(n9)
+    r.apply(ops9)
+    arrays["random9_events_state_rng"] = r.generate_events(2000)
+    r = oracle.KetRef(n9)
+    r.apply(ops9)
+    r.seed(23)
+    arrays["random9_projective_qubits"] = np.array([2, 5, 8, 0], dtype=np.int64)
+    arrays["random9_projective_outcomes"] = np.array(
+        [r.projective_measurement(int(q)) for q in arrays["random9_projective_qubits"]], dtype=np.int64)
+    arrays["random9_projective_amps"] = r.amplitudes()
+    arrays["random9_measure"] = np.array([r.measure()], dtype=np.int64)
+
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **arrays)
     with open(os.path.join(HERE, "cases.json"), "w") as f:
         json.dump(meta, f, indent=0)

@@ -89,6 +89,52 @@ def test_reference_fused_brick_equals_unfused(pkg):
     np.testing.assert_allclose(a.amplitudes(), b.amplitudes(), rtol=0, atol=1e-14)
 
 
+def test_sampling_restatement_matches_reference_fixtures(golden):
+    """MT19937-64 + uniform_real_distribution + upper_bound over the prefix of
+    |a|^2 (generate_events.hpp), projective_measurement.hpp and measure.hpp:
+    indices and outcomes equal, collapsed amplitudes bit-equal."""
+    meta, arr = golden
+    n = meta["random9"]["n"]
+    ops = as_ops(meta["random9"]["ops"])
+
+    def fresh():
+        o = oracle.COracle(n)
+        o.apply(ops)
+        return o
+
+    assert np.array_equal(fresh().generate_events(2000, 5), arr["random9_events_seeded"])
+    assert np.array_equal(fresh().generate_events(2000), arr["random9_events_state_rng"])
+    o = fresh()
+    o.seed(23)
+    outs = [o.projective_measurement(int(q)) for q in arr["random9_projective_qubits"]]
+    assert outs == list(arr["random9_projective_outcomes"])
+    assert np.array_equal(o.amplitudes(), arr["random9_projective_amps"])
+    assert o.measure() == arr["random9_measure"][0]
+
+
+@pytest.mark.skipif(not REF_BUILT, reason="oracle/_ref not built (needs the reference sources)")
+@pytest.mark.parametrize("n", [7, 12])
+def test_sampling_restatement_equals_reference_on_fresh_states(pkg, n):
+    ops = pkg.circuits.random_circuit(n, 250, seed=n)
+    r, o = oracle.KetRef(n), oracle.COracle(n)
+    r.apply(ops)
+    o.apply(ops)
+    r.seed(n)
+    o.seed(n)
+    for q in range(n):
+        assert r.projective_measurement(q) == o.projective_measurement(q)
+    assert np.array_equal(r.amplitudes(), o.amplitudes())
+    r, o = oracle.KetRef(n), oracle.COracle(n)
+    r.apply(ops)
+    o.apply(ops)
+    assert np.array_equal(o.generate_events(5000, 77), r.generate_events(5000, 77))
+    r, o = oracle.KetRef(n), oracle.COracle(n)  # the reference left prefix sums in its buffer
+    r.apply(ops)
+    o.apply(ops)
+    assert r.measure() == o.measure()
+    assert np.array_equal(r.amplitudes(), o.amplitudes())
+
+
 @pytest.mark.parametrize("prog", ["runtime_gate_numerical", "fused_runtime_gate_numerical", "runtime_observable_numerical"])
 def test_reference_own_tests_pass_with_shim(prog):
     """The reference's ket/test/*.cpp, compiled unchanged against oracle/shim."""
