@@ -154,6 +154,39 @@ int rbk_apply_matrix2(rbk_state* s, const double* m, uint32_t target, const uint
 /* diag(d0, d1) on target: d = {d0re, d0im, d1re, d1im}. */
 int rbk_apply_diagonal2(rbk_state* s, const double* d, uint32_t target, const uint32_t* controls, int num_controls);
 
+/* ---- further gate families of ket / bra's instruction set -------------------
+ * adjoint = 0 applies the gate, 1 its adjoint (bra's "+" mnemonics). */
+/* +X / -X: ket::gate::x_rotation_half_pi / adj_ (ket/include/ket/gate/x_rotation_half_pi.hpp:34, :254) */
+int rbk_x_rotation_half_pi(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int num_controls);
+/* +Y / -Y: ket::gate::y_rotation_half_pi / adj_ (y_rotation_half_pi.hpp:33, :251) */
+int rbk_y_rotation_half_pi(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int num_controls);
+/* SX / SX+: ket::gate::sqrt_pauli_x (sqrt_pauli_x.hpp:32, :259) */
+int rbk_sqrt_pauli_x(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int num_controls);
+/* SY / SY+: ket::gate::sqrt_pauli_y (sqrt_pauli_y.hpp:33, :256) */
+int rbk_sqrt_pauli_y(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int num_controls);
+/* SZ, S, SZZ, SZn and their controlled forms: ket::gate::sqrt_pauli_z (sqrt_pauli_z.hpp:55-205,
+ * :428-520): |1> of each target times i (adjoint: -i) where all controls are one. */
+int rbk_sqrt_pauli_z(rbk_state* s, int adjoint, const uint32_t* targets, int num_targets, const uint32_t* controls,
+                     int num_controls);
+/* XX, Xn, YY, ZZ, ... and C...C forms: the product of single-qubit Paulis paulis[k] (one of
+ * "IXYZ") on targets[k] (ket::gate::runtime::ranges::pauli_x/_y/_z, pauli_x.hpp:288-572). */
+int rbk_pauli_string(rbk_state* s, const char* paulis, const uint32_t* targets, int num_targets,
+                     const uint32_t* controls, int num_controls);
+/* EXX, EXn, EYn, EZn, ... and C...C forms: exp(i phase P) for the Pauli product P
+ * (exponential_pauli_x.hpp / _y.hpp / _z.hpp, runtime forms). */
+int rbk_exponential_pauli_string(rbk_state* s, double phase, const char* paulis, const uint32_t* targets, int num_targets,
+                                 const uint32_t* controls, int num_controls);
+/* ESWAP and C...CESWAP: exp(i phase SWAP) (ket/include/ket/gate/exponential_swap.hpp:37-40, :103). */
+int rbk_exponential_swap(rbk_state* s, double phase, uint32_t qubit1, uint32_t qubit2, const uint32_t* controls,
+                         int num_controls);
+/* CLEAR i / SET i: ket::gate::clear / set (clear.hpp, set.hpp): the qubit projected onto
+ * |0> / |1> and the state renormalised. */
+int rbk_clear(rbk_state* s, uint32_t qubit);
+int rbk_set(rbk_state* s, uint32_t qubit);
+/* SHORBOX nx N a: ket::ranges::shor_box (ket/include/ket/shor_box.hpp) with the exponent
+ * register on the top nx qubits; replaces the state.  0 < divisor <= 2^32, base < 2^32. */
+int rbk_shor_box(rbk_state* s, uint32_t num_exponent_qubits, uint64_t divisor, uint64_t base);
+
 /* ---- observables ---------------------------------------------------------- */
 /* sum |a_i|^2 */
 int rbk_norm2(rbk_state* s, double* out);

@@ -1,0 +1,357 @@
+"""TEST INFRASTRUCTURE ONLY: bra's .qcx front end restated in Python, driving
+the reference's own ket code (oracle/_ref/libketref.so through oracle.KetRef).
+
+It checks the engine's C++ interpreter (riken-braket_b200/csrc/qcx.cpp) from
+the other side: an independent parse of the same text (bra/src/interpreter.cpp:
+372-826 and interpret_controlled_gates :3341-3508), executed gate by gate with
+the ket calls bra's nompi_state makes (bra/src/nompi_state.cpp), printing what
+bra::state prints (bra/src/state.cpp:1980-2110) without the timing lines.
+
+Fusion blocks whose gates all have bra fused-gate classes in the reference
+leg run through bra's fusion (ORC codes of oracle_ops.h); other blocks run
+unfused (bra's fused and unfused results agree to rounding,
+ket/test/fused_runtime_gate_numerical.cpp).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+import oracle
+
+# Gate kinds (oracle_ops.h KG_*; the engine's RBK_QCX_* use the same numbers).
+KG = dict(H=1, NOT=2, X=3, Y=4, Z=5, SWAP=6, SX=7, SX_ADJ=8, SY=9, SY_ADJ=10, SZ=11, SZ_ADJ=12, U1=13, U1_ADJ=14,
+          U2=15, U2_ADJ=16, U3=17, U3_ADJ=18, R=19, R_ADJ=20, ROTX=21, ROTX_ADJ=22, ROTY=23, ROTY_ADJ=24, EX=25,
+          EX_ADJ=26, EY=27, EY_ADJ=28, EZ=29, EZ_ADJ=30, ESWAP=31, ESWAP_ADJ=32, TOFFOLI=33, CLEAR=34, SET=35,
+          SHORBOX=36)
+OP = dict(GATE=1, BEGIN_FUSION=2, END_FUSION=3, MEASUREMENT=4, AMPLITUDES=5, GENERATE_EVENTS=6, EXIT=7,
+          PROJECTIVE=8, EXPECTATION=9, PRINT=10, NOOP=11)
+
+CONSTANTS = {":REAL": 0.0, ":IMAG": 0.0, ":PI": math.pi, ":HALF_PI": math.pi / 2, ":TWO_PI": 2 * math.pi,
+             ":ROOT_TWO": math.sqrt(2.0), ":HALF_ROOT_TWO": math.sqrt(0.5)}
+
+
+class QcxError(Exception):
+    pass
+
+
+def _real(tok):
+    if tok[0].isdigit() or tok[0] in "+-.":
+        return float(tok)
+    if tok in CONSTANTS:
+        return CONSTANTS[tok]
+    if tok.startswith(":REAL:") and len(tok) > 6 and (tok[6].isdigit() or tok[6] in "+-."):
+        return float(tok[6:])
+    raise QcxError(f"unsupported value {tok}")
+
+
+def _count(body, letter):
+    """'XXX' -> 3, 'X3' -> 3, else 0."""
+    if not body or body[0] != letter:
+        return 0
+    if set(body) == {letter}:
+        return len(body)
+    if len(body) > 1 and body[1:].isdigit():
+        return int(body[1:])
+    return 0
+
+
+def parse(text):
+    """Returns (num_qubits, initial_state, instructions); each instruction is a
+    dict with op, kind, targets, controls, params, ints, values, text, line."""
+    n, init, code = None, 0, []
+
+    def ins(op, line, **kw):
+        d = dict(op=OP[op], kind=0, targets=[], controls=[], params=[0.0, 0.0, 0.0], ints=[0, 0], values=[], text="",
+                 line=line)
+        d.update(kw)
+        code.append(d)
+
+    def qubit(tok):
+        q = int(tok)
+        if not tok.isdigit() or q >= n:
+            raise QcxError(f"bad qubit {tok}")
+        return q
+
+    def gate(cols, line, kind, nc, nt, npar, exponent=False, all_controls=False):
+        if len(cols) != 1 + nc + nt + npar:
+            raise QcxError(f"line {line}: wrong operand count")
+        qs = [qubit(t) for t in cols[1:1 + nc + nt]]
+        if len(set(qs)) != len(qs):
+            raise QcxError(f"line {line}: repeated qubit")
+        ctl = qs if all_controls else qs[:nc]
+        tgt = [] if all_controls else qs[nc:]
+        params = [0.0, 0.0, 0.0]
+        for k in range(npar):
+            tok = cols[1 + nc + nt + k]
+            params[k] = float(int(tok)) if exponent else _real(tok)
+        ins("GATE", line, kind=KG[kind], targets=tgt, controls=ctl, params=params)
+
+    def plain_or_controlled(cols, line, m, nc):
+        adj = len(m) > 1 and m.endswith("+")
+        base = m[:-1] if adj else m
+        if base in ("I", "IC") and not adj:
+            if len(cols) != 2 + nc:
+                raise QcxError(f"line {line}: wrong operand count")
+            [qubit(t) for t in cols[1:]]
+            ins("NOOP", line)
+            return True
+        if not adj and _count(m, "I") >= 2:
+            if len(cols) != 1 + nc + _count(m, "I"):
+                raise QcxError("arity")
+            ins("NOOP", line)
+            return True
+        if not adj and base in ("H", "NOT"):
+            gate(cols, line, base, nc, 1, 0)
+            return True
+        if not adj and base == "Z":
+            gate(cols, line, "Z", nc, 1, 0, all_controls=True)
+            return True
+        for letter in "XYZ":
+            if not adj and _count(m, letter) >= 1:
+                gate(cols, line, letter, nc, _count(m, letter), 0)
+                return True
+        if not adj and base == "SWAP":
+            gate(cols, line, "SWAP", nc, 2, 0)
+            return True
+        suffix = "_ADJ" if adj else ""
+        if base in ("S", "SZ"):
+            gate(cols, line, "SZ" + suffix, nc, 1, 0, all_controls=True)
+            return True
+        if base.startswith("S") and _count(base[1:], "Z") >= 1:
+            k = _count(base[1:], "Z")
+            gate(cols, line, "SZ" + suffix, nc, k, 0, all_controls=(k == 1))
+            return True
+        if base == "T":
+            gate(cols, line, "R" + suffix, nc, 1, 0, all_controls=True)
+            code[-1]["params"][0] = 3.0
+            return True
+        if base in ("SX", "SY"):
+            gate(cols, line, base + suffix, nc, 1, 0)
+            return True
+        if base == "U1":
+            gate(cols, line, "U1" + suffix, nc, 1, 1, all_controls=True)
+            return True
+        if base in ("U2", "U3"):
+            gate(cols, line, base + suffix, nc, 1, int(base[1]))
+            return True
+        if base == "R":
+            gate(cols, line, "R" + suffix, nc, 1, 1, exponent=True, all_controls=True)
+            return True
+        rot = {"+X": "ROTX", "-X": "ROTX_ADJ", "+Y": "ROTY", "-Y": "ROTY_ADJ"}
+        if not adj and base in rot:
+            gate(cols, line, rot[base], nc, 1, 0)
+            return True
+        if base == "ESWAP":
+            gate(cols, line, "ESWAP" + suffix, nc, 2, 1)
+            return True
+        if base.startswith("E"):
+            for letter in "XYZ":
+                k = _count(base[1:], letter)
+                if k >= 1:
+                    gate(cols, line, "E" + letter + suffix, nc, k, 1)
+                    return True
+        return False
+
+    done = False
+    for line_no, raw in enumerate(text.splitlines(), start=1):
+        if done:
+            break
+        cols = raw.split("!", 1)[0].split()
+        if not cols:
+            continue
+        m = cols[0].upper()
+        word = lambda i: cols[i].upper() if i < len(cols) else ""  # noqa: E731
+        if m == "QUBITS":
+            n = int(cols[1])
+            continue
+        if m == "CIRCUITS":
+            if int(cols[1]) != 1:
+                raise QcxError("several circuits")
+            continue
+        if m == "INITIAL":
+            init = int(cols[2])
+            continue
+        if m == "BIT" or m in ("MPIPROCESSES", "MPISWAPBUFFER"):
+            continue
+        if m == "EXIT":
+            ins("EXIT", line_no)
+            done = True
+        elif m == "BEGIN":
+            if word(1) == "MEASUREMENT":
+                ins("MEASUREMENT", line_no, ints=[3, 0])
+            elif word(1) == "FUSION":
+                ins("BEGIN_FUSION", line_no)
+            else:
+                raise QcxError("BEGIN")
+        elif m == "END":
+            if word(1) != "FUSION":
+                raise QcxError("END")
+            ins("END_FUSION", line_no)
+        elif m == "DO":
+            if word(1) == "MEASUREMENT":
+                ins("MEASUREMENT", line_no, ints=[int(cols[2]) if len(cols) == 3 else 3, 0])
+            elif word(1) == "AMPLITUDES":
+                ins("AMPLITUDES", line_no, values=[int(t) for t in cols[2:]])
+            else:
+                raise QcxError("DO")
+        elif m == "GENERATE":
+            ins("GENERATE_EVENTS", line_no, ints=[int(cols[2]), int(cols[3])])
+            done = True
+        elif m == "EXPECTATION":
+            pauli = cols[1][len(":PAULIS:"):].upper()
+            ins("EXPECTATION", line_no, text=pauli, targets=[qubit(t) for t in cols[2:]])
+        elif m in ("PRINT", "PRINTLN"):
+            ins("PRINT", line_no, text=" ".join(cols[1:]), ints=[int(m == "PRINTLN"), 0])
+        elif m in ("U", "U+"):
+            gate(cols, line_no, "R" if m == "U" else "R_ADJ", 0, 2, 1, exponent=True, all_controls=True)
+        elif m == "TOFFOLI":
+            gate(cols, line_no, "TOFFOLI", 2, 1, 0)
+        elif m == "M":
+            ins("PROJECTIVE", line_no, targets=[qubit(cols[1])])
+        elif m in ("CLEAR", "SET"):
+            gate(cols, line_no, m, 0, 1, 0)
+        elif m == "SHORBOX":
+            nx, div, base = (int(t) for t in cols[1:4])
+            ins("GATE", line_no, kind=KG["SHORBOX"], params=[float(nx), float(div), float(base)], ints=[div, base])
+        elif plain_or_controlled(cols, line_no, m, 0):
+            pass
+        elif m.startswith("C") and len(m) >= 2:
+            cs = len(m) - len(m.lstrip("C"))
+            j = 1
+            while j < len(m) and m[j].isdigit():
+                j += 1
+            if cs > 1:
+                nc, rest = cs, m[cs:]
+            elif j > 1:
+                nc, rest = int(m[1:j]), m[j:]
+            else:
+                nc, rest = 1, m[1:]
+            if nc <= 0 or not rest or not plain_or_controlled(cols, line_no, rest, nc):
+                raise QcxError(f"line {line_no}: unknown mnemonic {m}")
+        else:
+            raise QcxError(f"line {line_no}: unknown mnemonic {m}")
+    if n is None:
+        raise QcxError("no QUBITS")
+    return n, init, code
+
+
+# ---- execution on the reference ----------------------------------------------
+
+_FUSIBLE = {"H", "X", "Y", "U2", "U3", "EX", "EY", "EZ", "SWAP"}
+_NAME = {v: k for k, v in KG.items()}
+
+
+def _as_core(g):
+    """ORC instruction tuple of oracle.encode() if bra fuses this gate in the reference leg, else None."""
+    name, t, c, p = _NAME[g["kind"]], g["targets"], g["controls"], g["params"]
+    if name in ("NOT", "X") and len(t) == 1 and len(c) == 1:
+        return ("CNOT", (c[0], t[0]), ())
+    if name == "Z" and not t and len(c) == 1:
+        return ("Z", (c[0],), ())
+    if name == "Z" and not t and len(c) == 2:
+        return ("CZ", (c[0], c[1]), ())
+    if name == "U1" and len(c) == 1:
+        return ("U1", (c[0],), (p[0],))
+    if name in ("R", "R_ADJ") and len(c) == 2:
+        k = int(p[0])
+        return ("U", (c[0], c[1]), (-k if name == "R_ADJ" else k,))
+    if name in _FUSIBLE and not c and len(t) == (2 if name == "SWAP" else 1):
+        npar = {"U2": 2, "U3": 3, "EX": 1, "EY": 1, "EZ": 1}.get(name, 0)
+        return (name, tuple(t), tuple(p[:npar]))
+    if name == "NOT" and len(t) == 1 and not c:
+        return ("X", tuple(t), ())
+    return None
+
+
+def _g(v, precision=6):
+    """C++ ostream default floating output (printf %g) at the given precision."""
+    return "%.*g" % (precision, v)
+
+
+def _centre(s, width):
+    pad = width - len(s)
+    return s if pad <= 0 else " " * (pad // 2) + s + " " * (pad - pad // 2)
+
+
+def _bits(v, n):
+    return format(v, "0%db" % n) if n else ""
+
+
+def run(text, seed=1, threads=1):
+    """Returns (output text without timing lines, final amplitudes, reference state)."""
+    n, init, code = parse(text)
+    r = oracle.KetRef(n, initial_index=init, threads=threads)
+    r.seed(seed)
+    out = []
+    outcomes = [-1] * n
+    last_measured = 0
+    result = 0j
+    i = 0
+    while i < len(code):
+        ins = code[i]
+        op = ins["op"]
+        if op == OP["BEGIN_FUSION"]:
+            j = i + 1
+            while j < len(code) and code[j]["op"] != OP["END_FUSION"]:
+                j += 1
+            block = code[i + 1:j]
+            cores = [_as_core(g) if g["op"] == OP["GATE"] else None for g in block]
+            if block and all(cores):
+                r.apply([("BEGIN FUSION", (), ())] + cores + [("END FUSION", (), ())])
+                i = j + 1
+                continue
+            i += 1
+            continue
+        if op == OP["END_FUSION"] or op == OP["NOOP"]:
+            pass
+        elif op == OP["GATE"]:
+            r.gate(ins["kind"], ins["targets"], ins["controls"], ins["params"])
+        elif op == OP["MEASUREMENT"]:
+            p = ins["ints"][0]
+            spins = r.spins().reshape(n, 3)
+            out.append("Expectation values of spins:\n")
+            if p > 0:
+                w = max(p + 3, 8)
+                out.append(" ".join(_centre(s, w) for s in ("<Qx>", "<Qy>", "<Qz>")) + "\n")
+                for q in range(n):
+                    out.append(" ".join(_centre("% .*f" % (p, 0.5 - spins[q, k]), w) for k in range(3)) + "\n")
+            else:
+                out.append("<Qx> <Qy> <Qz>\n")
+                prec = -p if p < 0 else 6
+                for q in range(n):
+                    out.append(" ".join(_g(0.5 - spins[q, k], prec) for k in range(3)) + "\n")
+        elif op == OP["AMPLITUDES"]:
+            a = r.amplitudes()
+            idx = ins["values"] or range(1 << n)
+            for k in idx:
+                out.append("%s => %s + %s i\n" % (_bits(k, n), _g(a[k].real), _g(a[k].imag)))
+        elif op == OP["GENERATE_EVENTS"]:
+            ev = r.generate_events(ins["ints"][0], ins["ints"][1])
+            out.append("Events:\n")
+            out.extend("%d %s\n" % (k, _bits(int(e), n)) for k, e in enumerate(ev))
+        elif op == OP["EXIT"]:
+            out.append("Measurement result: %d\n" % r.measure())
+        elif op == OP["PROJECTIVE"]:
+            q = ins["targets"][0]
+            outcomes[q] = r.projective_measurement(q)
+            last_measured = q
+        elif op == OP["EXPECTATION"]:
+            result = r.expectation_on(ins["text"], ins["targets"])
+        elif op == OP["PRINT"]:
+            parts = []
+            for a in ins["text"].split():
+                if a[0].isdigit() or a[0] in "+-.":
+                    parts.append(a)
+                elif a == ":RESULT":
+                    parts.append("(%s,%s)" % (_g(result.real), _g(result.imag)))
+                elif a == ":OUTCOME":
+                    parts.append(str(outcomes[last_measured]))
+                elif a.startswith(":OUTCOMES:"):
+                    parts.append(str(outcomes[int(a[10:])]))
+                elif a in CONSTANTS:
+                    parts.append(_g(CONSTANTS[a]))
+            out.append(" ".join(parts) + ("\n" if ins["ints"][0] else ""))
+        i += 1
+    return "".join(out), r.amplitudes(), r

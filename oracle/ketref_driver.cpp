@@ -54,6 +54,16 @@
 #include <ket/gate/exponential_pauli_x.hpp>
 #include <ket/gate/exponential_pauli_y.hpp>
 #include <ket/gate/exponential_pauli_z.hpp>
+#include <ket/gate/exponential_swap.hpp>
+#include <ket/gate/sqrt_pauli_x.hpp>
+#include <ket/gate/sqrt_pauli_y.hpp>
+#include <ket/gate/sqrt_pauli_z.hpp>
+#include <ket/gate/x_rotation_half_pi.hpp>
+#include <ket/gate/y_rotation_half_pi.hpp>
+#include <ket/gate/toffoli.hpp>
+#include <ket/gate/clear.hpp>
+#include <ket/gate/set.hpp>
+#include <ket/shor_box.hpp>
 #include <ket/gate/utility/index_with_qubits.hpp>
 #include <ket/gate/utility/pauli_index_coeff.hpp>
 #include <ket/all_spin_expectation_values.hpp>
@@ -292,6 +302,201 @@ void apply_one(ref_state& s, oracle_op const& op)
   }
 }
 
+// The wider instruction set, unfused, following bra's nompi_state dispatch
+// (bra/src/nompi_state.cpp:326-1280 and :1359-2600): one target and at most one
+// control use ket::gate::ranges::X, everything else the runtime forms
+// ket::gate::runtime::ranges::X(targets, controls).
+struct gate_args
+{
+  std::vector<qubit_t> t;
+  std::vector<control_t> c;
+  double const* p;
+};
+
+template <typename One, typename OneCtl, typename Many>
+void dispatch_target(gate_args const& a, One one, OneCtl one_ctl, Many many)
+{
+  if (a.t.size() == 1 && a.c.empty()) one(a.t[0]);
+  else if (a.t.size() == 1 && a.c.size() == 1) one_ctl(a.t[0], a.c[0]);
+  else many(a.t, a.c);
+}
+
+// Gates on control-type qubits only (Z, SZ, U1, R): 1 or 2 qubits use the
+// variadic forms, more the runtime form over all of them.
+template <typename One, typename Two, typename Many>
+void dispatch_controls(gate_args const& a, One one, Two two, Many many)
+{
+  if (a.c.size() == 1) one(a.c[0]);
+  else if (a.c.size() == 2) two(a.c[0], a.c[1]);
+  else many(a.c);
+}
+
+#define KR ket::gate::ranges
+#define KRT ket::gate::runtime::ranges
+
+void apply_gate(ref_state& s, int kind, gate_args const& a)
+{
+  auto& P = s.policy;
+  auto& D = s.data;
+  double const* p = a.p;
+  switch (kind)
+  {
+   case KG_H:
+    dispatch_target(a, [&](qubit_t t) { KR::hadamard(P, D, t); }, [&](qubit_t t, control_t c) { KR::hadamard(P, D, t, c); },
+                    [&](auto const& t, auto const& c) { KRT::hadamard(P, D, t.at(0), c); });
+    break;
+   case KG_NOT:
+    dispatch_target(a, [&](qubit_t t) { KR::not_(P, D, t); }, [&](qubit_t t, control_t c) { KR::not_(P, D, t, c); },
+                    [&](auto const& t, auto const& c) { KRT::not_(P, D, t.at(0), c); });
+    break;
+   case KG_X:
+    if (a.c.empty() && a.t.size() == 2) KR::pauli_x(P, D, a.t[0], a.t[1]);
+    else if (a.c.empty() && a.t.size() > 2) KRT::pauli_x(P, D, a.t);
+    else dispatch_target(a, [&](qubit_t t) { KR::pauli_x(P, D, t); }, [&](qubit_t t, control_t c) { KR::pauli_x(P, D, t, c); },
+                         [&](auto const& t, auto const& c) { KRT::pauli_x(P, D, t, c); });
+    break;
+   case KG_Y:
+    if (a.c.empty() && a.t.size() == 2) KR::pauli_y(P, D, a.t[0], a.t[1]);
+    else if (a.c.empty() && a.t.size() > 2) KRT::pauli_y(P, D, a.t);
+    else dispatch_target(a, [&](qubit_t t) { KR::pauli_y(P, D, t); }, [&](qubit_t t, control_t c) { KR::pauli_y(P, D, t, c); },
+                         [&](auto const& t, auto const& c) { KRT::pauli_y(P, D, t, c); });
+    break;
+   case KG_Z:
+    if (a.t.empty())
+      dispatch_controls(a, [&](control_t c) { KR::pauli_z(P, D, c); }, [&](control_t c1, control_t c2) { KR::pauli_z(P, D, c1, c2); },
+                        [&](auto const& c) { KRT::pauli_z(P, D, c); });
+    else if (a.c.empty() && a.t.size() == 2) KR::pauli_z(P, D, a.t[0], a.t[1]);
+    else if (a.c.empty()) KRT::pauli_z(P, D, a.t);
+    else KRT::pauli_z(P, D, a.t, a.c);
+    break;
+   case KG_SWAP:
+    if (a.c.empty()) KR::swap(P, D, a.t.at(0), a.t.at(1));
+    else KRT::swap(P, D, a.t.at(0), a.t.at(1), a.c);
+    break;
+#define KG_TARGET_GATE(CODE, NAME)                                                                                       \
+   case CODE:                                                                                                            \
+    dispatch_target(a, [&](qubit_t t) { KR::NAME(P, D, t); }, [&](qubit_t t, control_t c) { KR::NAME(P, D, t, c); },       \
+                    [&](auto const& t, auto const& c) { KRT::NAME(P, D, t.at(0), c); });                                \
+    break;
+   KG_TARGET_GATE(KG_SX, sqrt_pauli_x)
+   KG_TARGET_GATE(KG_SX_ADJ, adj_sqrt_pauli_x)
+   KG_TARGET_GATE(KG_SY, sqrt_pauli_y)
+   KG_TARGET_GATE(KG_SY_ADJ, adj_sqrt_pauli_y)
+   KG_TARGET_GATE(KG_ROTX, x_rotation_half_pi)
+   KG_TARGET_GATE(KG_ROTX_ADJ, adj_x_rotation_half_pi)
+   KG_TARGET_GATE(KG_ROTY, y_rotation_half_pi)
+   KG_TARGET_GATE(KG_ROTY_ADJ, adj_y_rotation_half_pi)
+#undef KG_TARGET_GATE
+   case KG_SZ: case KG_SZ_ADJ:
+   {
+    bool const adj = kind == KG_SZ_ADJ;
+    if (a.t.empty())
+      dispatch_controls(a,
+                        [&](control_t c) { if (adj) KR::adj_sqrt_pauli_z(P, D, c); else KR::sqrt_pauli_z(P, D, c); },
+                        [&](control_t c1, control_t c2) { if (adj) KR::adj_sqrt_pauli_z(P, D, c1, c2); else KR::sqrt_pauli_z(P, D, c1, c2); },
+                        [&](auto const& c) { if (adj) KRT::adj_sqrt_pauli_z(P, D, c); else KRT::sqrt_pauli_z(P, D, c); });
+    else if (a.c.empty() && a.t.size() == 2)
+    { if (adj) KR::adj_sqrt_pauli_z(P, D, a.t[0], a.t[1]); else KR::sqrt_pauli_z(P, D, a.t[0], a.t[1]); }
+    else if (a.c.empty())
+    { if (adj) KRT::adj_sqrt_pauli_z(P, D, a.t); else KRT::sqrt_pauli_z(P, D, a.t); }
+    else
+    { if (adj) KRT::adj_sqrt_pauli_z(P, D, a.t, a.c); else KRT::sqrt_pauli_z(P, D, a.t, a.c); }
+    break;
+   }
+   case KG_U1: case KG_U1_ADJ:
+   {
+    bool const adj = kind == KG_U1_ADJ;
+    dispatch_controls(a,
+                      [&](control_t c) { if (adj) KR::adj_phase_shift(P, D, p[0], c); else KR::phase_shift(P, D, p[0], c); },
+                      [&](control_t c1, control_t c2) { if (adj) KR::adj_phase_shift(P, D, p[0], c1, c2); else KR::phase_shift(P, D, p[0], c1, c2); },
+                      [&](auto const& c) { if (adj) KRT::adj_phase_shift(P, D, p[0], c); else KRT::phase_shift(P, D, p[0], c); });
+    break;
+   }
+   case KG_R: case KG_R_ADJ:  // bra::state::phase_shift: phase_coefficients_[k], negative k = adjoint
+   {
+    int k = static_cast<int>(p[0]);
+    bool adj = kind == KG_R_ADJ;
+    if (k < 0) { k = -k; adj = !adj; }
+    complex_t const coeff = s.phase_table.at(static_cast<std::size_t>(k));
+    dispatch_controls(a,
+                      [&](control_t c) { if (adj) KR::adj_phase_shift_coeff(P, D, coeff, c); else KR::phase_shift_coeff(P, D, coeff, c); },
+                      [&](control_t c1, control_t c2) { if (adj) KR::adj_phase_shift_coeff(P, D, coeff, c1, c2); else KR::phase_shift_coeff(P, D, coeff, c1, c2); },
+                      [&](auto const& c) { if (adj) KRT::adj_phase_shift_coeff(P, D, coeff, c); else KRT::phase_shift_coeff(P, D, coeff, c); });
+    break;
+   }
+   case KG_U2: case KG_U2_ADJ:
+   {
+    bool const adj = kind == KG_U2_ADJ;
+    dispatch_target(a,
+                    [&](qubit_t t) { if (adj) KR::adj_phase_shift2(P, D, p[0], p[1], t); else KR::phase_shift2(P, D, p[0], p[1], t); },
+                    [&](qubit_t t, control_t c) { if (adj) KR::adj_phase_shift2(P, D, p[0], p[1], t, c); else KR::phase_shift2(P, D, p[0], p[1], t, c); },
+                    [&](auto const& t, auto const& c) { if (adj) KRT::adj_phase_shift2(P, D, p[0], p[1], t.at(0), c); else KRT::phase_shift2(P, D, p[0], p[1], t.at(0), c); });
+    break;
+   }
+   case KG_U3: case KG_U3_ADJ:
+   {
+    bool const adj = kind == KG_U3_ADJ;
+    dispatch_target(a,
+                    [&](qubit_t t) { if (adj) KR::adj_phase_shift3(P, D, p[0], p[1], p[2], t); else KR::phase_shift3(P, D, p[0], p[1], p[2], t); },
+                    [&](qubit_t t, control_t c) { if (adj) KR::adj_phase_shift3(P, D, p[0], p[1], p[2], t, c); else KR::phase_shift3(P, D, p[0], p[1], p[2], t, c); },
+                    [&](auto const& t, auto const& c) { if (adj) KRT::adj_phase_shift3(P, D, p[0], p[1], p[2], t.at(0), c); else KRT::phase_shift3(P, D, p[0], p[1], p[2], t.at(0), c); });
+    break;
+   }
+#define KG_EXP_GATE(CODE, ADJCODE, NAME)                                                                                 \
+   case CODE: case ADJCODE:                                                                                              \
+   {                                                                                                                     \
+    bool const adj = kind == ADJCODE;                                                                                    \
+    if (a.c.empty() && a.t.size() == 1)                                                                                  \
+    { if (adj) KR::adj_##NAME(P, D, p[0], a.t[0]); else KR::NAME(P, D, p[0], a.t[0]); }                                  \
+    else if (a.c.empty() && a.t.size() == 2)                                                                             \
+    { if (adj) KR::adj_##NAME(P, D, p[0], a.t[0], a.t[1]); else KR::NAME(P, D, p[0], a.t[0], a.t[1]); }                  \
+    else if (a.c.size() == 1 && a.t.size() == 1)                                                                         \
+    { if (adj) KR::adj_##NAME(P, D, p[0], a.t[0], a.c[0]); else KR::NAME(P, D, p[0], a.t[0], a.c[0]); }                  \
+    else if (a.c.empty())                                                                                                \
+    { if (adj) KRT::adj_##NAME(P, D, p[0], a.t); else KRT::NAME(P, D, p[0], a.t); }                                      \
+    else                                                                                                                 \
+    { if (adj) KRT::adj_##NAME(P, D, p[0], a.t, a.c); else KRT::NAME(P, D, p[0], a.t, a.c); }                            \
+    break;                                                                                                               \
+   }
+   KG_EXP_GATE(KG_EX, KG_EX_ADJ, exponential_pauli_x)
+   KG_EXP_GATE(KG_EY, KG_EY_ADJ, exponential_pauli_y)
+   KG_EXP_GATE(KG_EZ, KG_EZ_ADJ, exponential_pauli_z)
+#undef KG_EXP_GATE
+   case KG_ESWAP: case KG_ESWAP_ADJ:
+   {
+    bool const adj = kind == KG_ESWAP_ADJ;
+    if (a.c.empty())
+    { if (adj) KR::adj_exponential_swap(P, D, p[0], a.t.at(0), a.t.at(1)); else KR::exponential_swap(P, D, p[0], a.t.at(0), a.t.at(1)); }
+    else
+    { if (adj) KRT::adj_exponential_swap(P, D, p[0], a.t.at(0), a.t.at(1), a.c); else KRT::exponential_swap(P, D, p[0], a.t.at(0), a.t.at(1), a.c); }
+    break;
+   }
+   case KG_TOFFOLI:
+    KR::toffoli(P, D, a.t.at(0), a.c.at(0), a.c.at(1));
+    break;
+   case KG_CLEAR:
+    KR::clear(P, D, a.t.at(0));
+    break;
+   case KG_SET:
+    KR::set(P, D, a.t.at(0));
+    break;
+   case KG_SHORBOX:  // p = {nx, divisor, base}; exponent qubits on top (bra/src/state.cpp shor_box)
+   {
+    auto const nx = static_cast<unsigned>(p[0]);
+    std::vector<qubit_t> ex, mod;
+    for (unsigned q = s.n - nx; q < s.n; ++q) ex.push_back(qb(static_cast<int>(q)));
+    for (unsigned q = 0; q < s.n - nx; ++q) mod.push_back(qb(static_cast<int>(q)));
+    ket::ranges::shor_box(P, D, static_cast<bra::state_integer_type>(p[2]), static_cast<bra::state_integer_type>(p[1]), ex, mod);
+    break;
+   }
+   default:
+    throw std::invalid_argument("ketref: unsupported gate kind");
+  }
+}
+
+#undef KR
+#undef KRT
+
 thread_local std::string g_error;
 
 } // namespace
@@ -424,6 +629,59 @@ std::uint64_t ketref_measure(void* h)
 {
   auto& s = *static_cast<ref_state*>(h);
   return static_cast<std::uint64_t>(ket::ranges::measure(ket::utility::policy::make_sequential(), s.data, s.rng));
+}
+
+// EXPECTATION :PAULIS:<s> q_0 ... q_{m-1}: bra::nompi_state::do_expectation_value
+// (bra/src/nompi_state.cpp:1155-1202) with the operated qubits as listed.
+void ketref_expectation_on(void* h, char const* pauli, int num_qubits, int const* qubits, double* out)
+{
+  auto& s = *static_cast<ref_state*>(h);
+  std::string const str(pauli, static_cast<std::size_t>(num_qubits));
+  std::vector<qubit_t> operated;
+  for (int i = 0; i < num_qubits; ++i) operated.push_back(qb(qubits[i]));
+  auto const nq = operated.size();
+  auto const value = ket::runtime::ranges::expectation_value(
+    s.policy, s.data,
+    [&str, nq](auto const first, auto const index_wo_qubits,
+               auto const& unsorted_qubits_or_masks, auto const& sorted_qubits_or_index_masks)
+    {
+      complex_t acc{};
+      auto const last_index = bra::state_integer_type{1} << nq;
+      for (auto index = bra::state_integer_type{0}; index < last_index; ++index)
+      {
+        auto const it = first + ket::gate::utility::index_with_qubits(
+          index_wo_qubits, index,
+          std::begin(unsorted_qubits_or_masks), std::end(unsorted_qubits_or_masks),
+          std::begin(sorted_qubits_or_index_masks), std::end(sorted_qubits_or_index_masks));
+        auto const other = ket::gate::utility::pauli_index_coeff<complex_t>(str, index);
+        auto const other_it = first + ket::gate::utility::index_with_qubits(
+          index_wo_qubits, other.first,
+          std::begin(unsorted_qubits_or_masks), std::end(unsorted_qubits_or_masks),
+          std::begin(sorted_qubits_or_index_masks), std::end(sorted_qubits_or_index_masks));
+        acc += std::conj(*it) * (other.second * *other_it);
+      }
+      return acc;
+    },
+    operated);
+  out[0] = value.real();
+  out[1] = value.imag();
+}
+
+// One gate of the wider instruction set (kinds in oracle_ops.h).
+int ketref_gate(void* h, int kind, int num_targets, int const* targets, int num_controls, int const* controls,
+                double const* params)
+{
+  auto& s = *static_cast<ref_state*>(h);
+  try
+  {
+    gate_args a;
+    for (int i = 0; i < num_targets; ++i) a.t.push_back(qb(targets[i]));
+    for (int i = 0; i < num_controls; ++i) a.c.push_back(cq(controls[i]));
+    a.p = params;
+    apply_gate(s, kind, a);
+  }
+  catch (std::exception const& e) { g_error = e.what(); return -1; }
+  return 0;
 }
 
 // M q (bra/src/nompi_state.cpp:1102-1103).

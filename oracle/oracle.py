@@ -79,6 +79,10 @@ class KetRef:
                                            ctypes.c_void_p, ctypes.c_void_p]
         lib.ketref_inner_product.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.ketref_seed.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        lib.ketref_gate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_void_p]
+        lib.ketref_expectation_on.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_void_p]
         lib.ketref_generate_events.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p]
         lib.ketref_measure.argtypes = [ctypes.c_void_p]
         lib.ketref_measure.restype = ctypes.c_uint64
@@ -134,6 +138,23 @@ class KetRef:
 
     def seed(self, seed):
         self.lib.ketref_seed(self.h, seed)
+
+    def gate(self, kind, targets=(), controls=(), params=(0.0, 0.0, 0.0)):
+        """One gate of bra's wider instruction set (kinds KG_* of oracle_ops.h),
+        dispatched as bra::nompi_state does."""
+        t = np.ascontiguousarray(list(targets) or [0], dtype=np.int32)
+        c = np.ascontiguousarray(list(controls) or [0], dtype=np.int32)
+        p = np.zeros(3, dtype=np.float64)
+        p[:len(params)] = params
+        if self.lib.ketref_gate(self.h, kind, len(targets), t.ctypes.data, len(controls), c.ctypes.data, p.ctypes.data) != 0:
+            raise RuntimeError(self.lib.ketref_last_error().decode())
+
+    def expectation_on(self, pauli, qubits):
+        """bra's EXPECTATION :PAULIS:<pauli> q_0 ... (character k acts on qubits[k])."""
+        q = np.ascontiguousarray(list(qubits), dtype=np.int32)
+        out = np.empty(2, dtype=np.float64)
+        self.lib.ketref_expectation_on(self.h, pauli.encode(), len(qubits), q.ctypes.data, out.ctypes.data)
+        return complex(out[0], out[1])
 
     def generate_events(self, num, seed=-1):
         """Like the reference, this overwrites the amplitudes with prefix sums."""

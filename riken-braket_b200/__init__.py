@@ -7,5 +7,5 @@ workload generators (circuits.py) and the adjoint-gradient harness.  The
 directory name is not a Python identifier; load it with ``load_package()``
 from __graft_entry__.py (or importlib) under the name ``riken_braket_b200``.
 """
-from . import adjoint, circuits, rbk  # noqa: F401
+from . import adjoint, circuits, qcx, rbk  # noqa: F401
 from .rbk import C64, C128, RbkError, State  # noqa: F401

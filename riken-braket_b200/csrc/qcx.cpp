@@ -1,0 +1,885 @@
+// qcx.cpp -- bra's .qcx interpreter over the C ABI of the engine (rbk_qcx.h).
+//
+// Parsing restates bra::interpreter::invoke (bra/src/interpreter.cpp:372-826)
+// and its column readers; the controlled-gate prefixes C..C / Cn follow
+// interpret_controlled_gates (:3341-3508).  Execution restates the nompi
+// bra::state methods (bra/src/state.cpp:1980-2110) on an rbk_state: every gate
+// becomes one or a few queued engine gates, and the printing reproduces bra's
+// text line for line.
+#include "rbk_qcx.h"
+
+#include <algorithm>
+#include <cctype>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iomanip>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace rbk {
+int set_last_error(int code, const char* msg);
+}
+
+struct rbk_qcx_program {
+  int num_qubits = -1;
+  uint64_t initial_state = 0;
+  std::vector<rbk_qcx_instruction> code;
+  std::vector<std::vector<uint64_t>> amplitude_lists;  // DO AMPLITUDES index lists, by instruction
+};
+
+namespace {
+
+using columns = std::vector<std::string>;
+
+struct qcx_error : std::runtime_error {
+  int code;
+  qcx_error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void bad(const std::string& m) { throw qcx_error(RBK_ERR_INVALID, m); }
+[[noreturn]] void unsupported(const std::string& m) { throw qcx_error(RBK_ERR_UNSUPPORTED, m); }
+
+std::string upper(std::string s)
+{
+  for (auto& c : s) c = static_cast<char>(std::toupper(static_cast<unsigned char>(c)));
+  return s;
+}
+
+bool all_of_char(const std::string& s, size_t from, char c)
+{
+  return s.size() > from && std::all_of(s.begin() + from, s.end(), [c](char x) { return x == c; });
+}
+
+bool all_digits(const std::string& s, size_t from, size_t to)
+{
+  return to > from && std::all_of(s.begin() + from, s.begin() + to, [](char x) { return std::isdigit(static_cast<unsigned char>(x)); });
+}
+
+// boost::lexical_cast<unsigned> / <int> / <double>: the whole column must convert.
+uint64_t to_unsigned(const std::string& s)
+{
+  if (s.empty() || !std::all_of(s.begin(), s.end(), [](char x) { return std::isdigit(static_cast<unsigned char>(x)); }))
+    bad("expected a non-negative integer, got '" + s + "'");
+  errno = 0;
+  const unsigned long long v = std::strtoull(s.c_str(), nullptr, 10);
+  if (errno) bad("integer out of range: '" + s + "'");
+  return v;
+}
+
+int64_t to_int(const std::string& s)
+{
+  size_t i = (!s.empty() && (s[0] == '+' || s[0] == '-')) ? 1 : 0;
+  if (s.size() == i || !std::all_of(s.begin() + i, s.end(), [](char x) { return std::isdigit(static_cast<unsigned char>(x)); }))
+    bad("expected an integer, got '" + s + "'");
+  return std::strtoll(s.c_str(), nullptr, 10);
+}
+
+double parse_double(const std::string& s)
+{
+  char* end = nullptr;
+  const double v = std::strtod(s.c_str(), &end);
+  if (s.empty() || end != s.c_str() + s.size()) bad("expected a number, got '" + s + "'");
+  return v;
+}
+
+// bra::state::to_real (bra/src/state.cpp:771-800) for literals and built-in constants.
+double to_real(const std::string& s)
+{
+  if (s.empty()) bad("empty value");
+  const char f = s.front();
+  if (std::isdigit(static_cast<unsigned char>(f)) || f == '+' || f == '-' || f == '.') return parse_double(s);
+  if (s == ":REAL" || s == ":IMAG") return 0.0;
+  if (s == ":PI") return 3.141592653589793238462643383279502884;
+  if (s == ":HALF_PI") return 1.570796326794896619231321691639751442;
+  if (s == ":TWO_PI") return 6.283185307179586476925286766559005768;
+  if (s == ":ROOT_TWO") return 1.414213562373095048801688724209698079;
+  if (s == ":HALF_ROOT_TWO") return 0.7071067811865475244008443621048490393;
+  if (s.rfind(":REAL:", 0) == 0 && s.size() > 6) {
+    const std::string rest = s.substr(6);
+    const char g = rest.front();
+    if (std::isdigit(static_cast<unsigned char>(g)) || g == '+' || g == '-' || g == '.') return parse_double(rest);
+  }
+  unsupported("classical variables are not supported ('" + s + "')");
+}
+
+// Phase exponent of R / U / T: an integer literal (bra's int_visitor).
+int64_t to_phase_exponent(const std::string& s)
+{
+  if (!s.empty() && s.front() == ':') unsupported("classical variables are not supported ('" + s + "')");
+  return to_int(s);
+}
+
+rbk_qcx_instruction blank(int op, int line)
+{
+  rbk_qcx_instruction in;
+  std::memset(&in, 0, sizeof(in));
+  in.op = op;
+  in.line = line;
+  return in;
+}
+
+struct parser {
+  rbk_qcx_program& prog;
+  int line = 0;
+  bool done = false;
+
+  uint32_t qubit(const std::string& s)
+  {
+    const uint64_t q = to_unsigned(s);
+    if (prog.num_qubits < 0) bad("QUBITS must come before the first gate");
+    if (q >= static_cast<uint64_t>(prog.num_qubits)) bad("qubit " + s + " is out of range");
+    return static_cast<uint32_t>(q);
+  }
+
+  void expect(const columns& c, size_t n)
+  {
+    if (c.size() != n) bad("'" + c[0] + "' expects " + std::to_string(n - 1) + " operands, got " + std::to_string(c.size() - 1));
+  }
+
+  // A gate: controls first, then targets, then nparams angle columns (or a phase exponent).
+  void gate(const columns& c, int kind, int nc, int nt, int nparams, bool exponent = false, bool all_controls = false)
+  {
+    expect(c, 1 + nc + nt + nparams);
+    auto in = blank(RBK_QCX_GATE, line);
+    in.kind = kind;
+    if (nc + nt > RBK_QCX_MAX_QUBITS) bad("too many qubits");
+    std::vector<uint32_t> seen;
+    for (int i = 0; i < nc + nt; ++i) {
+      const uint32_t q = qubit(c[1 + i]);
+      if (std::find(seen.begin(), seen.end(), q) != seen.end()) bad("qubit " + c[1 + i] + " appears twice");
+      seen.push_back(q);
+      if (i < nc || all_controls) in.controls[in.num_controls++] = q;
+      else in.targets[in.num_targets++] = q;
+    }
+    for (int k = 0; k < nparams; ++k) {
+      const std::string& v = c[1 + nc + nt + k];
+      in.params[k] = exponent ? static_cast<double>(to_phase_exponent(v)) : to_real(v);
+    }
+    prog.code.push_back(in);
+  }
+
+  void noop(const columns& c, int nqubits)
+  {
+    expect(c, 1 + nqubits);
+    for (int i = 0; i < nqubits; ++i) qubit(c[1 + i]);
+    prog.code.push_back(blank(RBK_QCX_NOOP, line));
+  }
+
+  // Number of repeated letters ("XXX" -> 3) or explicit count ("X3" -> 3) after the
+  // first `skip` characters; 0 if the mnemonic has neither form.
+  static int multiplicity(const std::string& m, size_t skip, char letter, bool adjoint)
+  {
+    const size_t end = m.size() - (adjoint ? 1 : 0);
+    if (end <= skip) return 0;
+    const std::string body = m.substr(skip, end - skip);
+    if (body.empty() || body[0] != letter) return 0;
+    if (all_of_char(body, 0, letter)) return static_cast<int>(body.size());
+    if (all_digits(body, 1, body.size())) return std::atoi(body.c_str() + 1);
+    return 0;
+  }
+
+  // Gates that can carry control prefixes; nc = number of controls (0: plain).
+  // Returns false if the mnemonic is not a gate.
+  bool gate_mnemonic(const columns& c, const std::string& m, int nc)
+  {
+    const bool adj = m.size() > 1 && m.back() == '+';
+    const std::string base = adj ? m.substr(0, m.size() - 1) : m;
+    if (base == "I") { noop(c, nc + 1); return true; }
+    if (base == "IC") { noop(c, nc + 1); return true; }
+    if (int k = multiplicity(m, 0, 'I', false); k >= 2 && !adj) { noop(c, nc + k); return true; }
+    if (base == "H" && !adj) { gate(c, RBK_QCX_H, nc, 1, 0); return true; }
+    if (base == "NOT" && !adj) { gate(c, RBK_QCX_NOT, nc, 1, 0); return true; }
+    for (char p : {'X', 'Y'}) {
+      if (adj) break;
+      const int kind = p == 'X' ? RBK_QCX_X : RBK_QCX_Y;
+      if (base.size() == 1 && base[0] == p) { gate(c, kind, nc, 1, 0); return true; }
+      if (int k = multiplicity(m, 0, p, false); k >= 1) { gate(c, kind, nc, k, 0); return true; }
+    }
+    if (!adj && base == "Z") {  // Z c, CZ c1 c2, CnZ: every qubit of control type
+      gate(c, RBK_QCX_Z, nc, 1, 0, false, true);
+      return true;
+    }
+    if (!adj) {
+      if (int k = multiplicity(m, 0, 'Z', false); k >= 1) { gate(c, RBK_QCX_Z, nc, k, 0); return true; }
+    }
+    if (base == "SWAP" && !adj) { gate(c, RBK_QCX_SWAP, nc, 2, 0); return true; }
+    if (base == "S" || base == "SZ") { gate(c, adj ? RBK_QCX_SZ_ADJ : RBK_QCX_SZ, nc, 1, 0, false, true); return true; }
+    if (int k = multiplicity(m, 1, 'Z', adj); k >= 1 && m[0] == 'S') {  // SZZ, SZ..Z, SZn (+)
+      gate(c, adj ? RBK_QCX_SZ_ADJ : RBK_QCX_SZ, nc, k, 0, false, k == 1);
+      return true;
+    }
+    if (base == "T") {  // bra::gate::t_gate: phase_shift(3, c) (bra/src/t_gate.cpp)
+      gate(c, adj ? RBK_QCX_R_ADJ : RBK_QCX_R, nc, 1, 0, false, true);
+      prog.code.back().params[0] = 3;
+      return true;
+    }
+    if (base == "SX") { gate(c, adj ? RBK_QCX_SX_ADJ : RBK_QCX_SX, nc, 1, 0); return true; }
+    if (base == "SY") { gate(c, adj ? RBK_QCX_SY_ADJ : RBK_QCX_SY, nc, 1, 0); return true; }
+    if (base == "U1") { gate(c, adj ? RBK_QCX_U1_ADJ : RBK_QCX_U1, nc, 1, 1, false, true); return true; }
+    if (base == "U2") { gate(c, adj ? RBK_QCX_U2_ADJ : RBK_QCX_U2, nc, 1, 2); return true; }
+    if (base == "U3") { gate(c, adj ? RBK_QCX_U3_ADJ : RBK_QCX_U3, nc, 1, 3); return true; }
+    if (base == "R") { gate(c, adj ? RBK_QCX_R_ADJ : RBK_QCX_R, nc, 1, 1, true, true); return true; }
+    if (base == "+X" && !adj) { gate(c, RBK_QCX_ROTX, nc, 1, 0); return true; }
+    if (base == "-X" && !adj) { gate(c, RBK_QCX_ROTX_ADJ, nc, 1, 0); return true; }
+    if (base == "+Y" && !adj) { gate(c, RBK_QCX_ROTY, nc, 1, 0); return true; }
+    if (base == "-Y" && !adj) { gate(c, RBK_QCX_ROTY_ADJ, nc, 1, 0); return true; }
+    if (base == "ESWAP") { gate(c, adj ? RBK_QCX_ESWAP_ADJ : RBK_QCX_ESWAP, nc, 2, 1); return true; }
+    if (m.size() >= 2 && m[0] == 'E') {
+      const int kinds[3][2] = {{RBK_QCX_EX, RBK_QCX_EX_ADJ}, {RBK_QCX_EY, RBK_QCX_EY_ADJ}, {RBK_QCX_EZ, RBK_QCX_EZ_ADJ}};
+      const char letters[3] = {'X', 'Y', 'Z'};
+      for (int l = 0; l < 3; ++l) {
+        if (int k = multiplicity(m, 1, letters[l], adj); k >= 1) {
+          gate(c, kinds[l][adj ? 1 : 0], nc, k, 1);
+          return true;
+        }
+      }
+    }
+    return false;
+  }
+
+  // Control prefixes (interpret_controlled_gates, interpreter.cpp:3341-3370):
+  // "CC..C<gate>" has one control per C; "C<n><gate>" has n; a single "C" has one.
+  bool controlled(const columns& c, const std::string& m)
+  {
+    size_t cs = 0;
+    while (cs < m.size() && m[cs] == 'C') ++cs;
+    size_t digits_end = 1;
+    while (digits_end < m.size() && std::isdigit(static_cast<unsigned char>(m[digits_end]))) ++digits_end;
+    int nc;
+    std::string rest;
+    if (cs > 1) {
+      nc = static_cast<int>(cs);
+      rest = m.substr(cs);
+    } else if (digits_end > 1) {
+      nc = std::atoi(m.substr(1, digits_end - 1).c_str());
+      rest = m.substr(digits_end);
+    } else {
+      nc = 1;
+      rest = m.substr(1);
+    }
+    if (nc <= 0 || rest.empty()) return false;
+    return gate_mnemonic(c, rest, nc);
+  }
+
+  void statement(columns c)
+  {
+    c[0] = upper(c[0]);
+    const std::string& m = c[0];
+    auto word = [&](size_t i) { return i < c.size() ? upper(c[i]) : std::string{}; };
+    if (m == "QUBITS") {
+      expect(c, 2);
+      const uint64_t n = to_unsigned(c[1]);
+      if (n < 1 || n > 34) bad("QUBITS must be between 1 and 34");
+      prog.num_qubits = static_cast<int>(n);
+      return;
+    }
+    if (m == "CIRCUITS") {
+      expect(c, 2);
+      if (to_unsigned(c[1]) != 1) unsupported("several circuits (CIRCUITS > 1) are not supported");
+      return;
+    }
+    if (m == "INITIAL") {  // INITIAL STATE v
+      if (c.size() != 3 || word(1) != "STATE") bad("expected INITIAL STATE <value>");
+      prog.initial_state = to_unsigned(c[2]);
+      return;
+    }
+    if (m == "BIT") {  // BIT ASSIGNMENT: the initial permutation of MPI builds; nompi ignores it
+      if (c.size() < 2 || word(1) != "ASSIGNMENT") bad("expected BIT ASSIGNMENT <qubits>");
+      if (prog.num_qubits >= 0 && c.size() != 2 + static_cast<size_t>(prog.num_qubits))
+        bad("BIT ASSIGNMENT needs one entry per qubit");
+      for (size_t i = 2; i < c.size(); ++i) qubit(c[i]);
+      return;
+    }
+    if (m == "MPIPROCESSES" || m == "MPISWAPBUFFER") return;
+    if (m == "DEPOLARIZING" || m == "PERMUTATION" || m == "RANDOM" || m == "VAR" || m == "LET" || m == "SEND" ||
+        m == "RECEIVE" || m == "BROADCAST" || m == "GATHER" || m == "SCATTER" || m == "JUMP" || m == "JUMPIF" ||
+        m == "INNERPROD" || m == "FIDELITY" || m.front() == '@')
+      unsupported("'" + m + "' is not supported");
+    if (prog.num_qubits < 0) bad("QUBITS must come first");
+    if (m == "EXIT") {
+      expect(c, 1);
+      prog.code.push_back(blank(RBK_QCX_EXIT, line));
+      done = true;  // bra stops reading at EXIT (interpreter.cpp:579-590)
+      return;
+    }
+    if (m == "BEGIN") {
+      const std::string w = word(1);
+      if (w == "MEASUREMENT") {
+        auto in = blank(RBK_QCX_MEASUREMENT, line);
+        in.ints[0] = 3;
+        prog.code.push_back(in);
+      } else if (w == "FUSION") {
+        prog.code.push_back(blank(RBK_QCX_BEGIN_FUSION, line));
+      } else if (w == "CIRCUIT" || w == "LEARNING") {
+        unsupported("BEGIN " + w + " is not supported");
+      } else {
+        bad("unknown BEGIN statement");
+      }
+      return;
+    }
+    if (m == "END") {
+      const std::string w = word(1);
+      if (w == "FUSION") prog.code.push_back(blank(RBK_QCX_END_FUSION, line));
+      else if (w == "CIRCUIT") unsupported("END CIRCUIT is not supported");
+      else bad("unknown END statement");
+      return;
+    }
+    if (m == "DO") {
+      const std::string w = word(1);
+      if (w == "MEASUREMENT") {
+        if (c.size() > 3) bad("DO MEASUREMENT takes at most one precision");
+        auto in = blank(RBK_QCX_MEASUREMENT, line);
+        in.ints[0] = c.size() == 3 ? to_int(c[2]) : 3;
+        prog.code.push_back(in);
+      } else if (w == "AMPLITUDES") {
+        auto in = blank(RBK_QCX_AMPLITUDES, line);
+        std::vector<uint64_t> idx;
+        for (size_t i = 2; i < c.size(); ++i) {
+          const uint64_t v = to_unsigned(c[i]);
+          if (v >= (1ull << prog.num_qubits)) bad("amplitude index " + c[i] + " is out of range");
+          idx.push_back(v);
+        }
+        in.num_values = static_cast<int32_t>(idx.size());
+        for (size_t i = 0; i < idx.size() && i < RBK_QCX_MAX_VALUES; ++i) in.values[i] = idx[i];
+        prog.amplitude_lists.resize(prog.code.size() + 1);
+        prog.amplitude_lists[prog.code.size()] = std::move(idx);
+        prog.code.push_back(in);
+      } else {
+        bad("unknown DO statement");
+      }
+      return;
+    }
+    if (m == "GENERATE") {  // GENERATE EVENTS n seed; bra stops reading here (interpreter.cpp:764-785)
+      if (c.size() != 4 || word(1) != "EVENTS") bad("expected GENERATE EVENTS <events> <seed>");
+      auto in = blank(RBK_QCX_GENERATE_EVENTS, line);
+      in.ints[0] = to_int(c[2]);
+      in.ints[1] = to_int(c[3]);
+      if (in.ints[0] < 0 || in.ints[0] > (1 << 30)) bad("number of events out of range");
+      prog.code.push_back(in);
+      done = true;
+      return;
+    }
+    if (m == "EXPECTATION") {  // EXPECTATION :PAULIS:<s> q1 q2 ... (interpreter.cpp:3218-3240)
+      if (c.size() < 3) bad("expected EXPECTATION <operator> <qubits>");
+      const std::string& op = c[1];
+      if (op.rfind(":PAULIS:", 0) != 0 || op.size() <= 8) unsupported("EXPECTATION takes a :PAULIS:<string> literal");
+      auto in = blank(RBK_QCX_EXPECTATION, line);
+      const std::string str = upper(op.substr(8));
+      if (str.size() != c.size() - 2) bad("the Pauli string length must equal the number of qubits");
+      if (str.size() >= sizeof(in.text) || str.size() > RBK_QCX_MAX_QUBITS) bad("Pauli string too long");
+      for (char ch : str)
+        if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z') bad("Pauli strings use I, X, Y, Z");
+      std::memcpy(in.text, str.c_str(), str.size() + 1);
+      std::vector<uint32_t> seen;
+      for (size_t i = 2; i < c.size(); ++i) {
+        const uint32_t q = qubit(c[i]);
+        if (std::find(seen.begin(), seen.end(), q) != seen.end()) bad("qubit " + c[i] + " appears twice");
+        seen.push_back(q);
+        in.targets[in.num_targets++] = q;
+      }
+      prog.code.push_back(in);
+      return;
+    }
+    if (m == "PRINT" || m == "PRINTLN") {
+      auto in = blank(RBK_QCX_PRINT, line);
+      std::string joined;
+      for (size_t i = 1; i < c.size(); ++i) joined += (i > 1 ? " " : "") + c[i];
+      if (joined.size() >= sizeof(in.text)) bad("PRINT arguments too long");
+      std::memcpy(in.text, joined.c_str(), joined.size() + 1);
+      in.ints[0] = m == "PRINTLN";
+      prog.code.push_back(in);
+      return;
+    }
+    if (m == "U" || m == "U+") {  // "U c1 c2 k" = CR c1 c2 k (docs/bra.md; interpreter.cpp:2747-2765)
+      gate(c, m == "U" ? RBK_QCX_R : RBK_QCX_R_ADJ, 0, 2, 1, true, true);
+      return;
+    }
+    if (m == "TOFFOLI") {  // TOFFOLI c1 c2 t (interpreter.cpp:3189-3197)
+      gate(c, RBK_QCX_TOFFOLI, 2, 1, 0);
+      return;
+    }
+    if (m == "M") {
+      expect(c, 2);
+      auto in = blank(RBK_QCX_PROJECTIVE, line);
+      in.targets[in.num_targets++] = qubit(c[1]);
+      prog.code.push_back(in);
+      return;
+    }
+    if (m == "CLEAR" || m == "SET") {
+      gate(c, m == "CLEAR" ? RBK_QCX_CLEAR : RBK_QCX_SET, 0, 1, 0);
+      return;
+    }
+    if (m == "SHORBOX") {  // SHORBOX nx divisor base (interpreter.cpp:3208-3216)
+      expect(c, 4);
+      auto in = blank(RBK_QCX_GATE, line);
+      in.kind = RBK_QCX_SHORBOX;
+      const uint64_t nx = to_unsigned(c[1]);
+      if (nx > static_cast<uint64_t>(prog.num_qubits)) bad("SHORBOX has more exponent qubits than qubits");
+      in.params[0] = static_cast<double>(nx);
+      in.params[1] = static_cast<double>(to_unsigned(c[2]));
+      in.params[2] = static_cast<double>(to_unsigned(c[3]));
+      in.ints[0] = static_cast<int64_t>(to_unsigned(c[2]));
+      in.ints[1] = static_cast<int64_t>(to_unsigned(c[3]));
+      prog.code.push_back(in);
+      return;
+    }
+    if (gate_mnemonic(c, m, 0)) return;
+    if (m.size() >= 2 && m[0] == 'C' && controlled(c, m)) return;
+    bad("unknown mnemonic '" + m + "'");
+  }
+
+  void run(const std::string& text)
+  {
+    std::istringstream in(text);
+    std::string raw;
+    while (!done && std::getline(in, raw)) {
+      ++line;
+      raw.erase(std::find(raw.begin(), raw.end(), '!'), raw.end());
+      columns c;
+      std::istringstream ls(raw);
+      std::string tok;
+      while (ls >> tok) c.push_back(tok);
+      if (c.empty()) continue;
+      try {
+        statement(std::move(c));
+      } catch (qcx_error const& e) {
+        throw qcx_error(e.code, "line " + std::to_string(line) + ": " + e.what());
+      }
+    }
+    if (prog.num_qubits < 0) bad("no QUBITS statement");
+    if (prog.initial_state >= (1ull << prog.num_qubits)) bad("INITIAL STATE is out of range");
+  }
+};
+
+}  // namespace
+
+// ---- execution ---------------------------------------------------------------
+
+namespace {
+
+using clock_type = std::chrono::steady_clock;
+using cplx = std::complex<double>;
+
+// bra::state_detail::duration_to_second (bra/include/bra/state.hpp:118-123).
+double seconds(clock_type::time_point from, clock_type::time_point to)
+{
+  return 0.000001 * static_cast<double>(std::chrono::duration_cast<std::chrono::microseconds>(to - from).count());
+}
+
+// bra::state_detail::integer_to_bits_string (bra/include/bra/state.hpp:100-117): most significant qubit first.
+std::string bits(uint64_t v, int n)
+{
+  std::string s(static_cast<size_t>(n), '0');
+  for (int b = 0; b < n; ++b)
+    if ((v >> b) & 1) s[static_cast<size_t>(n - 1 - b)] = '1';
+  return s;
+}
+
+// fmt's "{:^W}" centring: the odd padding character goes to the right.
+std::string centre(const std::string& s, int width)
+{
+  const int pad = width - static_cast<int>(s.size());
+  if (pad <= 0) return s;
+  return std::string(static_cast<size_t>(pad / 2), ' ') + s + std::string(static_cast<size_t>(pad - pad / 2), ' ');
+}
+
+std::string fixed_with_space_sign(double v, int precision)
+{
+  char buf[64];
+  std::snprintf(buf, sizeof(buf), "% .*f", precision, v);
+  return buf;
+}
+
+void check(int rc)
+{
+  if (rc != RBK_OK) throw qcx_error(rc, rbk_last_error());
+}
+
+struct runner {
+  const rbk_qcx_program& prog;
+  const rbk_qcx_options& opt;
+  rbk_state* s = nullptr;
+  std::ostringstream out;
+  clock_type::time_point start, last;
+  std::vector<int> last_outcomes;
+  int last_measured = 0;
+  cplx result{0.0, 0.0};
+
+  runner(const rbk_qcx_program& p, const rbk_qcx_options& o) : prog(p), opt(o) {}
+
+  void mark(const char* what)
+  {
+    check(rbk_state_synchronize(s));
+    const auto now = clock_type::now();
+    if (opt.print_timing) out << what << " finished: " << seconds(start, now) << " (" << seconds(last, now) << ")\n";
+    last = now;
+  }
+
+  void gate(const rbk_qcx_instruction& g)
+  {
+    const uint32_t* t = g.targets;
+    const uint32_t* c = g.num_controls ? g.controls : nullptr;
+    const int nt = g.num_targets, nc = g.num_controls;
+    const double* p = g.params;
+    const bool adj = g.kind == RBK_QCX_SX_ADJ || g.kind == RBK_QCX_SY_ADJ || g.kind == RBK_QCX_SZ_ADJ ||
+                     g.kind == RBK_QCX_U1_ADJ || g.kind == RBK_QCX_U2_ADJ || g.kind == RBK_QCX_U3_ADJ ||
+                     g.kind == RBK_QCX_R_ADJ || g.kind == RBK_QCX_ROTX_ADJ || g.kind == RBK_QCX_ROTY_ADJ ||
+                     g.kind == RBK_QCX_EX_ADJ || g.kind == RBK_QCX_EY_ADJ || g.kind == RBK_QCX_EZ_ADJ ||
+                     g.kind == RBK_QCX_ESWAP_ADJ;
+    switch (g.kind) {
+      case RBK_QCX_H: check(rbk_hadamard(s, t[0], c, nc)); break;
+      case RBK_QCX_NOT: check(rbk_pauli_x(s, t[0], c, nc)); break;
+      case RBK_QCX_X: case RBK_QCX_Y: {
+        if (nt == 1) check(g.kind == RBK_QCX_X ? rbk_pauli_x(s, t[0], c, nc) : rbk_pauli_y(s, t[0], c, nc));
+        else check(rbk_pauli_string(s, std::string(static_cast<size_t>(nt), g.kind == RBK_QCX_X ? 'X' : 'Y').c_str(), t, nt, c, nc));
+        break;
+      }
+      case RBK_QCX_Z:
+        if (nt == 0) check(rbk_pauli_z(s, g.controls, nc));
+        else check(rbk_pauli_string(s, std::string(static_cast<size_t>(nt), 'Z').c_str(), t, nt, c, nc));
+        break;
+      case RBK_QCX_SWAP: check(rbk_swap(s, t[0], t[1], c, nc)); break;
+      case RBK_QCX_SX: case RBK_QCX_SX_ADJ: check(rbk_sqrt_pauli_x(s, adj, t[0], c, nc)); break;
+      case RBK_QCX_SY: case RBK_QCX_SY_ADJ: check(rbk_sqrt_pauli_y(s, adj, t[0], c, nc)); break;
+      case RBK_QCX_SZ: case RBK_QCX_SZ_ADJ:
+        if (nt == 0) check(rbk_phase_shift_coeff(s, 0.0, adj ? -1.0 : 1.0, g.controls, nc));
+        else check(rbk_sqrt_pauli_z(s, adj, t, nt, c, nc));
+        break;
+      case RBK_QCX_U1: case RBK_QCX_U1_ADJ: {
+        // ket::gate::phase_shift(phase) multiplies by exp_i(phase); adj_ by its conjugate
+        const cplx e = std::exp(cplx{0.0, p[0]});
+        const cplx coeff = adj ? std::conj(e) : e;
+        check(rbk_phase_shift_coeff(s, coeff.real(), coeff.imag(), g.controls, nc));
+        break;
+      }
+      case RBK_QCX_U2:
+        check(rbk_phase_shift2(s, p[0], p[1], t[0], c, nc));
+        break;
+      case RBK_QCX_U3:
+        check(rbk_phase_shift3(s, p[0], p[1], p[2], t[0], c, nc));
+        break;
+      case RBK_QCX_U2_ADJ: case RBK_QCX_U3_ADJ: {
+        // U3(theta, phi, lambda)^dagger = [[cos, e^{-i phi} sin], [-e^{-i lambda} sin, e^{-i(phi+lambda)} cos]]
+        // (theta/2 inside cos, sin; U2 is U3 with theta = pi/2, phase_shift.hpp:660-709, :1200-1254)
+        const double half = g.kind == RBK_QCX_U2_ADJ ? 0.25 * 3.141592653589793238462643383279502884 : 0.5 * p[0];
+        const double phi = g.kind == RBK_QCX_U2_ADJ ? p[0] : p[1];
+        const double lam = g.kind == RBK_QCX_U2_ADJ ? p[1] : p[2];
+        const double cs = g.kind == RBK_QCX_U2_ADJ ? 0.7071067811865475244008443621048490393 : std::cos(half);
+        const double sn = g.kind == RBK_QCX_U2_ADJ ? 0.7071067811865475244008443621048490393 : std::sin(half);
+        const cplx m00{cs, 0.0}, m01 = std::exp(cplx{0.0, -phi}) * sn, m10 = -std::exp(cplx{0.0, -lam}) * sn,
+                   m11 = std::exp(cplx{0.0, -(phi + lam)}) * cs;
+        const double m[8] = {m00.real(), m00.imag(), m01.real(), m01.imag(), m10.real(), m10.imag(), m11.real(), m11.imag()};
+        check(rbk_apply_matrix2(s, m, t[0], c, nc));
+        break;
+      }
+      case RBK_QCX_R: case RBK_QCX_R_ADJ: {
+        const int k = static_cast<int>(p[0]);
+        check(rbk_controlled_phase_shift_k(s, adj ? -k : k, g.controls, nc));
+        break;
+      }
+      case RBK_QCX_ROTX: case RBK_QCX_ROTX_ADJ: check(rbk_x_rotation_half_pi(s, adj, t[0], c, nc)); break;
+      case RBK_QCX_ROTY: case RBK_QCX_ROTY_ADJ: check(rbk_y_rotation_half_pi(s, adj, t[0], c, nc)); break;
+      case RBK_QCX_EX: case RBK_QCX_EX_ADJ: case RBK_QCX_EY: case RBK_QCX_EY_ADJ: case RBK_QCX_EZ: case RBK_QCX_EZ_ADJ: {
+        const double phase = adj ? -p[0] : p[0];  // adj_exponential_pauli_*: exp(-i theta P)
+        const char letter = (g.kind <= RBK_QCX_EX_ADJ) ? 'X' : (g.kind <= RBK_QCX_EY_ADJ) ? 'Y' : 'Z';
+        if (nt == 1) {
+          if (letter == 'X') check(rbk_exponential_pauli_x(s, phase, t[0], c, nc));
+          else if (letter == 'Y') check(rbk_exponential_pauli_y(s, phase, t[0], c, nc));
+          else check(rbk_exponential_pauli_z(s, phase, t[0], c, nc));
+        } else {
+          check(rbk_exponential_pauli_string(s, phase, std::string(static_cast<size_t>(nt), letter).c_str(), t, nt, c, nc));
+        }
+        break;
+      }
+      case RBK_QCX_ESWAP: case RBK_QCX_ESWAP_ADJ: check(rbk_exponential_swap(s, adj ? -p[0] : p[0], t[0], t[1], c, nc)); break;
+      case RBK_QCX_TOFFOLI: check(rbk_pauli_x(s, t[0], g.controls, 2)); break;
+      case RBK_QCX_CLEAR: check(rbk_clear(s, t[0])); break;
+      case RBK_QCX_SET: check(rbk_set(s, t[0])); break;
+      case RBK_QCX_SHORBOX:
+        check(rbk_shor_box(s, static_cast<uint32_t>(p[0]), static_cast<uint64_t>(g.ints[0]), static_cast<uint64_t>(g.ints[1])));
+        break;
+      default: throw qcx_error(RBK_ERR_INVALID, "unknown gate kind");
+    }
+  }
+
+  // bra::state::measurement (bra/src/state.cpp:1980-2034): the printed numbers are
+  // 0.5 - <S> of each axis, i.e. the probability-like "qubit value" in [0, 1].
+  void measurement(int precision)
+  {
+    mark("Operations");
+    std::vector<double> spins(static_cast<size_t>(3 * prog.num_qubits));
+    check(rbk_spin_expectation_values(s, spins.data()));
+    out << "Expectation values of spins:\n";
+    if (precision > 0) {
+      const int width = std::max(precision + 3, 8);
+      out << centre("<Qx>", width) << ' ' << centre("<Qy>", width) << ' ' << centre("<Qz>", width) << '\n';
+      for (int q = 0; q < prog.num_qubits; ++q)
+        out << centre(fixed_with_space_sign(0.5 - spins[3 * q], precision), width) << ' '
+            << centre(fixed_with_space_sign(0.5 - spins[3 * q + 1], precision), width) << ' '
+            << centre(fixed_with_space_sign(0.5 - spins[3 * q + 2], precision), width) << '\n';
+    } else {
+      out << "<Qx> <Qy> <Qz>\n";
+      std::ostringstream vals;
+      if (precision < 0) vals << std::setprecision(-precision);
+      for (int q = 0; q < prog.num_qubits; ++q)
+        vals << (0.5 - spins[3 * q]) << ' ' << (0.5 - spins[3 * q + 1]) << ' ' << (0.5 - spins[3 * q + 2]) << '\n';
+      out << vals.str();
+    }
+    mark("Expectation values");
+  }
+
+  // bra::nompi_state::do_amplitudes (bra/src/nompi_state.cpp:1108-1133): "bits => re + im i".
+  void amplitudes(const std::vector<uint64_t>& indices)
+  {
+    mark("Operations");
+    const uint64_t size = 1ull << prog.num_qubits;
+    int precision = RBK_C128;
+    check(rbk_state_precision(s, &precision));
+    auto print_range = [&](uint64_t first, uint64_t count, bool newline_each) {
+      std::vector<double> buf(2 * count);
+      std::vector<float> fbuf;
+      if (precision == RBK_C128) check(rbk_state_download(s, buf.data(), first, count));
+      else {
+        fbuf.resize(2 * count);
+        check(rbk_state_download(s, fbuf.data(), first, count));
+      }
+      for (uint64_t i = 0; i < count; ++i) {
+        if (!newline_each && first + i > 0) out << '\n';
+        out << bits(first + i, prog.num_qubits) << " => ";
+        if (precision == RBK_C128) out << buf[2 * i] << " + " << buf[2 * i + 1] << " i";
+        else out << fbuf[2 * i] << " + " << fbuf[2 * i + 1] << " i";
+        if (newline_each) out << '\n';
+      }
+    };
+    if (indices.empty()) {
+      const uint64_t chunk = 1ull << 20;
+      for (uint64_t first = 0; first < size; first += chunk) print_range(first, std::min(chunk, size - first), false);
+      out << '\n';
+    } else {
+      for (uint64_t idx : indices) print_range(idx, 1, true);
+    }
+    mark("Amplitudes");
+  }
+
+  void generate_events(int num, int64_t seed)
+  {
+    mark("Operations");
+    std::vector<uint64_t> ev(static_cast<size_t>(num));
+    check(rbk_generate_events(s, num, seed, ev.data()));
+    out << "Events:\n";
+    for (int i = 0; i < num; ++i) out << i << ' ' << bits(ev[static_cast<size_t>(i)], prog.num_qubits) << '\n';
+    mark("Events");
+  }
+
+  void exit_measure()
+  {
+    mark("Operations");
+    uint64_t v = 0;
+    check(rbk_measure(s, &v));
+    out << "Measurement result: " << v << '\n';
+    mark("Measurement");
+  }
+
+  // EXPECTATION :PAULIS:<s> q...: character k of the string acts on the k-th listed qubit.
+  void expectation(const rbk_qcx_instruction& in)
+  {
+    std::string full(static_cast<size_t>(prog.num_qubits), 'I');
+    for (int k = 0; k < in.num_targets; ++k) full[in.targets[k]] = in.text[k];
+    const double coeff[2] = {1.0, 0.0};
+    double r[2];
+    check(rbk_expectation_pauli(s, 1, full.c_str(), coeff, r));
+    result = cplx{r[0], r[1]};
+  }
+
+  // bra::state::generate_print_string (bra/src/state.cpp:495-538) for literals and built-ins.
+  void print(const rbk_qcx_instruction& in)
+  {
+    std::istringstream args(in.text);
+    std::string a;
+    bool first = true;
+    while (args >> a) {
+      if (!first) out << ' ';
+      first = false;
+      const char f = a.front();
+      if (std::isdigit(static_cast<unsigned char>(f)) || f == '+' || f == '-' || f == '.') { out << a; continue; }
+      if (f != ':') continue;  // classical variables do not exist here
+      if (a == ":RESULT") out << result;
+      else if (a == ":I") out << cplx{0.0, 1.0};
+      else if (a == ":MINUS_I") out << cplx{0.0, -1.0};
+      else if (a == ":COMPLEX") out << cplx{0.0, 0.0};
+      else if (a == ":INT") out << 0;
+      else if (a == ":OUTCOME") out << last_outcomes[static_cast<size_t>(last_measured)];
+      else if (a == ":OUTCOMES") out << last_outcomes.front();
+      else if (a.rfind(":OUTCOMES:", 0) == 0) {
+        const int64_t q = to_int(a.substr(10));
+        if (q < 0 || q >= prog.num_qubits) throw qcx_error(RBK_ERR_INVALID, "line " + std::to_string(in.line) + ": qubit out of range");
+        out << last_outcomes[static_cast<size_t>(q)];
+      } else {
+        out << to_real(a);
+      }
+    }
+    if (in.ints[0]) out << '\n';
+  }
+
+  void execute()
+  {
+    const size_t count = prog.code.size();
+    for (size_t i = 0; i < count; ++i) {
+      const auto& in = prog.code[i];
+      try {
+        switch (in.op) {
+          case RBK_QCX_GATE: gate(in); break;
+          case RBK_QCX_BEGIN_FUSION: check(rbk_begin_fusion(s)); break;
+          case RBK_QCX_END_FUSION: check(rbk_end_fusion(s)); break;
+          case RBK_QCX_MEASUREMENT: measurement(static_cast<int>(in.ints[0])); break;
+          case RBK_QCX_AMPLITUDES:
+            amplitudes(i < prog.amplitude_lists.size() ? prog.amplitude_lists[i] : std::vector<uint64_t>{});
+            break;
+          case RBK_QCX_GENERATE_EVENTS: generate_events(static_cast<int>(in.ints[0]), in.ints[1]); break;
+          case RBK_QCX_EXIT: exit_measure(); break;
+          case RBK_QCX_PROJECTIVE: {
+            int outcome = 0;
+            check(rbk_projective_measurement(s, in.targets[0], &outcome));
+            last_outcomes[in.targets[0]] = outcome;
+            last_measured = static_cast<int>(in.targets[0]);
+            break;
+          }
+          case RBK_QCX_EXPECTATION: expectation(in); break;
+          case RBK_QCX_PRINT: print(in); break;
+          case RBK_QCX_NOOP: break;
+          default: throw qcx_error(RBK_ERR_INVALID, "unknown instruction");
+        }
+      } catch (qcx_error const& e) {
+        throw qcx_error(e.code, "line " + std::to_string(in.line) + ": " + e.what());
+      }
+    }
+  }
+};
+
+template <typename F>
+int guard(F&& f)
+{
+  try {
+    return f();
+  } catch (qcx_error const& e) {
+    return rbk::set_last_error(e.code, e.what());
+  } catch (std::bad_alloc const&) {
+    return rbk::set_last_error(RBK_ERR_OOM, "host memory exhausted");
+  } catch (std::exception const& e) {
+    return rbk::set_last_error(RBK_ERR_STATE, e.what());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void rbk_qcx_default_options(rbk_qcx_options* o)
+{
+  if (!o) return;
+  o->precision = RBK_C128;
+  o->device = 0;
+  o->seed = 1;
+  o->deferred = 1;
+  o->print_timing = 1;
+}
+
+int rbk_qcx_parse(const char* text, size_t length, rbk_qcx_program** out)
+{
+  return guard([&]() -> int {
+    if (!out || (!text && length)) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto* p = new rbk_qcx_program;
+    try {
+      parser ps{*p};
+      ps.run(std::string(text ? text : "", length));
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    p->amplitude_lists.resize(p->code.size());
+    *out = p;
+    return RBK_OK;
+  });
+}
+
+int rbk_qcx_destroy(rbk_qcx_program* p)
+{
+  delete p;
+  return RBK_OK;
+}
+
+int rbk_qcx_num_qubits(const rbk_qcx_program* p, int* out)
+{
+  if (!p || !out) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
+  *out = p->num_qubits;
+  return RBK_OK;
+}
+
+int rbk_qcx_initial_state(const rbk_qcx_program* p, uint64_t* out)
+{
+  if (!p || !out) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
+  *out = p->initial_state;
+  return RBK_OK;
+}
+
+int rbk_qcx_num_instructions(const rbk_qcx_program* p, int* out)
+{
+  if (!p || !out) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
+  *out = static_cast<int>(p->code.size());
+  return RBK_OK;
+}
+
+int rbk_qcx_get_instruction(const rbk_qcx_program* p, int index, rbk_qcx_instruction* out)
+{
+  if (!p || !out) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
+  if (index < 0 || static_cast<size_t>(index) >= p->code.size()) return rbk::set_last_error(RBK_ERR_INVALID, "index out of range");
+  *out = p->code[static_cast<size_t>(index)];
+  return RBK_OK;
+}
+
+int rbk_qcx_run(const rbk_qcx_program* p, const rbk_qcx_options* options, char** text, rbk_state** state_out)
+{
+  return guard([&]() -> int {
+    if (!p || !text) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
+    *text = nullptr;
+    if (state_out) *state_out = nullptr;
+    rbk_qcx_options opt;
+    rbk_qcx_default_options(&opt);
+    if (options) opt = *options;
+    runner r(*p, opt);
+    r.last_outcomes.assign(static_cast<size_t>(p->num_qubits), -1);  // ket::gate::outcome::unspecified
+    r.start = r.last = clock_type::now();
+    check(rbk_state_create(p->num_qubits, opt.precision, p->initial_state, opt.device, &r.s));
+    try {
+      check(rbk_state_seed(r.s, opt.seed));
+      check(rbk_state_set_deferred(r.s, opt.deferred));
+      r.execute();
+      check(rbk_state_synchronize(r.s));
+    } catch (...) {
+      rbk_state_destroy(r.s);
+      throw;
+    }
+    const std::string o = r.out.str();
+    char* buf = static_cast<char*>(std::malloc(o.size() + 1));
+    if (!buf) {
+      rbk_state_destroy(r.s);
+      return rbk::set_last_error(RBK_ERR_OOM, "host memory exhausted");
+    }
+    std::memcpy(buf, o.c_str(), o.size() + 1);
+    *text = buf;
+    if (state_out) *state_out = r.s;
+    else rbk_state_destroy(r.s);
+    return RBK_OK;
+  });
+}
+
+void rbk_qcx_free_text(char* text) { std::free(text); }
+
+}  // extern "C"

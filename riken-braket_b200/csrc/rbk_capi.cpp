@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -1229,5 +1230,290 @@ extern "C" int rbk_projective_measurement(rbk_state* s, uint32_t qubit, int* out
     *outcome = one;
     if ((rc = rbk_apply_diagonal2(s, d, qubit, nullptr, 0))) return rc;
     return flush(s);
+  });
+}
+
+// ---- further ket gate families ---------------------------------------------
+// Gates outside the brick/QFT hot path that bra's instruction set reaches.
+// Each is written as a short sequence of the queued primitives above, so it
+// joins the same fused passes; only CLEAR/SET and SHORBOX run kernels of their
+// own.
+
+namespace {
+
+int enqueue_matrix(rbk_state* s, const std::array<cplx, 4>& u, uint32_t target, const uint32_t* controls, int nc)
+{
+  double m[8];
+  for (int k = 0; k < 4; ++k) put(m, k, u[k]);
+  return enqueue_target(s, rbk::OPK_MAT, target, controls, nc, m);
+}
+
+// controls + extra, as one qubit list.
+std::vector<uint32_t> with_qubit(const uint32_t* controls, int nc, uint32_t extra)
+{
+  std::vector<uint32_t> v(controls, controls + nc);
+  v.push_back(extra);
+  return v;
+}
+
+// Targets and controls all valid and pairwise distinct.
+int check_targets_controls(rbk_state* s, const uint32_t* targets, int nt, const uint32_t* controls, int nc)
+{
+  if (int rc = check_state(s)) return rc;
+  if (nt < 1) return fail(RBK_ERR_INVALID, "at least one target qubit is needed");
+  if (nc < 0) return fail(RBK_ERR_INVALID, "negative control count");
+  std::vector<uint32_t> all(targets, targets + nt);
+  if (nc > 0) {
+    if (!controls) return fail(RBK_ERR_INVALID, "null control array");
+    all.insert(all.end(), controls, controls + nc);
+  }
+  uint64_t mask = 0;
+  return check_qubits(s, all.data(), static_cast<int>(all.size()), &mask);
+}
+
+// Probabilities of qubit q being 0 and 1 (logical qubit; one reduction pass).
+int qubit_probabilities(rbk_state* s, uint32_t q, double* p0, double* p1)
+{
+  int rc = launch_reduction(s, [&] {
+    return s->precision == RBK_C128 ? rbk::launch_zsum<double>(s->amps, s->n, s->d_partials, s->d_out, s->stream)
+                                    : rbk::launch_zsum<float>(s->amps, s->n, s->d_partials, s->d_out, s->stream);
+  });
+  if (rc) return rc;
+  if ((rc = read_out(s, s->n + 1))) return rc;
+  *p1 = s->h_out[1 + s->perm[q]];
+  *p0 = s->h_out[0] - *p1;
+  return RBK_OK;
+}
+
+// Keeps the half of qubit q equal to `one`, scaled by p^(-1/2); zeroes the other.
+int collapse(rbk_state* s, uint32_t q, int one, double p)
+{
+  double d[4] = {0, 0, 0, 0};
+  d[one ? 2 : 0] = std::pow(p, -0.5);
+  if (int rc = rbk_apply_diagonal2(s, d, q, nullptr, 0)) return rc;
+  return flush(s);
+}
+
+}  // namespace
+
+extern "C" int rbk_x_rotation_half_pi(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int nc)
+{
+  // +X: ((a0 + i a1), (i a0 + a1)) / sqrt2; -X conjugates i (x_rotation_half_pi.hpp:34, :254)
+  return guarded([&]() -> int {
+    const double si = adjoint ? -kOneDivRootTwo : kOneDivRootTwo;
+    const std::array<cplx, 4> u{cplx{kOneDivRootTwo, 0}, cplx{0, si}, cplx{0, si}, cplx{kOneDivRootTwo, 0}};
+    return enqueue_matrix(s, u, target, controls, nc);
+  });
+}
+
+extern "C" int rbk_y_rotation_half_pi(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int nc)
+{
+  // +Y: ((a0 + a1), (-a0 + a1)) / sqrt2; -Y: ((a0 - a1), (a0 + a1)) / sqrt2 (y_rotation_half_pi.hpp:33, :251)
+  return guarded([&]() -> int {
+    const double r = kOneDivRootTwo, off = adjoint ? -r : r;
+    const std::array<cplx, 4> u{cplx{r, 0}, cplx{off, 0}, cplx{-off, 0}, cplx{r, 0}};
+    return enqueue_matrix(s, u, target, controls, nc);
+  });
+}
+
+extern "C" int rbk_sqrt_pauli_x(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int nc)
+{
+  // sX = [[1+i, 1-i], [1-i, 1+i]] / 2, sX+ its conjugate (sqrt_pauli_x.hpp:32, :259)
+  return guarded([&]() -> int {
+    const double sg = adjoint ? -0.5 : 0.5;
+    const cplx p{0.5, sg}, m{0.5, -sg};
+    const std::array<cplx, 4> u{p, m, m, p};
+    return enqueue_matrix(s, u, target, controls, nc);
+  });
+}
+
+extern "C" int rbk_sqrt_pauli_y(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int nc)
+{
+  // sY = (1+i)/2 [[1, -1], [1, 1]]; sY+ = (1-i)/2 [[1, 1], [-1, 1]] (sqrt_pauli_y.hpp:33, :256)
+  return guarded([&]() -> int {
+    const cplx c = adjoint ? cplx{0.5, -0.5} : cplx{0.5, 0.5};
+    const std::array<cplx, 4> u = adjoint ? std::array<cplx, 4>{c, c, -c, c} : std::array<cplx, 4>{c, -c, c, c};
+    return enqueue_matrix(s, u, target, controls, nc);
+  });
+}
+
+extern "C" int rbk_sqrt_pauli_z(rbk_state* s, int adjoint, const uint32_t* targets, int nt, const uint32_t* controls, int nc)
+{
+  // C...C(sZ_t1 ... sZ_tm): each target's |1> times i (or -i) where all controls are one
+  // (sqrt_pauli_z.hpp:55-57, :459-461; runtime form :137-205)
+  return guarded([&]() -> int {
+    if (int rc = check_targets_controls(s, targets, nt, controls, nc)) return rc;
+    const cplx c{0.0, adjoint ? -1.0 : 1.0};
+    for (int k = 0; k < nt; ++k) {
+      auto qs = with_qubit(controls, nc, targets[k]);
+      if (int rc = enqueue_phase(s, c, qs.data(), static_cast<int>(qs.size()))) return rc;
+    }
+    return RBK_OK;
+  });
+}
+
+extern "C" int rbk_pauli_string(rbk_state* s, const char* paulis, const uint32_t* targets, int nt, const uint32_t* controls,
+                                int nc)
+{
+  // C...C(P_t1 ... P_tm), P in {X, Y, Z}: the single-qubit Paulis commute, so the
+  // product is applied factor by factor under the same controls (pauli_x.hpp runtime
+  // form :288-572; pauli_y.hpp, pauli_z.hpp likewise).  Exact: every factor only
+  // moves amplitudes and multiplies them by +-1 or +-i.
+  return guarded([&]() -> int {
+    if (!paulis) return fail(RBK_ERR_INVALID, "null Pauli string");
+    if (int rc = check_targets_controls(s, targets, nt, controls, nc)) return rc;
+    for (int k = 0; k < nt; ++k) {
+      const char p = paulis[k];
+      int rc;
+      if (p == 'X') rc = enqueue_target(s, rbk::OPK_X, targets[k], controls, nc, nullptr);
+      else if (p == 'Y') rc = enqueue_target(s, rbk::OPK_Y, targets[k], controls, nc, nullptr);
+      else if (p == 'Z') {
+        auto qs = with_qubit(controls, nc, targets[k]);
+        rc = enqueue_phase(s, cplx{-1.0, 0.0}, qs.data(), static_cast<int>(qs.size()));
+      } else if (p == 'I') rc = RBK_OK;
+      else return fail(RBK_ERR_INVALID, "Pauli string characters must be I, X, Y or Z");
+      if (rc) return rc;
+    }
+    return RBK_OK;
+  });
+}
+
+extern "C" int rbk_exponential_pauli_string(rbk_state* s, double phase, const char* paulis, const uint32_t* targets, int nt,
+                                            const uint32_t* controls, int nc)
+{
+  // C...C exp(i phase P_t1 ... P_tm) (exponential_pauli_x.hpp, _y.hpp, _z.hpp runtime forms).
+  // One target: the single-qubit kernels.  Several: rotate each X/Y factor into Z
+  // (H for X; S+ then H for Y), gather the parity of the targets into the last one
+  // with CNOTs, apply C...C exp(i phase Z) there, and undo the ladder and the basis
+  // change.  The outer steps need no controls: they cancel where a control is zero.
+  return guarded([&]() -> int {
+    if (!paulis) return fail(RBK_ERR_INVALID, "null Pauli string");
+    if (int rc = check_targets_controls(s, targets, nt, controls, nc)) return rc;
+    std::vector<uint32_t> act;
+    std::vector<char> kind;
+    for (int k = 0; k < nt; ++k) {
+      const char p = paulis[k];
+      if (p == 'I') continue;
+      if (p != 'X' && p != 'Y' && p != 'Z') return fail(RBK_ERR_INVALID, "Pauli string characters must be I, X, Y or Z");
+      act.push_back(targets[k]);
+      kind.push_back(p);
+    }
+    if (act.empty()) {  // exp(i phase I) under the controls: a phase on the all-ones subspace
+      if (nc == 0) {
+        const cplx c = exp_i(phase);
+        double d[4] = {c.real(), c.imag(), c.real(), c.imag()};
+        return rbk_apply_diagonal2(s, d, targets[0], nullptr, 0);
+      }
+      return enqueue_phase(s, exp_i(phase), controls, nc);
+    }
+    const int m = static_cast<int>(act.size());
+    if (m == 1) {
+      if (kind[0] == 'X') return rbk_exponential_pauli_x(s, phase, act[0], controls, nc);
+      if (kind[0] == 'Y') return rbk_exponential_pauli_y(s, phase, act[0], controls, nc);
+      return rbk_exponential_pauli_z(s, phase, act[0], controls, nc);
+    }
+    const cplx sdag[2] = {{1.0, 0.0}, {0.0, -1.0}};
+    for (int k = 0; k < m; ++k) {
+      if (kind[k] == 'Y') {
+        double d[4] = {sdag[0].real(), sdag[0].imag(), sdag[1].real(), sdag[1].imag()};
+        if (int rc = rbk_apply_diagonal2(s, d, act[k], nullptr, 0)) return rc;
+      }
+      if (kind[k] != 'Z')
+        if (int rc = rbk_hadamard(s, act[k], nullptr, 0)) return rc;
+    }
+    for (int k = 0; k + 1 < m; ++k) {
+      const uint32_t c1[1] = {act[k]};
+      if (int rc = enqueue_target(s, rbk::OPK_X, act[k + 1], c1, 1, nullptr)) return rc;
+    }
+    if (int rc = rbk_exponential_pauli_z(s, phase, act[m - 1], controls, nc)) return rc;
+    for (int k = m - 2; k >= 0; --k) {
+      const uint32_t c1[1] = {act[k]};
+      if (int rc = enqueue_target(s, rbk::OPK_X, act[k + 1], c1, 1, nullptr)) return rc;
+    }
+    for (int k = 0; k < m; ++k) {
+      if (kind[k] != 'Z')
+        if (int rc = rbk_hadamard(s, act[k], nullptr, 0)) return rc;
+      if (kind[k] == 'Y') {
+        double d[4] = {1.0, 0.0, 0.0, 1.0};  // S
+        if (int rc = rbk_apply_diagonal2(s, d, act[k], nullptr, 0)) return rc;
+      }
+    }
+    return RBK_OK;
+  });
+}
+
+extern "C" int rbk_exponential_swap(rbk_state* s, double phase, uint32_t q1, uint32_t q2, const uint32_t* controls, int nc)
+{
+  // C...C exp(i phase SWAP) = e^{i phase} on |00>, |11>; [[cos, i sin], [i sin, cos]] on
+  // |01>, |10> (exponential_swap.hpp:37-40, :103).  After CNOT(q1 -> q2) the swapped
+  // pair differs only in q1 with q2 = 1, and |00>, |11> sit at q2 = 0: so
+  // CNOT . [C...C exp(i phase X_q1) controlled by q2 too] . [C...C diag(e^{i phase}, 1) on q2] . CNOT.
+  return guarded([&]() -> int {
+    const uint32_t t[2] = {q1, q2};
+    if (int rc = check_targets_controls(s, t, 2, controls, nc)) return rc;
+    const uint32_t c1[1] = {q1};
+    if (int rc = enqueue_target(s, rbk::OPK_X, q2, c1, 1, nullptr)) return rc;
+    auto cq2 = with_qubit(controls, nc, q2);
+    if (int rc = rbk_exponential_pauli_x(s, phase, q1, cq2.data(), static_cast<int>(cq2.size()))) return rc;
+    const cplx e = exp_i(phase);
+    double d[4] = {e.real(), e.imag(), 1.0, 0.0};
+    if (int rc = rbk_apply_diagonal2(s, d, q2, controls, nc)) return rc;
+    return enqueue_target(s, rbk::OPK_X, q2, c1, 1, nullptr);
+  });
+}
+
+extern "C" int rbk_clear(rbk_state* s, uint32_t qubit)
+{
+  // CLEAR i: ket::gate::clear (ket/include/ket/gate/clear.hpp): qubit i projected onto |0>,
+  // renormalised by p0^(-1/2).
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (qubit >= static_cast<uint32_t>(s->n)) return fail(RBK_ERR_INVALID, "qubit index out of range");
+    if (s->in_fusion) return fail(RBK_ERR_STATE, "CLEAR inside a fusion block");
+    double p0 = 0, p1 = 0;
+    if (int rc = qubit_probabilities(s, qubit, &p0, &p1)) return rc;
+    return collapse(s, qubit, 0, p0);
+  });
+}
+
+extern "C" int rbk_set(rbk_state* s, uint32_t qubit)
+{
+  // SET i: ket::gate::set (ket/include/ket/gate/set.hpp): projected onto |1>, renormalised by p1^(-1/2).
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (qubit >= static_cast<uint32_t>(s->n)) return fail(RBK_ERR_INVALID, "qubit index out of range");
+    if (s->in_fusion) return fail(RBK_ERR_STATE, "SET inside a fusion block");
+    double p0 = 0, p1 = 0;
+    if (int rc = qubit_probabilities(s, qubit, &p0, &p1)) return rc;
+    return collapse(s, qubit, 1, p1);
+  });
+}
+
+extern "C" int rbk_shor_box(rbk_state* s, uint32_t num_exponent_qubits, uint64_t divisor, uint64_t base)
+{
+  // SHORBOX nx N a: ket::ranges::shor_box (ket/include/ket/shor_box.hpp) with the exponent on
+  // the top nx qubits and the modular register on the rest (bra/src/state.cpp, shor_box).
+  // The previous contents are discarded.
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (s->in_fusion) return fail(RBK_ERR_STATE, "SHORBOX inside a fusion block");
+    if (num_exponent_qubits > static_cast<uint32_t>(s->n)) return fail(RBK_ERR_INVALID, "more exponent qubits than qubits");
+    if (divisor == 0 || divisor > (1ull << 32) || base >= (1ull << 32))
+      return fail(RBK_ERR_INVALID, "SHORBOX needs 0 < divisor <= 2^32 and base < 2^32");
+    s->queue.clear();
+    for (int q = 0; q < s->n; ++q) s->perm[q] = s->inv[q] = q;
+    device_guard g(s->device);
+    if (int rc = mark_launch_start(s)) return rc;
+    const uint64_t size = 1ull << s->n;
+    RBK_CUDA(cudaMemsetAsync(s->amps, 0, size * amp_bytes(s->precision), s->stream));
+    const int nx = static_cast<int>(num_exponent_qubits);
+    const double coeff = std::pow(static_cast<double>(1ull << nx), -0.5);
+    const cudaError_t e = s->precision == RBK_C128
+                              ? rbk::launch_shor_box<double>(s->amps, s->n, nx, divisor, base, coeff, s->stream)
+                              : rbk::launch_shor_box<float>(s->amps, s->n, nx, divisor, base, coeff, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "shor box");
+    ++s->stats.kernel_launches;
+    RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
+    return RBK_OK;
   });
 }

@@ -508,3 +508,51 @@ template cudaError_t launch_prob_scan<double>(const void*, uint64_t, double*, do
 template cudaError_t launch_prob_scan<float>(const void*, uint64_t, double*, double*, cudaStream_t);
 
 }  // namespace rbk
+
+namespace rbk {
+
+// ---------------------------------------------------------------------------
+// SHORBOX: ket::shor_box (ket/include/ket/shor_box.hpp) writes, for every
+// exponent e < 2^nx, the amplitude 2^(-nx/2) at the index whose top nx qubits
+// hold e bit-reversed and whose low n - nx qubits hold (base^e mod divisor)
+// truncated to n - nx bits; e = 0 holds 1 (the running value starts at 1 and
+// is reduced only after use).  The reference walks e sequentially; here every
+// thread computes its own power by squaring.  With divisor, base < 2^32 every
+// product stays below 2^64, so the values are the reference's exactly.
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void shor_box_kernel(typename ctype<Real>::c* __restrict__ a, int n, int nx, uint64_t divisor, uint64_t base,
+                                Real coeff)
+{
+  using C = typename ctype<Real>::c;
+  const uint64_t count = 1ull << nx;
+  const int low = n - nx;
+  const uint64_t low_mask = (1ull << low) - 1;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < count; e += stride) {
+    uint64_t v = 1;
+    if (e > 0) {
+      uint64_t x = base % divisor, r = 1 % divisor;
+      for (uint64_t k = e; k; k >>= 1) {
+        if (k & 1) r = r * x % divisor;
+        x = x * x % divisor;
+      }
+      v = r;
+    }
+    const uint64_t rev = nx > 0 ? (__brevll(e) >> (64 - nx)) : 0;
+    a[(rev << low) | (v & low_mask)] = C{coeff, (Real)0};
+  }
+}
+
+template <typename Real>
+cudaError_t launch_shor_box(void* state, int n, int nx, uint64_t divisor, uint64_t base, double coeff, cudaStream_t stream)
+{
+  const uint64_t count = 1ull << nx;
+  shor_box_kernel<Real><<<grid_for(count, 256), 256, 0, stream>>>(static_cast<typename ctype<Real>::c*>(state), n, nx,
+                                                                divisor, base, static_cast<Real>(coeff));
+  return cudaGetLastError();
+}
+template cudaError_t launch_shor_box<double>(void*, int, int, uint64_t, uint64_t, double, cudaStream_t);
+template cudaError_t launch_shor_box<float>(void*, int, int, uint64_t, uint64_t, double, cudaStream_t);
+
+}  // namespace rbk

@@ -24,6 +24,9 @@ struct pauli_terms {
 template <typename Real> cudaError_t launch_tile_pass(void* state, int n, const dev_pass& pass, int shape, cudaStream_t stream);
 template <typename Real> cudaError_t launch_gate(void* state, int n, const gate_rec& g, cudaStream_t stream);
 template <typename Real> cudaError_t launch_set_basis(void* state, int n, uint64_t index, cudaStream_t stream);
+// ket::shor_box on a zeroed state: 2^nx amplitudes of value coeff (divisor, base < 2^32).
+template <typename Real>
+cudaError_t launch_shor_box(void* state, int n, int nx, uint64_t divisor, uint64_t base, double coeff, cudaStream_t stream);
 
 int reduction_blocks();
 

@@ -84,6 +84,17 @@ _SIGNATURES = {
     "rbk_expectation_pauli": ([_P, _I, ctypes.c_char_p, _P, _P], _I),
     "rbk_inner_product": ([_P, _P, _P], _I),
     "rbk_fidelity": ([_P, _P, ctypes.POINTER(_D)], _I),
+    "rbk_x_rotation_half_pi": ([_P, _I, _U32, _U32P, _I], _I),
+    "rbk_y_rotation_half_pi": ([_P, _I, _U32, _U32P, _I], _I),
+    "rbk_sqrt_pauli_x": ([_P, _I, _U32, _U32P, _I], _I),
+    "rbk_sqrt_pauli_y": ([_P, _I, _U32, _U32P, _I], _I),
+    "rbk_sqrt_pauli_z": ([_P, _I, _U32P, _I, _U32P, _I], _I),
+    "rbk_pauli_string": ([_P, ctypes.c_char_p, _U32P, _I, _U32P, _I], _I),
+    "rbk_exponential_pauli_string": ([_P, _D, ctypes.c_char_p, _U32P, _I, _U32P, _I], _I),
+    "rbk_exponential_swap": ([_P, _D, _U32, _U32, _U32P, _I], _I),
+    "rbk_clear": ([_P, _U32], _I),
+    "rbk_set": ([_P, _U32], _I),
+    "rbk_shor_box": ([_P, _U32, _U64, _U64], _I),
     "rbk_state_seed": ([_P, _U64], _I),
     "rbk_generate_events": ([_P, _I, ctypes.c_int64, _P], _I),
     "rbk_measure": ([_P, ctypes.POINTER(_U64)], _I),
@@ -128,6 +139,16 @@ class State:
         self.n = num_qubits
         self.precision = precision
         self.dtype = np.complex128 if precision == C128 else np.complex64
+
+    @classmethod
+    def adopt(cls, handle, num_qubits, precision):
+        """Wraps an rbk_state* created elsewhere (e.g. by rbk_qcx_run); the wrapper owns it."""
+        s = cls.__new__(cls)
+        s.h = handle if isinstance(handle, ctypes.c_void_p) else ctypes.c_void_p(handle)
+        s.n = num_qubits
+        s.precision = precision
+        s.dtype = np.complex128 if precision == C128 else np.complex64
+        return s
 
     def close(self):
         if getattr(self, "h", None):
@@ -310,6 +331,51 @@ class State:
                 self.end_fusion()
             else:
                 raise ValueError(f"unsupported instruction {mnem}")
+
+    # -- further gate families ---------------------------------------------
+    def x_rotation_half_pi(self, t, controls=(), adjoint=False):
+        c, nc = _qarr(controls)
+        _check(lib().rbk_x_rotation_half_pi(self.h, int(adjoint), t, c, nc))
+
+    def y_rotation_half_pi(self, t, controls=(), adjoint=False):
+        c, nc = _qarr(controls)
+        _check(lib().rbk_y_rotation_half_pi(self.h, int(adjoint), t, c, nc))
+
+    def sqrt_pauli_x(self, t, controls=(), adjoint=False):
+        c, nc = _qarr(controls)
+        _check(lib().rbk_sqrt_pauli_x(self.h, int(adjoint), t, c, nc))
+
+    def sqrt_pauli_y(self, t, controls=(), adjoint=False):
+        c, nc = _qarr(controls)
+        _check(lib().rbk_sqrt_pauli_y(self.h, int(adjoint), t, c, nc))
+
+    def sqrt_pauli_z(self, targets, controls=(), adjoint=False):
+        t, nt = _qarr(targets)
+        c, nc = _qarr(controls)
+        _check(lib().rbk_sqrt_pauli_z(self.h, int(adjoint), t, nt, c, nc))
+
+    def pauli_string(self, paulis, targets, controls=()):
+        t, nt = _qarr(targets)
+        c, nc = _qarr(controls)
+        _check(lib().rbk_pauli_string(self.h, paulis.encode(), t, nt, c, nc))
+
+    def exponential_pauli_string(self, phase, paulis, targets, controls=()):
+        t, nt = _qarr(targets)
+        c, nc = _qarr(controls)
+        _check(lib().rbk_exponential_pauli_string(self.h, phase, paulis.encode(), t, nt, c, nc))
+
+    def exponential_swap(self, phase, q1, q2, controls=()):
+        c, nc = _qarr(controls)
+        _check(lib().rbk_exponential_swap(self.h, phase, q1, q2, c, nc))
+
+    def clear(self, q):
+        _check(lib().rbk_clear(self.h, q))
+
+    def set(self, q):
+        _check(lib().rbk_set(self.h, q))
+
+    def shor_box(self, num_exponent_qubits, divisor, base):
+        _check(lib().rbk_shor_box(self.h, num_exponent_qubits, divisor, base))
 
     # -- observables -----------------------------------------------------------
     def norm2(self):

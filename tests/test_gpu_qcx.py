@@ -1,0 +1,114 @@
+"""bra's .qcx programs end to end on the GPU (rbk_qcx_run and bin/rbk-bra)
+against the reference's results for the same text (tests/golden/qcx_*,
+produced by running the reference ket code through oracle/bra_ref.py).
+
+Printed numbers are compared to within one unit of the last printed digit
+(bra prints 3 to 9 digits; a value at a rounding boundary or a signed zero may
+print differently), event indices and measurement results exactly, and the
+final state to 1e-12 (c128) max amplitude error."""
+import glob
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+PROGRAMS = sorted(glob.glob(os.path.join(GOLDEN, "qcx", "*.qcx")))
+TOL64 = 1e-12
+NUM = re.compile(r"^[-+]?(\d+\.?\d*|\.\d+)([eE][-+]?\d+)?$")
+
+
+@pytest.fixture(scope="module")
+def expected():
+    return json.load(open(os.path.join(GOLDEN, "qcx_expected.json"))), dict(np.load(os.path.join(GOLDEN, "qcx_golden.npz")))
+
+
+def last_digit(tok):
+    """Unit in the last printed digit of a decimal token."""
+    mant, _, exp = tok.lower().partition("e")
+    decimals = len(mant.split(".")[1]) if "." in mant else 0
+    return 10.0 ** (-decimals + (int(exp) if exp else 0))
+
+
+def same_output(got, want):
+    gl, wl = got.splitlines(), want.splitlines()
+    assert len(gl) == len(wl), (got, want)
+    for g, w in zip(gl, wl):
+        gt = re.split(r"([\s(),]+)", g)
+        wt = re.split(r"([\s(),]+)", w)
+        assert len(gt) == len(wt), (g, w)
+        for a, b in zip(gt, wt):
+            if NUM.match(b) and NUM.match(a) and not re.match(r"^[01]+$", b):
+                assert abs(float(a) - float(b)) <= max(1e-12, 1.01 * last_digit(b)), (g, w)
+            elif a.strip() != b.strip():
+                assert a == b, (g, w)
+
+
+@pytest.mark.parametrize("path", PROGRAMS, ids=os.path.basename)
+def test_program_vs_reference(pkg, expected, path):
+    exp, arrays = expected
+    name = os.path.basename(path)[:-4]
+    out, state = pkg.qcx.run(open(path).read(), keep_state=True)
+    with state:
+        same_output(out, exp[name]["output"])
+        if exp[name]["amplitudes"]:
+            assert np.abs(state.amplitudes() - arrays[name]).max() <= TOL64
+
+
+@pytest.mark.parametrize("name", ["fused_brick", "bigger_mixed", "every_gate"])
+def test_unfused_execution_agrees(pkg, expected, name):
+    exp, arrays = expected
+    out, state = pkg.qcx.run(open(os.path.join(GOLDEN, "qcx", name + ".qcx")).read(), deferred=False, keep_state=True)
+    with state:
+        same_output(out, exp[name]["output"])
+        assert np.abs(state.amplitudes() - arrays[name]).max() <= TOL64
+
+
+def test_timing_lines_follow_bra(pkg, expected):
+    exp, _ = expected
+    text = open(os.path.join(GOLDEN, "qcx", "measure_and_events.qcx")).read()
+    out, _ = pkg.qcx.run(text, timing=True)
+    timing = re.compile(r"^(Operations|Expectation values|Events|Amplitudes|Measurement) finished: \S+ \(\S+\)$")
+    lines = out.splitlines()
+    assert sum(bool(timing.match(line)) for line in lines) == 4
+    same_output("\n".join(line for line in lines if not timing.match(line)) + "\n", exp["measure_and_events"]["output"])
+
+
+def test_c64_program_within_float_tolerance(pkg, expected):
+    exp, arrays = expected
+    out, state = pkg.qcx.run(open(os.path.join(GOLDEN, "qcx", "fused_brick.qcx")).read(), precision=pkg.C64,
+                             keep_state=True)
+    with state:
+        a = state.amplitudes().astype(np.complex128)
+        ref = arrays["fused_brick"]
+        assert np.abs(a - ref).max() <= 2e-5
+        assert abs(np.vdot(ref, a)) ** 2 / np.vdot(a, a).real >= 1 - 1e-9
+
+
+def test_command_line_drop_in(pkg, expected):
+    exp, _ = expected
+    exe = os.path.join(ROOT, "riken-braket_b200", "bin", "rbk-bra")
+    for name in ("hadamards8", "shor_program", "exit_program"):
+        path = os.path.join(GOLDEN, "qcx", name + ".qcx")
+        r = subprocess.run([exe, "--file", path, "--no-timing", "--threads", "4"], capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr
+        same_output(r.stdout, exp[name]["output"])
+    r = subprocess.run([exe, "--no-timing"], input="QUBITS 2\nH 0\nCNOT 0 1\nBOGUS 1\n", capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 1 and "line 4" in r.stderr
+
+
+def test_seed_option_changes_the_state_generator(pkg):
+    text = "QUBITS 6\n" + "".join("H %d\n" % q for q in range(6)) + "GENERATE EVENTS 30 -1\n"
+    a, _ = pkg.qcx.run(text, seed=1)
+    b, _ = pkg.qcx.run(text, seed=2)
+    c, _ = pkg.qcx.run(text, seed=1)
+    assert a == c and a != b
