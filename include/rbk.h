@@ -259,6 +259,37 @@ int rbk_adjoint_gradient(int num_qubits, int precision, int device, const rbk_ci
                          const double* theta, int num_params, int num_terms, const char* strings,
                          const double* coeffs, double* energy, double* grad);
 
+/* ---- batches of parametrised circuits (no counterpart in the reference) -----
+ * Energies and adjoint gradients of many independent circuits of uneven size,
+ * each with its own parameters and observable (same conventions as
+ * rbk_adjoint_gradient).  Instances with n <= 12 (c128) / n <= 13 (c64) run in
+ * one persistent kernel launch, replayed from a CUDA graph, one CTA per
+ * instance with both state vectors in shared memory; the CTA size is chosen by
+ * timing the candidates at rbk_batch_create.  Larger instances run through
+ * rbk_adjoint_gradient.  Parameters and gradients are concatenated in instance
+ * order. */
+typedef struct rbk_batch rbk_batch;
+typedef struct rbk_batch_instance {
+  int32_t num_qubits;
+  int32_t num_gates;
+  const rbk_circuit_gate* gates;
+  int32_t num_params;
+  int32_t num_terms;
+  const char* strings;   /* num_terms strings of num_qubits characters */
+  const double* coeffs;  /* num_terms (re, im) */
+} rbk_batch_instance;
+typedef struct rbk_batch_stats {
+  int num_small;       /* instances in the persistent launch */
+  int num_large;       /* instances through rbk_adjoint_gradient */
+  int threads;         /* CTA size picked by the autotuner */
+  float small_ms;      /* device time of the persistent launch when tuned */
+  double last_run_ms;  /* host wall time of the last rbk_batch_run */
+} rbk_batch_stats;
+int rbk_batch_create(int precision, int device, int num_instances, const rbk_batch_instance* instances, rbk_batch** out);
+int rbk_batch_run(rbk_batch* batch, const double* theta, double* energies, double* grads);
+int rbk_batch_get_stats(const rbk_batch* batch, rbk_batch_stats* out);
+int rbk_batch_destroy(rbk_batch* batch);
+
 /* Pauli-string expectation value of a caller-owned device state, with no
  * device memory allocated.  No counterpart in the reference: it exists for
  * callers that cannot allocate when they need the value -- code in a CUDA

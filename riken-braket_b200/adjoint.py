@@ -79,6 +79,78 @@ def adjoint_gradient(n, spec, theta, terms, precision=rbk.C128, device=0):
     return energy.value, grad
 
 
+class BatchInstance(ctypes.Structure):
+    _fields_ = [("num_qubits", ctypes.c_int32), ("num_gates", ctypes.c_int32), ("gates", ctypes.c_void_p),
+                ("num_params", ctypes.c_int32), ("num_terms", ctypes.c_int32), ("strings", ctypes.c_char_p),
+                ("coeffs", ctypes.c_void_p)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("num_small", ctypes.c_int), ("num_large", ctypes.c_int), ("threads", ctypes.c_int),
+                ("small_ms", ctypes.c_float), ("last_run_ms", ctypes.c_double)]
+
+
+class Batch:
+    """Many parametrised circuits at once (rbk_batch_*): instances is a list of
+    (num_qubits, spec, num_params, terms) with spec as for adjoint_gradient."""
+
+    def __init__(self, instances, precision=rbk.C128, device=0):
+        L = rbk.lib()
+        L.rbk_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.rbk_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.rbk_batch_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(BatchStats)]
+        L.rbk_batch_destroy.argtypes = [ctypes.c_void_p]
+        self._keep = []
+        arr = (BatchInstance * max(1, len(instances)))()
+        self.num_params = []
+        for i, (n, spec, num_params, terms) in enumerate(instances):
+            gates, count = gate_array(spec)
+            strings = b"".join(t.encode() for t, _ in terms)
+            coeffs = np.array([[complex(c).real, complex(c).imag] for _, c in terms], dtype=np.float64).ravel()
+            self._keep += [gates, strings, coeffs]
+            arr[i].num_qubits, arr[i].num_gates, arr[i].gates = n, count, ctypes.cast(gates, ctypes.c_void_p)
+            arr[i].num_params, arr[i].num_terms = num_params, len(terms)
+            arr[i].strings, arr[i].coeffs = strings, coeffs.ctypes.data
+            self.num_params.append(num_params)
+        h = ctypes.c_void_p()
+        rc = L.rbk_batch_create(precision, device, len(instances), ctypes.cast(arr, ctypes.c_void_p), ctypes.byref(h))
+        if rc != 0:
+            raise rbk.RbkError(rc, L.rbk_last_error().decode())
+        self.h = h
+        self.count = len(instances)
+
+    def run(self, thetas):
+        """thetas: list of per-instance parameter arrays.  Returns (energies, list of gradients)."""
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(t, dtype=np.float64) for t in thetas])
+                                    if thetas else np.zeros(0), dtype=np.float64)
+        energies = np.zeros(self.count, dtype=np.float64)
+        grads = np.zeros(max(1, flat.size), dtype=np.float64)
+        rc = rbk.lib().rbk_batch_run(self.h, flat.ctypes.data, energies.ctypes.data, grads.ctypes.data)
+        if rc != 0:
+            raise rbk.RbkError(rc, rbk.lib().rbk_last_error().decode())
+        out, k = [], 0
+        for p in self.num_params:
+            out.append(grads[k:k + p].copy())
+            k += p
+        return energies, out
+
+    def stats(self):
+        st = BatchStats()
+        rbk.lib().rbk_batch_get_stats(self.h, ctypes.byref(st))
+        return {f: getattr(st, f) for f, _ in BatchStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            rbk.lib().rbk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def make_autograd_function():
     """torch.autograd.Function over adjoint_gradient (gradient-check harness only)."""
     import torch

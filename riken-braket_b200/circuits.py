@@ -124,6 +124,21 @@ def ansatz_hamiltonian(n):
     return terms
 
 
+def batch_instances(count=4096, n_min=10, n_max=24, depth_min=4, depth_max=16, seed_base=1):
+    """Config-5 style batch: instance i draws, from its own generator seeded
+    seed_base + i, a qubit count n = round(exp(U[ln n_min, ln n_max])), a depth
+    U{depth_min..depth_max} and 2 n depth ansatz parameters U[-pi, pi).
+    Returns a list of (n, layers, thetas)."""
+    out = []
+    for i in range(count):
+        rng = _rng(seed_base + i)
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        layers = int(rng.integers(depth_min, depth_max + 1))
+        thetas = rng.uniform(-math.pi, math.pi, size=2 * n * layers)
+        out.append((n, layers, thetas))
+    return out
+
+
 def random_circuit(n, count, seed=1, kinds=None):
     """Random mix of the hot-path instructions (parity tests)."""
     rng = _rng(seed)
