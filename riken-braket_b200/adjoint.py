@@ -134,6 +134,13 @@ class Batch:
             k += p
         return energies, out
 
+    def set_workers(self, workers):
+        L = rbk.lib()
+        L.rbk_batch_set_workers.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        rc = L.rbk_batch_set_workers(self.h, workers)
+        if rc != 0:
+            raise rbk.RbkError(rc, L.rbk_last_error().decode())
+
     def stats(self):
         st = BatchStats()
         rbk.lib().rbk_batch_get_stats(self.h, ctypes.byref(st))

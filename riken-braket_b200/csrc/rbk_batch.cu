@@ -26,14 +26,18 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <exception>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "rbk.h"
+#include "rbk_adjoint.h"
 #include "rbk_device.cuh"
 #include "rbk_kernels.h"
 
@@ -352,9 +356,15 @@ struct rbk_batch {
   std::vector<std::string> large_strings;
   std::vector<std::vector<double>> large_coeffs;
   rbk_batch_stats stats{};
+  // Worker threads for the large instances, each with its own workspaces by size.
+  int workers = 4;
+  std::vector<std::map<int, rbk::adjoint_workspace*>> pools;
 
   ~rbk_batch()
   {
+    cudaSetDevice(device);
+    for (auto& pool : pools)
+      for (auto& kv : pool) rbk::adjoint_workspace_destroy(kv.second);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (h_theta) cudaFreeHost(h_theta);
@@ -492,6 +502,8 @@ extern "C" int rbk_batch_create(int precision, int device, int num_instances, co
     }
     b->small_count = static_cast<int>(small.size());
     b->small_out = small;
+    std::stable_sort(b->large.begin(), b->large.end(),
+                     [&](int x, int y) { return instances[x].num_qubits > instances[y].num_qubits; });
     for (int li : b->large) {
       const auto& I = instances[li];
       b->large_gates.emplace_back(I.gates, I.gates + I.num_gates);
@@ -578,16 +590,50 @@ extern "C" int rbk_batch_run(rbk_batch* b, const double* theta, double* energies
     const size_t np = static_cast<size_t>(b->total_params);
     if (np) std::memcpy(b->h_theta, theta, sizeof(double) * np);
     if (b->small_count > 0 && cudaGraphLaunch(b->exec, b->stream) != cudaSuccess) return fail(RBK_ERR_CUDA, "graph launch");
-    // Large instances meanwhile, through the engine's adjoint sweep.
-    for (size_t k = 0; k < b->large.size(); ++k) {
-      const int i = b->large[k];
-      const int pb = b->param_begin[i];
-      const auto& gs = b->large_gates[k];
-      const int nq = static_cast<int>(b->large_strings[k].size() / (b->large_coeffs[k].size() / 2));
-      if (int rc = rbk_adjoint_gradient(nq, b->precision, b->device, gs.data(), static_cast<int>(gs.size()), theta + pb,
-                                        b->num_params[i], static_cast<int>(b->large_coeffs[k].size() / 2),
-                                        b->large_strings[k].data(), b->large_coeffs[k].data(), &energies[i], grads + pb))
-        return rc;
+    // Large instances meanwhile, through the engine's adjoint sweep: worker
+    // threads take them largest first, each on its own streams and reusable
+    // state pairs, so that host planning overlaps device work.
+    if (!b->large.empty()) {
+      if (b->pools.empty()) b->pools.resize(static_cast<size_t>(b->workers));
+      std::atomic<size_t> next{0};
+      std::atomic<int> first_rc{RBK_OK};
+      std::mutex err_mu;
+      std::string err;
+      auto work = [&](int wid) {
+        cudaSetDevice(b->device);
+        auto& pool = b->pools[static_cast<size_t>(wid)];
+        while (first_rc.load() == RBK_OK) {
+          const size_t k = next.fetch_add(1);
+          if (k >= b->large.size()) break;
+          const int i = b->large[k];
+          const int pb = b->param_begin[i];
+          const auto& gs = b->large_gates[k];
+          const int nt = static_cast<int>(b->large_coeffs[k].size() / 2);
+          const int nq = static_cast<int>(b->large_strings[k].size() / static_cast<size_t>(nt));
+          int rc = RBK_OK;
+          auto it = pool.find(nq);
+          if (it == pool.end()) {
+            rbk::adjoint_workspace* w = nullptr;
+            rc = rbk::adjoint_workspace_create(nq, b->precision, b->device, &w);
+            if (rc == RBK_OK) it = pool.emplace(nq, w).first;
+          }
+          if (rc == RBK_OK)
+            rc = rbk::adjoint_run(it->second, gs.data(), static_cast<int>(gs.size()), theta + pb, b->num_params[i], nt,
+                                  b->large_strings[k].data(), b->large_coeffs[k].data(), &energies[i], grads + pb);
+          if (rc != RBK_OK) {
+            int expected = RBK_OK;
+            if (first_rc.compare_exchange_strong(expected, rc)) {
+              std::lock_guard<std::mutex> lk(err_mu);
+              err = rbk_last_error();
+            }
+          }
+        }
+      };
+      std::vector<std::thread> threads;
+      for (int t = 1; t < b->workers; ++t) threads.emplace_back(work, t);
+      work(0);
+      for (auto& t : threads) t.join();
+      if (first_rc.load() != RBK_OK) return fail(first_rc.load(), "batch: " + err);
     }
     if (b->small_count > 0) {
       if (int rc = sync_bounded(b->stream)) return rc;
@@ -605,6 +651,17 @@ extern "C" int rbk_batch_run(rbk_batch* b, const double* theta, double* energies
   } catch (std::exception const& e) {
     return fail(RBK_ERR_STATE, e.what());
   }
+}
+
+extern "C" int rbk_batch_set_workers(rbk_batch* b, int workers)
+{
+  if (!b || workers < 1 || workers > 64) return fail(RBK_ERR_INVALID, "workers must be between 1 and 64");
+  cudaSetDevice(b->device);
+  for (auto& pool : b->pools)
+    for (auto& kv : pool) rbk::adjoint_workspace_destroy(kv.second);
+  b->pools.clear();
+  b->workers = workers;
+  return RBK_OK;
 }
 
 extern "C" int rbk_batch_get_stats(const rbk_batch* b, rbk_batch_stats* out)

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -11,11 +12,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <memory>
 #include <random>
 #include <string>
 #include <thread>
 #include <vector>
 
+#include "rbk_adjoint.h"
 #include "rbk_internal.h"
 #include "rbk_kernels.h"
 #include "rbk_plan.h"
@@ -1011,11 +1014,170 @@ struct device_buffer {
 
 }  // namespace
 
-extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, const rbk_circuit_gate* gates,
-                                    int num_gates, const double* theta, int num_params, int num_terms,
-                                    const char* strings, const double* coeffs, double* energy, double* grad)
+// Tile bits of the tiled overlap launches (both states of a tile in shared memory).
+constexpr int kOverlapTileBits128 = 11, kOverlapTileBits64 = 12;
+
+// Overlaps of one group on the device, with as few reads of the states as
+// possible: one tiled launch covers every overlap whose flip bit is among the
+// launch's tile bits (the low coalescing bits plus up to K - LOW chosen ones);
+// Z-type overlaps (no flip) ride along in the first launch.
+int launch_group_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
+                          const std::vector<rbk::overlap_spec>& specs, int first_slot, double* ov, double* mpart,
+                          double* tpart);
+
+// Two states of one size on one stream plus the sweep's device buffers, kept
+// between calls so that repeated gradients (batches, optimiser loops)
+// allocate nothing.
+struct rbk::adjoint_workspace {
+  int n = 0, precision = RBK_C128, device = 0;
+  rbk_state* psi = nullptr;
+  rbk_state* lam = nullptr;
+  double* ov = nullptr;  // (re, im) of <lambda|P|psi> per parametrised gate, then E
+  int ov_cap = 0;
+  double* mpart = nullptr;
+  double* tpart = nullptr;  // tiled overlaps (n >= tile bits)
+  ~adjoint_workspace()
+  {
+    if (ov) cudaFree(ov);
+    if (mpart) cudaFree(mpart);
+    if (tpart) cudaFree(tpart);
+    if (lam) rbk_state_destroy(lam);
+    if (psi) rbk_state_destroy(psi);
+  }
+};
+
+int launch_group_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
+                          const std::vector<rbk::overlap_spec>& specs, int first_slot, double* ov, double* mpart,
+                          double* tpart)
+{
+  const bool c128 = w.precision == RBK_C128;
+  const int n = w.n;
+  const int K = c128 ? kOverlapTileBits128 : kOverlapTileBits64;
+  const int LOW = c128 ? rbk::precision_traits<double>::LOW : rbk::precision_traits<float>::LOW;
+  cudaError_t e = cudaSuccess;
+  if (n < K || !tpart) {
+    for (size_t c0 = 0; c0 < specs.size(); c0 += rbk::kMaxOverlaps) {
+      rbk::overlap_set set{};
+      set.count = static_cast<int>(std::min<size_t>(rbk::kMaxOverlaps, specs.size() - c0));
+      for (int y = 0; y < set.count; ++y) set.spec[y] = specs[c0 + y];
+      double* out = ov + 2 * (first_slot + c0);
+      e = c128 ? rbk::launch_overlaps<double>(lam->amps, psi->amps, n, set, mpart, out, psi->stream)
+               : rbk::launch_overlaps<float>(lam->amps, psi->amps, n, set, mpart, out, psi->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "overlaps");
+    }
+    return RBK_OK;
+  }
+  std::vector<int> high;
+  for (const auto& sp : specs)
+    if (sp.flip) {
+      const int b = __builtin_ctzll(sp.flip);
+      if (b >= LOW && std::find(high.begin(), high.end(), b) == high.end()) high.push_back(b);
+    }
+  std::sort(high.begin(), high.end());
+  const int per = K - LOW;
+  const int chunks = std::max<int>(1, static_cast<int>((high.size() + per - 1) / per));
+  std::vector<char> done(specs.size(), 0);
+  for (int c = 0; c < chunks; ++c) {
+    uint64_t tmask = (1ull << LOW) - 1;
+    int tile_phys[16];
+    int k = 0;
+    for (int b = 0; b < LOW; ++b) tile_phys[k++] = b;
+    for (size_t h = static_cast<size_t>(c) * per; h < high.size() && h < static_cast<size_t>(c + 1) * per; ++h) {
+      tile_phys[k++] = high[h];
+      tmask |= 1ull << high[h];
+    }
+    for (int b = LOW; b < n && k < K; ++b)
+      if (!(tmask & (1ull << b))) { tile_phys[k++] = b; tmask |= 1ull << b; }
+    rbk::tile_overlap_set base{};
+    base.K = K;
+    for (int b = 0; b < K; ++b) base.tile_phys[b] = static_cast<uint8_t>(tile_phys[b]);
+    int src = 0;
+    for (int b = 0; b < n;) {
+      if (tmask & (1ull << b)) { ++b; continue; }
+      int len = 0;
+      while (b + len < n && !(tmask & (1ull << (b + len)))) ++len;
+      base.run_src[base.num_runs] = static_cast<uint8_t>(src);
+      base.run_len[base.num_runs] = static_cast<uint8_t>(len);
+      base.run_dst[base.num_runs] = static_cast<uint8_t>(b);
+      ++base.num_runs;
+      src += len;
+      b += len;
+    }
+    auto local = [&](uint64_t mask) {
+      uint32_t m = 0;
+      for (int t = 0; t < K; ++t)
+        if (mask & (1ull << tile_phys[t])) m |= 1u << t;
+      return m;
+    };
+    std::vector<size_t> mine;
+    for (size_t y = 0; y < specs.size(); ++y) {
+      if (done[y]) continue;
+      const uint64_t f = specs[y].flip;
+      if ((f == 0 && c == 0) || (f != 0 && (f & tmask) == f)) { mine.push_back(y); done[y] = 1; }
+    }
+    for (size_t c0 = 0; c0 < mine.size(); c0 += rbk::kMaxOverlaps) {
+      rbk::tile_overlap_set set = base;
+      set.count = static_cast<int>(std::min<size_t>(rbk::kMaxOverlaps, mine.size() - c0));
+      for (int y = 0; y < set.count; ++y) {
+        const auto& sp = specs[mine[c0 + y]];
+        auto& t = set.spec[y];
+        t.flip_local = local(sp.flip);
+        t.sign_local = local(sp.sign);
+        t.sign = sp.sign & ~tmask;
+        t.wr = sp.wr;
+        t.wi = sp.wi;
+        t.out_slot = first_slot + static_cast<int>(mine[c0 + y]);
+      }
+      e = c128 ? rbk::launch_tile_overlaps<double>(lam->amps, psi->amps, n, set, tpart, ov, psi->stream)
+               : rbk::launch_tile_overlaps<float>(lam->amps, psi->amps, n, set, tpart, ov, psi->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "tiled overlaps");
+    }
+  }
+  for (size_t y = 0; y < specs.size(); ++y)
+    if (!done[y]) return fail(RBK_ERR_STATE, "adjoint sweep: an overlap was not scheduled");
+  return RBK_OK;
+}
+
+int rbk::adjoint_workspace_create(int num_qubits, int precision, int device, adjoint_workspace** out)
 {
   return guarded([&]() -> int {
+    if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    auto w = std::make_unique<adjoint_workspace>();
+    w->n = num_qubits;
+    w->precision = precision;
+    w->device = device;
+    if (int rc = rbk_state_create(num_qubits, precision, 0, device, &w->psi)) return rc;
+    if (int rc = rbk_state_create(num_qubits, precision, 0, device, &w->lam)) return rc;
+    device_guard dg(device);
+    // One stream for both states: every kernel of the sweep is ordered without host waits.
+    cudaStreamSynchronize(w->lam->stream);
+    cudaStreamDestroy(w->lam->stream);
+    w->lam->stream = w->psi->stream;
+    w->lam->owns_stream = false;
+    RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&w->mpart), sizeof(double) * rbk::overlaps_partials_doubles()));
+    const int K = precision == RBK_C128 ? kOverlapTileBits128 : kOverlapTileBits64;
+    if (num_qubits >= K)
+      RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&w->tpart), sizeof(double) * rbk::tile_overlaps_partials_doubles(num_qubits, K)));
+    *out = w.release();
+    return RBK_OK;
+  });
+}
+
+void rbk::adjoint_workspace_destroy(adjoint_workspace* w)
+{
+  if (!w) return;
+  device_guard dg(w->device);
+  delete w;
+}
+
+int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int num_gates, const double* theta,
+                     int num_params, int num_terms, const char* strings, const double* coeffs, double* energy,
+                     double* grad)
+{
+  return guarded([&]() -> int {
+    if (!w) return fail(RBK_ERR_INVALID, "null workspace");
+    const int num_qubits = w->n, precision = w->precision;
     if (num_gates < 0 || (num_gates > 0 && !gates) || num_params < 0 || (num_params > 0 && (!theta || !grad)) ||
         num_terms < 1 || !strings || !coeffs || !energy)
       return fail(RBK_ERR_INVALID, "bad adjoint-gradient arguments");
@@ -1063,20 +1225,21 @@ extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, c
       H.begin[H.num_groups] = nt;
     }
 
-    state_guard psi, lam;
-    if (int rc = rbk_state_create(num_qubits, precision, 0, device, &psi.s)) return rc;
-    if (int rc = rbk_state_create(num_qubits, precision, 0, device, &lam.s)) return rc;
-    device_guard dg(device);
-    // One stream for both states: every kernel below is ordered without host waits.
-    cudaStreamSynchronize(lam.s->stream);
-    cudaStreamDestroy(lam.s->stream);
-    lam.s->stream = psi.s->stream;
-    lam.s->owns_stream = false;
+    struct { rbk_state* s; } psi{w->psi}, lam{w->lam};
+    device_guard dg(w->device);
+    if (int rc = rbk_state_reset(psi.s, 0)) return rc;
+    if (int rc = rbk_state_reset(lam.s, 0)) return rc;
 
     int num_pg = 0;
     for (int i = 0; i < num_gates; ++i) num_pg += gates[i].param >= 0 ? 1 : 0;
-    device_buffer ov;  // (re, im) of <lambda|P|psi> per parametrised gate, then E
-    RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&ov.p), sizeof(double) * 2 * (num_pg + 1)));
+    if (w->ov_cap < num_pg + 1) {
+      if (w->ov) cudaFree(w->ov);
+      w->ov = nullptr;
+      w->ov_cap = 0;
+      RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&w->ov), sizeof(double) * 2 * (num_pg + 1)));
+      w->ov_cap = num_pg + 1;
+    }
+    struct { double* p; } ov{w->ov};
 
     for (int i = 0; i < num_gates; ++i)
       if (int rc = apply_circuit_gate(psi.s, gates[i], theta, false)) return rc;
@@ -1093,27 +1256,57 @@ extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, c
     std::vector<int> slot_param(num_pg);
     std::vector<double> slot_scale(num_pg);
     int slot = num_pg;
-    for (int i = num_gates - 1; i >= 0; --i) {
-      const auto& g = gates[i];
-      if (g.param >= 0) {
+    struct { double* p; } mpart{w->mpart};  // partial sums of the grouped overlaps
+    auto single_qubit = [](const rbk_circuit_gate& g) {
+      return g.kind == RBK_GATE_H || g.kind == RBK_GATE_X || g.kind == RBK_GATE_Y || g.kind == RBK_GATE_Z ||
+             g.kind == RBK_GATE_U1 || g.kind == RBK_GATE_U2 || g.kind == RBK_GATE_U3 || g.kind == RBK_GATE_EX ||
+             g.kind == RBK_GATE_EY || g.kind == RBK_GATE_EZ;
+    };
+    int i = num_gates - 1;
+    while (i >= 0) {
+      // A run of single-qubit gates on distinct qubits commutes gate by gate, so
+      // every rotation in it sees the same (psi, lambda) pair -- the one after the
+      // run -- and all its overlaps come from one launch: for rotation k,
+      // <lambda_k|P_k|psi_k> = <lambda|G P_k G^dagger|psi> with G the later gates
+      // of the run, which act on other qubits.
+      int j = i;
+      uint64_t used = 0;
+      while (j >= 0 && single_qubit(gates[j]) && !(used & (1ull << gates[j].qubits[0]))) {
+        used |= 1ull << gates[j].qubits[0];
+        --j;
+      }
+      if (j == i) j = i - 1;  // a gate on two qubits: no rotation, un-applied below
+      std::vector<rbk::overlap_spec> specs;
+      int first = slot;
+      for (int k = i; k > j; --k)
+        if (gates[k].param >= 0) --first;
+      if (first < slot) {
         if (int rc = flush(psi.s)) return rc;
         if (int rc = flush(lam.s)) return rc;
         if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
-        --slot;
-        slot_param[slot] = g.param;
-        slot_scale[slot] = g.scale;
-        const uint64_t t = 1ull << psi.s->perm[g.qubits[0]];
-        uint64_t flip = 0, sign = 0;
-        double wr = 1.0, wi = 0.0;
-        if (g.kind == RBK_GATE_EX) flip = t;
-        else if (g.kind == RBK_GATE_EY) { flip = t; sign = t; wr = 0.0; wi = -1.0; }
-        else sign = t;  // EZ
-        e = c128 ? rbk::launch_overlap<double>(lam.s->amps, psi.s->amps, num_qubits, flip, sign, wr, wi, psi.s->d_partials, ov.p + 2 * slot, psi.s->stream)
-                 : rbk::launch_overlap<float>(lam.s->amps, psi.s->amps, num_qubits, flip, sign, wr, wi, psi.s->d_partials, ov.p + 2 * slot, psi.s->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "overlap");
+        specs.resize(static_cast<size_t>(slot - first));
+        int y = slot - first;
+        for (int k = i; k > j; --k) {
+          const auto& g = gates[k];
+          if (g.param < 0) continue;
+          --y;
+          slot_param[first + y] = g.param;
+          slot_scale[first + y] = g.scale;
+          const uint64_t t = 1ull << psi.s->perm[g.qubits[0]];
+          rbk::overlap_spec& sp = specs[static_cast<size_t>(y)];
+          sp = rbk::overlap_spec{0, 0, 1.0, 0.0};
+          if (g.kind == RBK_GATE_EX) sp.flip = t;
+          else if (g.kind == RBK_GATE_EY) { sp.flip = t; sp.sign = t; sp.wr = 0.0; sp.wi = -1.0; }
+          else sp.sign = t;  // EZ
+        }
+        if (int rc = launch_group_overlaps(*w, lam.s, psi.s, specs, first, ov.p, mpart.p, w->tpart)) return rc;
+        slot = first;
       }
-      if (int rc = apply_circuit_gate(psi.s, g, theta, true)) return rc;
-      if (int rc = apply_circuit_gate(lam.s, g, theta, true)) return rc;
+      for (int k = i; k > j; --k) {
+        if (int rc = apply_circuit_gate(psi.s, gates[k], theta, true)) return rc;
+        if (int rc = apply_circuit_gate(lam.s, gates[k], theta, true)) return rc;
+      }
+      i = j;
     }
     std::vector<double> host(2 * (num_pg + 1));
     RBK_CUDA(cudaMemcpyAsync(host.data(), ov.p, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, psi.s->stream));
@@ -1123,6 +1316,17 @@ extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, c
     for (int j = 0; j < num_pg; ++j) grad[slot_param[j]] += -2.0 * slot_scale[j] * host[2 * j + 1];
     return RBK_OK;
   });
+}
+
+extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, const rbk_circuit_gate* gates,
+                                    int num_gates, const double* theta, int num_params, int num_terms,
+                                    const char* strings, const double* coeffs, double* energy, double* grad)
+{
+  rbk::adjoint_workspace* w = nullptr;
+  if (int rc = rbk::adjoint_workspace_create(num_qubits, precision, device, &w)) return rc;
+  const int rc = rbk::adjoint_run(w, gates, num_gates, theta, num_params, num_terms, strings, coeffs, energy, grad);
+  rbk::adjoint_workspace_destroy(w);
+  return rc;
 }
 
 // ---- sampling and measurement ------------------------------------------------

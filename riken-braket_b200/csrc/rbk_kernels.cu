@@ -8,6 +8,8 @@
 //                      with FP64 accumulation, per-block partials reduced in a
 //                      fixed order (deterministic).
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <cstdint>
 
 #include "rbk_device.cuh"
@@ -361,6 +363,153 @@ cudaError_t launch_overlap(const void* lam, const void* psi, int n, uint64_t fli
   finish_partials_kernel<<<1, 32, 0, stream>>>(partials, blocks, 2, out);
   return cudaGetLastError();
 }
+
+// Several overlaps in one launch: blockIdx.y selects the Pauli of overlap y;
+// partials of overlap y sit at partials[(y * gridDim.x + x) * 2].
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads)
+overlaps_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename ctype<Real>::c* __restrict__ psi,
+                uint64_t size, const __grid_constant__ overlap_set S, double* partials)
+{
+  const overlap_spec P = S.spec[blockIdx.y];
+  double re = 0, im = 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += stride) {
+    const auto l = lam[i], p = psi[i ^ P.flip];
+    const double s = (__popcll(i & P.sign) & 1) ? -1.0 : 1.0;
+    const double cr = double(l.x) * double(p.x) + double(l.y) * double(p.y);
+    const double ci = double(l.x) * double(p.y) - double(l.y) * double(p.x);
+    re += s * (cr * P.wr - ci * P.wi);
+    im += s * (cr * P.wi + ci * P.wr);
+  }
+  double vals[2] = {re, im};
+  block_sum_store<2>(vals, 2, partials + (size_t(blockIdx.y) * gridDim.x + blockIdx.x) * 2);
+}
+
+// out[2y], out[2y+1] = sum over the partials of overlap y, in block order.
+__global__ void finish_overlaps_kernel(const double* __restrict__ partials, int blocks, double* __restrict__ out)
+{
+  if (threadIdx.x >= 2) return;
+  const double* p = partials + size_t(blockIdx.x) * blocks * 2 + threadIdx.x;
+  double acc = 0;
+  for (int b = 0; b < blocks; ++b) acc += p[2 * b];
+  out[2 * blockIdx.x + threadIdx.x] = acc;
+}
+
+size_t overlaps_partials_doubles() { return size_t(reduction_blocks()) * 2 * kMaxOverlaps; }
+
+template <typename Real>
+cudaError_t launch_overlaps(const void* lam, const void* psi, int n, const overlap_set& set, double* partials, double* out,
+                            cudaStream_t stream)
+{
+  if (set.count < 1 || set.count > kMaxOverlaps) return cudaErrorInvalidValue;
+  const int blocks = reduction_blocks();
+  overlaps_kernel<Real><<<dim3(blocks, set.count), kRedThreads, 0, stream>>>(
+    static_cast<const typename ctype<Real>::c*>(lam), static_cast<const typename ctype<Real>::c*>(psi), 1ull << n, set,
+    partials);
+  finish_overlaps_kernel<<<set.count, 32, 0, stream>>>(partials, blocks, out);
+  return cudaGetLastError();
+}
+// Tiled form: CTA b stages the tile of psi and lambda whose bits outside
+// T.tile_phys spell b (as a fused pass does) and evaluates every overlap of
+// the set whose flip bit is a tile bit, reading each state once for the whole
+// set instead of once per overlap.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads)
+tile_overlaps_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename ctype<Real>::c* __restrict__ psi,
+                     const __grid_constant__ tile_overlap_set T, double* partials)
+{
+  using C = typename ctype<Real>::c;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* ps = reinterpret_cast<C*>(smem_raw);
+  C* ls = ps + (1u << T.K);
+  __shared__ double red[kMaxOverlaps][kRedThreads / 32][2];
+  const uint32_t tile = 1u << T.K;
+  uint64_t base = 0;
+  {
+    const uint64_t b = blockIdx.x;
+    for (int r = 0; r < T.num_runs; ++r) base |= ((b >> T.run_src[r]) & ((1ull << T.run_len[r]) - 1)) << T.run_dst[r];
+  }
+  auto phys_of = [&](uint32_t j) {
+    uint64_t p = base;
+    for (int b = 0; b < T.K; ++b) p |= uint64_t((j >> b) & 1u) << T.tile_phys[b];
+    return p;
+  };
+  for (uint32_t j = threadIdx.x; j < tile; j += blockDim.x) {
+    const uint64_t p = phys_of(j);
+    ps[j] = psi[p];
+    ls[j] = lam[p];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int y = 0; y < T.count; ++y) {
+    const tile_overlap_spec S = T.spec[y];
+    const double base_sign = (__popcll(base & S.sign) & 1) ? -1.0 : 1.0;
+    double re = 0, im = 0;
+    for (uint32_t j = threadIdx.x; j < tile; j += blockDim.x) {
+      const C l = ls[j], p = ps[j ^ S.flip_local];
+      const double s = (__popc(j & S.sign_local) & 1) ? -base_sign : base_sign;
+      const double cr = double(l.x) * double(p.x) + double(l.y) * double(p.y);
+      const double ci = double(l.x) * double(p.y) - double(l.y) * double(p.x);
+      re += s * (cr * S.wr - ci * S.wi);
+      im += s * (cr * S.wi + ci * S.wr);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      re += __shfl_xor_sync(0xffffffffu, re, o);
+      im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) { red[y][warp][0] = re; red[y][warp][1] = im; }
+  }
+  __syncthreads();
+  for (int y = threadIdx.x; y < T.count; y += blockDim.x) {
+    double re = 0, im = 0;
+    for (int w = 0; w < kRedThreads / 32; ++w) { re += red[y][w][0]; im += red[y][w][1]; }
+    partials[(size_t(y) * gridDim.x + blockIdx.x) * 2] = re;
+    partials[(size_t(y) * gridDim.x + blockIdx.x) * 2 + 1] = im;
+  }
+}
+
+__global__ void finish_tile_overlaps_kernel(const double* __restrict__ partials, int blocks,
+                                            const __grid_constant__ tile_overlap_set T, double* __restrict__ out)
+{
+  if (threadIdx.x >= 2) return;
+  const double* p = partials + size_t(blockIdx.x) * blocks * 2 + threadIdx.x;
+  double acc = 0;
+  for (int b = 0; b < blocks; ++b) acc += p[2 * b];
+  out[2 * T.spec[blockIdx.x].out_slot + threadIdx.x] = acc;
+}
+
+size_t tile_overlaps_partials_doubles(int n, int K) { return (size_t(1) << (n > K ? n - K : 0)) * 2 * kMaxOverlaps; }
+
+template <typename Real>
+cudaError_t launch_tile_overlaps(const void* lam, const void* psi, int n, const tile_overlap_set& set, double* partials,
+                                 double* out, cudaStream_t stream)
+{
+  if (set.count < 1 || set.count > kMaxOverlaps || n < set.K) return cudaErrorInvalidValue;
+  const size_t smem = 2 * sizeof(typename ctype<Real>::c) << set.K;
+  static std::atomic<bool> configured[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!configured[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(tile_overlaps_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (16 << 12));
+    if (e != cudaSuccess) return e;
+    configured[dev].store(true, std::memory_order_release);
+  }
+  const unsigned tiles = unsigned(1ull << (n - set.K));
+  tile_overlaps_kernel<Real><<<tiles, kRedThreads, smem, stream>>>(static_cast<const typename ctype<Real>::c*>(lam),
+                                                                  static_cast<const typename ctype<Real>::c*>(psi), set,
+                                                                  partials);
+  finish_tile_overlaps_kernel<<<set.count, 32, 0, stream>>>(partials, int(tiles), set, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_tile_overlaps<double>(const void*, const void*, int, const tile_overlap_set&, double*, double*, cudaStream_t);
+template cudaError_t launch_tile_overlaps<float>(const void*, const void*, int, const tile_overlap_set&, double*, double*, cudaStream_t);
+
+template cudaError_t launch_overlaps<double>(const void*, const void*, int, const overlap_set&, double*, double*, cudaStream_t);
+template cudaError_t launch_overlaps<float>(const void*, const void*, int, const overlap_set&, double*, double*, cudaStream_t);
 
 template cudaError_t launch_pauli_apply<double>(const void*, void*, int, const pauli_sum&, cudaStream_t);
 template cudaError_t launch_pauli_apply<float>(const void*, void*, int, const pauli_sum&, cudaStream_t);

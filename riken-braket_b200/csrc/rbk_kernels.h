@@ -61,6 +61,27 @@ template <typename Real> cudaError_t launch_pauli_apply(const void* src, void* d
 // out (device, 2 doubles) = <lam| P |psi> with P = w (-1)^popcount(i & sign) X^flip
 template <typename Real> cudaError_t launch_overlap(const void* lam, const void* psi, int n, uint64_t flip, uint64_t sign,
                                                     double wr, double wi, double* partials, double* out, cudaStream_t stream);
+// Up to kMaxOverlaps overlaps <lam| P_y |psi> in one launch; out[2y], out[2y+1] = (re, im) of overlap y.
+constexpr int kMaxOverlaps = 64;
+struct overlap_spec { uint64_t flip, sign; double wr, wi; };
+struct overlap_set { int count; int pad; overlap_spec spec[kMaxOverlaps]; };
+size_t overlaps_partials_doubles();
+template <typename Real> cudaError_t launch_overlaps(const void* lam, const void* psi, int n, const overlap_set& set,
+                                                     double* partials, double* out, cudaStream_t stream);
+// The same for overlaps whose flip bits are all tile bits of one tile layout:
+// each state is read once per launch.  flip_local / sign_local are tile-index
+// masks; sign bits outside the tile go in sign (physical); the result of spec y
+// goes to out[2 out_slot], out[2 out_slot + 1].  K <= 12.
+struct tile_overlap_spec { uint32_t flip_local, sign_local; uint64_t sign; double wr, wi; int32_t out_slot, pad; };
+struct tile_overlap_set {
+  int count, K;
+  uint8_t tile_phys[16];
+  uint8_t num_runs, run_src[16], run_len[16], run_dst[16];
+  tile_overlap_spec spec[kMaxOverlaps];
+};
+size_t tile_overlaps_partials_doubles(int n, int K);
+template <typename Real> cudaError_t launch_tile_overlaps(const void* lam, const void* psi, int n, const tile_overlap_set& set,
+                                                          double* partials, double* out, cudaStream_t stream);
 
 // Sampling: prefix = inclusive scan of |a_i|^2 (scratch: scan_scratch_doubles(count)
 // doubles); events[k] = upper_bound(prefix, r[k]).

@@ -16,6 +16,8 @@
 // phase_shift.hpp:1235-1253, pauli_x.hpp:120-165, ...) and bra's fused replay
 // of a BEGIN/END FUSION block on every 2^k chunk (bra/src/nompi_state.cpp:1285-1357).
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <cstdint>
 
 #include "rbk_device.cuh"
@@ -319,15 +321,15 @@ cudaError_t launch_shape(void* state, int n, const dev_pass& pass, cudaStream_t 
 {
   using SH = tile_shape<Real, SHAPE>;
   const size_t smem = sizeof(typename ctype<Real>::c) << SH::K;
-  static bool configured[64] = {};
+  static std::atomic<bool> configured[64] = {};  // per device; states on several host threads may race here
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (!configured[dev]) {
+  if (!configured[dev].load(std::memory_order_acquire)) {
     e = cudaFuncSetAttribute(tile_pass_kernel<Real, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    configured[dev] = true;
+    configured[dev].store(true, std::memory_order_release);
   }
   if (n < SH::K) return cudaErrorInvalidValue;
   const uint64_t blocks = 1ull << (n - SH::K);
