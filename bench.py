@@ -26,6 +26,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -345,12 +347,14 @@ def run_adjoint(args):
     terms = C.ansatz_hamiltonian(n)
     _, theta = C.ansatz(n, layers, seed=SEED)
     spec, nparams = pkg.adjoint.ansatz_spec(n, layers)
+    ctx = pkg.adjoint.AdjointContext(n)  # an optimiser loop keeps its two state vectors
     for _ in range(args.warmup):
-        pkg.adjoint.adjoint_gradient(n, spec, theta, terms)
+        ctx.gradient(spec, theta, terms)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        e, g = pkg.adjoint.adjoint_gradient(n, spec, theta, terms)
+        e, g = ctx.gradient(spec, theta, terms)
     t_adj = (time.perf_counter() - t0) / args.steps
+    ctx.close()
 
     # Per-parameter plain GPU evaluation: E(theta +- pi/2 e_k) through the fused engine.
     s = pkg.State(n, pkg.C128)
@@ -393,7 +397,76 @@ def run_adjoint(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "energy + adjoint gradient, 20-qubit hardware-efficient ansatz, 16 layers, 640 parameters",
                    "per_parameter_gpu_ms": t_shift * 1e3, "speedup_vs_per_parameter_gpu": t_shift / t_adj,
-                   "max_abs_diff_vs_parameter_shift": err, "energy": e, "timing": "host wall clock per call (includes state set-up)"},
+                   "max_abs_diff_vs_parameter_shift": err, "energy": e,
+                   "timing": "host wall clock per gradient on a reused context (rbk_adjoint_run): parameters in, energy and gradient out"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args):
+    """Config 5: energies + adjoint gradients of a batch of independent ansatz
+    instances (n log-uniform in [10, 24], depth U{4..16}, per-instance seeds
+    1 + index) in complex<double> and complex<float>; the complex<float> results
+    are compared instance by instance with the complex<double> ones."""
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    A, C = pkg.adjoint, pkg.circuits
+    draws = C.batch_instances(args.instances)
+    inst, thetas = [], []
+    for n, layers, th in draws:
+        spec, k = A.ansatz_spec(n, layers)
+        inst.append((n, spec, k, C.ansatz_hamiltonian(n)))
+        thetas.append(th)
+    results, stats, times = {}, {}, {}
+    for prec, name in ((pkg.C128, "c128"), (pkg.C64, "c64")):
+        b = A.Batch(inst, precision=prec)
+        for _ in range(args.warmup):
+            b.run(thetas)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e, g = b.run(thetas)
+        times[name] = (time.perf_counter() - t0) / args.steps
+        results[name] = (e, g)
+        stats[name] = b.stats()
+        b.close()
+    e64, g64 = results["c128"]
+    e32, g32 = results["c64"]
+    e_err = float(np.max(np.abs(e32 - e64)))
+    g_err = float(max(np.abs(a - b).max() for a, b in zip(g32, g64)))
+    ns = np.array([d[0] for d in draws])
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        threads = os.cpu_count() or 1
+        # parameter-shift gradient on the reference's CPU code for a sample: 2 energies per parameter
+        secs, done = 0.0, 0
+        for i in range(0, len(draws), max(1, len(draws) // 8)):
+            n, layers, th = draws[i]
+            ops, _ = C.ansatz(n, layers, thetas=th)
+            r = oracle.KetRef(n, threads=threads, fast=True)
+            t = r.apply_timed(ops)
+            t1 = time.perf_counter()
+            r.expectation(C.ansatz_hamiltonian(n))
+            t += time.perf_counter() - t1
+            secs += t * 2 * len(th)
+            done += 1
+        cpu = {"value": done / secs, "unit": "instances/s", "cores": threads, "kind": "reference",
+               "sample": f"{done} instances spread over the batch, each one energy evaluation with the reference ket "
+                         f"code (release build) times 2 x parameters (parameter shift)"}
+    line = {
+        "metric": "batched energy + adjoint gradient, instances/s", "value": len(inst) / times["c128"],
+        "unit": "instances/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": times["c128"] * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(inst)} ansatz instances, n log-uniform in [10, 24] (round), depth U{{4..16}}, "
+                               "H = sum Z_i Z_i+1 + 0.5 sum X_i",
+                   "qubit_histogram": {str(k): int(v) for k, v in zip(*np.unique(ns, return_counts=True))},
+                   "c128": {"seconds": times["c128"], **stats["c128"]},
+                   "c64": {"seconds": times["c64"], "instances_per_s": len(inst) / times["c64"], **stats["c64"]},
+                   "c64_vs_c128_max_abs_energy_diff": e_err, "c64_vs_c128_max_abs_gradient_diff": g_err,
+                   "timing": "host wall clock per batch run (parameters in, energies and gradients out)"},
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -412,12 +485,16 @@ def main():
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--shape", type=int, default=None, help="tile shape (rbk_state_set_tile_shape)")
     ap.add_argument("--budget", type=int, default=None, help="dense gates per pass (rbk_state_set_pass_budget)")
-    ap.add_argument("--workload", default="brick", choices=["brick", "adjoint"],
-                    help="brick: the 30-qubit circuit (default); adjoint: energy + gradient of the 20-qubit ansatz")
+    ap.add_argument("--workload", default="brick", choices=["brick", "adjoint", "batch"],
+                    help="brick: the 30-qubit circuit (default); adjoint: energy + gradient of the 20-qubit ansatz; "
+                         "batch: energies + gradients of a batch of ansatz instances")
+    ap.add_argument("--instances", type=int, default=4096, help="batch workload: number of instances")
     args = ap.parse_args()
     globals()["N_QUBITS"], globals()["DEPTH"] = args.qubits, args.depth
     if args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "batch":
+        run_batch(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -292,6 +292,15 @@ int rbk_batch_set_workers(rbk_batch* batch, int workers);
 int rbk_batch_get_stats(const rbk_batch* batch, rbk_batch_stats* out);
 int rbk_batch_destroy(rbk_batch* batch);
 
+/* The same sweep on a context that keeps its two state vectors and buffers
+ * between calls (optimiser loops): create once per qubit count and precision,
+ * then rbk_adjoint_run with the arguments of rbk_adjoint_gradient. */
+typedef struct rbk_adjoint_ctx rbk_adjoint_ctx;
+int rbk_adjoint_create(int num_qubits, int precision, int device, rbk_adjoint_ctx** out);
+int rbk_adjoint_run(rbk_adjoint_ctx* ctx, const rbk_circuit_gate* gates, int num_gates, const double* theta,
+                    int num_params, int num_terms, const char* strings, const double* coeffs, double* energy, double* grad);
+int rbk_adjoint_destroy(rbk_adjoint_ctx* ctx);
+
 /* Pauli-string expectation value of a caller-owned device state, with no
  * device memory allocated.  No counterpart in the reference: it exists for
  * callers that cannot allocate when they need the value -- code in a CUDA

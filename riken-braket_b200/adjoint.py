@@ -158,6 +158,47 @@ class Batch:
             pass
 
 
+class AdjointContext:
+    """rbk_adjoint_create/run/destroy: repeated gradients of n-qubit circuits
+    without re-allocating the two state vectors."""
+
+    def __init__(self, n, precision=rbk.C128, device=0):
+        L = rbk.lib()
+        L.rbk_adjoint_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.rbk_adjoint_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.rbk_adjoint_destroy.argtypes = [ctypes.c_void_p]
+        h = ctypes.c_void_p()
+        rc = L.rbk_adjoint_create(n, precision, device, ctypes.byref(h))
+        if rc != 0:
+            raise rbk.RbkError(rc, L.rbk_last_error().decode())
+        self.h, self.n = h, n
+
+    def gradient(self, spec, theta, terms):
+        gates, count = gate_array(spec)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        strings = b"".join(s.encode() for s, _ in terms)
+        coeffs = np.array([[complex(c).real, complex(c).imag] for _, c in terms], dtype=np.float64).ravel()
+        energy = ctypes.c_double()
+        grad = np.zeros(theta.size, dtype=np.float64)
+        rc = rbk.lib().rbk_adjoint_run(self.h, ctypes.cast(gates, ctypes.c_void_p), count, theta.ctypes.data, theta.size,
+                                       len(terms), strings, coeffs.ctypes.data, ctypes.addressof(energy), grad.ctypes.data)
+        if rc != 0:
+            raise rbk.RbkError(rc, rbk.lib().rbk_last_error().decode())
+        return energy.value, grad
+
+    def close(self):
+        if getattr(self, "h", None):
+            rbk.lib().rbk_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def make_autograd_function():
     """torch.autograd.Function over adjoint_gradient (gradient-check harness only)."""
     import torch

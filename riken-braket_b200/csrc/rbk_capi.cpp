@@ -1318,6 +1318,29 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
   });
 }
 
+extern "C" int rbk_adjoint_create(int num_qubits, int precision, int device, rbk_adjoint_ctx** out)
+{
+  if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+  rbk::adjoint_workspace* w = nullptr;
+  const int rc = rbk::adjoint_workspace_create(num_qubits, precision, device, &w);
+  *out = reinterpret_cast<rbk_adjoint_ctx*>(w);
+  return rc;
+}
+
+extern "C" int rbk_adjoint_run(rbk_adjoint_ctx* ctx, const rbk_circuit_gate* gates, int num_gates, const double* theta,
+                               int num_params, int num_terms, const char* strings, const double* coeffs, double* energy,
+                               double* grad)
+{
+  return rbk::adjoint_run(reinterpret_cast<rbk::adjoint_workspace*>(ctx), gates, num_gates, theta, num_params, num_terms,
+                          strings, coeffs, energy, grad);
+}
+
+extern "C" int rbk_adjoint_destroy(rbk_adjoint_ctx* ctx)
+{
+  rbk::adjoint_workspace_destroy(reinterpret_cast<rbk::adjoint_workspace*>(ctx));
+  return RBK_OK;
+}
+
 extern "C" int rbk_adjoint_gradient(int num_qubits, int precision, int device, const rbk_circuit_gate* gates,
                                     int num_gates, const double* theta, int num_params, int num_terms,
                                     const char* strings, const double* coeffs, double* energy, double* grad)

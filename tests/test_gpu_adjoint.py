@@ -117,3 +117,21 @@ def test_autograd_harness_gradcheck(pkg):
     fn = pkg.adjoint.make_autograd_function()
     theta = torch.tensor(np.random.default_rng(0).uniform(-3, 3, nparams), dtype=torch.float64, requires_grad=True)
     assert torch.autograd.gradcheck(lambda t: fn.apply(t, n, spec, terms), (theta,), eps=1e-6, atol=1e-6)
+
+
+def test_adjoint_context_reuse_matches_one_shot(pkg):
+    """rbk_adjoint_create/run/destroy: repeated gradients on kept state vectors
+    equal the one-shot rbk_adjoint_gradient, for several parameter vectors."""
+    A, C = pkg.adjoint, pkg.circuits
+    n, layers = 12, 3
+    spec, k = A.ansatz_spec(n, layers)
+    terms = C.ansatz_hamiltonian(n)
+    ctx = A.AdjointContext(n)
+    try:
+        for seed in (1, 2, 3):
+            th = np.random.default_rng(seed).uniform(-np.pi, np.pi, size=k)
+            e1, g1 = ctx.gradient(spec, th, terms)
+            e2, g2 = A.adjoint_gradient(n, spec, th, terms)
+            assert e1 == e2 and np.array_equal(g1, g2)
+    finally:
+        ctx.close()
