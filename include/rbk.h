@@ -187,6 +187,21 @@ int rbk_set(rbk_state* s, uint32_t qubit);
  * register on the top nx qubits; replaces the state.  0 < divisor <= 2^32, base < 2^32. */
 int rbk_shor_box(rbk_state* s, uint32_t num_exponent_qubits, uint64_t divisor, uint64_t base);
 
+/* ---- dense unitaries --------------------------------------------------------
+ * u is 2^k x 2^k complex (re, im), row-major: u[r][c] = <r|U|c>, where bit i of
+ * the basis index is qubits[i].  The qubits are first moved onto the low
+ * physical bits by relabelling passes.  complex<float> states with k = 5 or 6
+ * (and n >= k + 7) run on the tensor cores as 3xTF32 split-precision GEMMs with
+ * FP32 accumulation (tcgen05, accumulator in TMEM); other cases on CUDA cores.
+ * No counterpart in ket beyond the fused blocks below; k <= 10. */
+int rbk_apply_unitary(rbk_state* s, const double* u, const uint32_t* qubits, int k);
+/* 0 (default): BEGIN/END FUSION blocks run gate by gate inside the fused passes.
+ * 1: on complex<float> states, a block that touches 5 or 6 qubits becomes its
+ *    2^k x 2^k unitary (built on the host in FP64) applied by rbk_apply_unitary,
+ *    i.e. on the tensor cores -- the bra-fused unitary of
+ *    bra/src/nompi_state.cpp:1285-1357 as one GEMM; other blocks stay gate by gate. */
+int rbk_state_set_fusion_mode(rbk_state* s, int mode);
+
 /* ---- observables ---------------------------------------------------------- */
 /* sum |a_i|^2 */
 int rbk_norm2(rbk_state* s, double* out);

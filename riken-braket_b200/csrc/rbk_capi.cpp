@@ -38,6 +38,8 @@ struct rbk_state {
   std::vector<hgate> queue;
   bool deferred = true;
   bool in_fusion = false;
+  int fusion_mode = 0;       // 1: c64 fusion blocks of 5-6 qubits become dense unitaries on tensor cores
+  size_t fusion_begin = 0;   // queue index of the current BEGIN FUSION
   int dense_budget = 0;
   int shape = 2;
   rbk_stats stats{};
@@ -606,11 +608,17 @@ int rbk_state_device_pointer(rbk_state* s, void** out)
   });
 }
 
+namespace {
+constexpr int RBK_NOT_FUSED = -1;
+int fuse_block_to_unitary(rbk_state* s);
+}  // namespace
+
 int rbk_begin_fusion(rbk_state* s)
 {
   if (int rc = check_state(s)) return rc;
   if (s->in_fusion) return fail(RBK_ERR_STATE, "BEGIN FUSION inside a fusion block");
   s->in_fusion = true;
+  s->fusion_begin = s->queue.size();
   return RBK_OK;
 }
 
@@ -619,6 +627,10 @@ int rbk_end_fusion(rbk_state* s)
   if (int rc = check_state(s)) return rc;
   if (!s->in_fusion) return fail(RBK_ERR_STATE, "END FUSION without BEGIN FUSION");
   s->in_fusion = false;
+  if (s->fusion_mode == 1 && s->precision == RBK_C64) {
+    const int rc = guarded([&] { return fuse_block_to_unitary(s); });
+    if (rc != RBK_NOT_FUSED) return rc;
+  }
   if (!s->deferred) return guarded([&] { return flush(s); });
   return RBK_OK;
 }
@@ -1743,4 +1755,214 @@ extern "C" int rbk_shor_box(rbk_state* s, uint32_t num_exponent_qubits, uint64_t
     RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
     return RBK_OK;
   });
+}
+
+// ---- dense k-qubit unitaries and the tensor-core fusion mode ---------------
+
+namespace {
+
+// Moves logical qubits q[0..k-1] onto physical bits 0..k-1 (in that order) with
+// the canonicalising passes: the planner moves logical j to physical j, so the
+// map is first renamed so that q[i] is "logical i", then restored.
+int move_to_low(rbk_state* s, const uint32_t* q, int k)
+{
+  if (int rc = flush(s)) return rc;
+  const int n = s->n;
+  std::vector<int> sigma(n, -1);  // real logical -> virtual logical
+  std::vector<char> used(n, 0);
+  for (int i = 0; i < k; ++i) { sigma[q[i]] = i; used[q[i]] = 1; }
+  int next = k;
+  for (int l = 0; l < n; ++l)
+    if (!used[l]) sigma[l] = next++;
+  bool in_place = true;
+  for (int i = 0; i < k; ++i) in_place = in_place && s->perm[q[i]] == i;
+  if (in_place) return RBK_OK;
+  std::vector<int> perm_v(n), inv_v(n);
+  for (int l = 0; l < n; ++l) perm_v[sigma[l]] = s->perm[l];
+  for (int v = 0; v < n; ++v) inv_v[perm_v[v]] = v;
+  std::vector<int> unsigma(n);
+  for (int l = 0; l < n; ++l) unsigma[sigma[l]] = l;
+  s->perm = perm_v;
+  s->inv = inv_v;
+  const int rc = canonicalize(s);
+  // canonicalize leaves virtual v on physical v, i.e. real l on physical sigma[l]
+  for (int l = 0; l < n; ++l) s->perm[l] = sigma[l];
+  for (int v = 0; v < n; ++v) s->inv[v] = unsigma[v];
+  return rc;
+}
+
+// W_hi, W_lo of the 3xTF32 kernel (see rbk_tc.cu) in its operand layout:
+// operand row = output column j of W, 4-float chunks along K.
+float tf32_round_host(float x)
+{
+  uint32_t b;
+  std::memcpy(&b, &x, 4);
+  if ((b & 0x7F800000u) != 0x7F800000u) b = (b + 0x1000u) & ~0x1FFFu;  // round to nearest, ties away (cvt.rna)
+  float r;
+  std::memcpy(&r, &b, 4);
+  return r;
+}
+
+std::vector<float> build_w_split(const std::vector<cplx>& U, int k)
+{
+  const int dim = 1 << k, K = 2 * dim;
+  std::vector<float> W(static_cast<size_t>(K) * K);  // W[kk * K + j]
+  for (int a = 0; a < dim; ++a)
+    for (int b = 0; b < dim; ++b) {
+      const cplx u = U[static_cast<size_t>(b) * dim + a];
+      W[(2 * a) * K + 2 * b] = static_cast<float>(u.real());
+      W[(2 * a + 1) * K + 2 * b] = static_cast<float>(-u.imag());
+      W[(2 * a) * K + 2 * b + 1] = static_cast<float>(u.imag());
+      W[(2 * a + 1) * K + 2 * b + 1] = static_cast<float>(u.real());
+    }
+  std::vector<float> out(rbk::tc_w_split_floats(k), 0.0f);
+  const size_t half = out.size() / 2;
+  for (int j = 0; j < K; ++j)        // operand row (N index)
+    for (int kk = 0; kk < K; ++kk) {  // K index
+      const size_t off = static_cast<size_t>(j >> 3) * (K / 4) * 32 + static_cast<size_t>(kk >> 2) * 32 + (j & 7) * 4 + (kk & 3);
+      const float w = W[static_cast<size_t>(kk) * K + j];
+      const float hi = tf32_round_host(w);
+      out[off] = hi;
+      out[half + off] = tf32_round_host(w - hi);
+    }
+  return out;
+}
+
+int apply_unitary(rbk_state* s, const std::vector<cplx>& U, const uint32_t* q, int k)
+{
+  device_guard g(s->device);
+  if (int rc = move_to_low(s, q, k)) return rc;
+  if (int rc = mark_launch_start(s)) return rc;
+  ++s->stats.gates_issued;
+  const bool tensor = s->precision == RBK_C64 && (k == 5 || k == 6) && s->n >= k + 7;
+  if (tensor) {
+    const std::vector<float> w = build_w_split(U, k);
+    device_buffer dw;
+    RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&dw.p), sizeof(float) * w.size()));
+    RBK_CUDA(cudaMemcpyAsync(dw.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice, s->stream));
+    int* flag = reinterpret_cast<int*>(s->d_out);
+    RBK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    const uint64_t tiles = (1ull << (s->n - k)) / 128;
+    const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(sms)));
+    const cudaError_t e = rbk::launch_unitary_tf32x3(static_cast<float*>(s->amps), s->n, k,
+                                                    reinterpret_cast<const float*>(dw.p), flag, grid, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tensor-core unitary");
+    ++s->stats.kernel_launches;
+    ++s->stats.passes;
+    int h = 0;
+    RBK_CUDA(cudaMemcpyAsync(s->h_out, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    if (int rc = bounded_sync(s)) return rc;
+    std::memcpy(&h, s->h_out, sizeof(int));
+    if (h) return fail(RBK_ERR_TIMEOUT, "tensor-core unitary: a wait for the MMAs ran out");
+  } else {
+    device_buffer du;
+    const size_t count = 2 * U.size();
+    RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&du.p), sizeof(double) * count));
+    RBK_CUDA(cudaMemcpyAsync(du.p, reinterpret_cast<const double*>(U.data()), sizeof(double) * count,
+                             cudaMemcpyHostToDevice, s->stream));
+    const cudaError_t e = s->precision == RBK_C128 ? rbk::launch_dense_rows<double>(s->amps, s->n, k, du.p, s->stream)
+                                                  : rbk::launch_dense_rows<float>(s->amps, s->n, k, du.p, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "dense unitary");
+    ++s->stats.kernel_launches;
+    ++s->stats.passes;
+    if (int rc = bounded_sync(s)) return rc;  // the matrix buffer is freed on return
+  }
+  RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
+  return RBK_OK;
+}
+
+// One queued gate on a vector over the local basis of the block's qubits.
+void host_apply(std::vector<cplx>& v, const hgate& g, const std::vector<int>& local)
+{
+  const int dim = static_cast<int>(v.size());
+  uint32_t cm = 0;
+  for (int l = 0; l < 64; ++l)
+    if (g.cmask & (1ull << l)) cm |= 1u << local[l];
+  auto m = [&](int i) { return cplx{g.m[2 * i], g.m[2 * i + 1]}; };
+  if (g.kind == rbk::OPK_NEG) {
+    for (int i = 0; i < dim; ++i)
+      if ((static_cast<uint32_t>(i) & cm) == cm) v[i] = -v[i];
+    return;
+  }
+  if (g.kind == rbk::HK_SWAP) {
+    const int a = local[g.target], b = local[g.target2];
+    for (int i = 0; i < dim; ++i)
+      if (((i >> a) & 1) && !((i >> b) & 1)) std::swap(v[i], v[i ^ (1 << a) ^ (1 << b)]);
+    return;
+  }
+  const int t = local[g.target];
+  for (int i = 0; i < dim; ++i) {
+    if ((static_cast<uint32_t>(i) & cm) != cm) continue;
+    if (g.kind == rbk::OPK_DIAG) {
+      if (g.diag_one && !((i >> t) & 1)) continue;
+      v[i] *= ((i >> t) & 1) ? m(1) : m(0);
+      continue;
+    }
+    if ((i >> t) & 1) continue;
+    const int j = i | (1 << t);
+    const cplx a0 = v[i], a1 = v[j];
+    if (g.kind == rbk::OPK_X) { v[i] = a1; v[j] = a0; }
+    else if (g.kind == rbk::OPK_Y) { v[i] = cplx{a1.imag(), -a1.real()}; v[j] = cplx{-a0.imag(), a0.real()}; }
+    else { v[i] = m(0) * a0 + m(1) * a1; v[j] = m(2) * a0 + m(3) * a1; }
+  }
+}
+
+// END FUSION in the tensor-core mode: the block's gates (queue[fusion_begin..])
+// become one dense unitary when they touch 5 or 6 qubits; otherwise the block
+// stays in the queue for the fused passes (RBK_NOT_FUSED).
+int fuse_block_to_unitary(rbk_state* s)
+{
+  const size_t b = s->fusion_begin, e = s->queue.size();
+  if (b >= e) return RBK_NOT_FUSED;
+  uint64_t touched = 0;
+  for (size_t i = b; i < e; ++i) {
+    const auto& g = s->queue[i];
+    touched |= g.cmask;
+    if (g.target >= 0) touched |= 1ull << g.target;
+    if (g.kind == rbk::HK_SWAP) touched |= 1ull << g.target2;
+  }
+  const int k = __builtin_popcountll(touched);
+  if (k < 5 || k > 6 || s->n < k + 7) return RBK_NOT_FUSED;
+  std::vector<uint32_t> q;
+  std::vector<int> local(64, -1);
+  for (int l = 0; l < s->n; ++l)
+    if (touched & (1ull << l)) { local[l] = static_cast<int>(q.size()); q.push_back(static_cast<uint32_t>(l)); }
+  const int dim = 1 << k;
+  std::vector<cplx> U(static_cast<size_t>(dim) * dim);
+  for (int c = 0; c < dim; ++c) {
+    std::vector<cplx> v(dim, cplx{0.0, 0.0});
+    v[c] = 1.0;
+    for (size_t i = b; i < e; ++i) host_apply(v, s->queue[i], local);
+    for (int r = 0; r < dim; ++r) U[static_cast<size_t>(r) * dim + c] = v[r];
+  }
+  s->queue.resize(b);
+  return apply_unitary(s, U, q.data(), k);
+}
+
+}  // namespace
+
+extern "C" int rbk_apply_unitary(rbk_state* s, const double* u, const uint32_t* qubits, int k)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!u) return fail(RBK_ERR_INVALID, "null matrix");
+    if (k < 1 || k > 10 || k > s->n) return fail(RBK_ERR_INVALID, "a dense unitary acts on 1 to 10 qubits");
+    uint64_t mask = 0;
+    if (int rc = check_qubits(s, qubits, k, &mask)) return rc;
+    if (s->in_fusion) return fail(RBK_ERR_STATE, "a dense unitary inside a fusion block");
+    const int dim = 1 << k;
+    std::vector<cplx> U(static_cast<size_t>(dim) * dim);
+    for (size_t i = 0; i < U.size(); ++i) U[i] = cplx{u[2 * i], u[2 * i + 1]};
+    return apply_unitary(s, U, qubits, k);
+  });
+}
+
+extern "C" int rbk_state_set_fusion_mode(rbk_state* s, int mode)
+{
+  if (int rc = check_state(s)) return rc;
+  if (mode < 0 || mode > 1) return fail(RBK_ERR_INVALID, "fusion mode must be 0 or 1");
+  s->fusion_mode = mode;
+  return RBK_OK;
 }

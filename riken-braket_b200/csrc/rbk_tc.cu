@@ -1,0 +1,315 @@
+// rbk_tc.cu -- dense k-qubit unitaries (k = 5, 6) on a complex<float> state as
+// tensor-core GEMMs with 3xTF32 split products (tcgen05, accumulator in TMEM).
+//
+// With the k target qubits on the low k physical bits, the state is a matrix
+// of R = 2^(n-k) rows of 2^k complex amplitudes, stored as 2K = 2^(k+1)
+// interleaved floats.  Applying U is out_row = in_row . W with the real
+// 2K x 2K matrix
+//   W[2a][2b] = Re U[b][a],  W[2a+1][2b] = -Im U[b][a],
+//   W[2a][2b+1] = Im U[b][a], W[2a+1][2b+1] = Re U[b][a],
+// a plain real GEMM of M = R rows, N = K = 2^(k+1).  Each product is split as
+// x = hi + lo with hi = tf32(x) and lo = tf32(x - hi), and
+//   A.W ~ A_hi.W_hi + A_hi.W_lo + A_lo.W_hi   (FP32 accumulation in TMEM),
+// which carries about 21 mantissa bits per product -- the FP32 result, on the
+// tensor cores.  This is the bra-fused 2^k x 2^k unitary of a fusion block
+// (bra/src/nompi_state.cpp:1285-1357 replays the gates instead).
+//
+// One CTA per SM (persistent), 128 threads.  W_hi and W_lo stay in shared
+// memory for the whole launch in the canonical K-major layout without swizzle
+// (8-row x 16-byte core matrices).  Each 128-row tile is staged in two K
+// halves: threads load, split and store A_hi / A_lo, one thread issues the 3 x
+// K/16 tcgen05.mma of the half, and tcgen05.commit signals an mbarrier.  The
+// epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31 = rows) and writes the rows back in place.  Every mbarrier wait is
+// bounded: on expiry the kernel raises an error flag, waits (bounded) for its
+// own MMAs, frees its TMEM and returns.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rbk_device.cuh"
+#include "rbk_kernels.h"
+
+namespace rbk {
+namespace {
+
+constexpr int kTcThreads = 128;
+constexpr int kTcM = 128;
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor, K-major, no swizzle (SWIZZLE_NONE = 0 in bits 61-63),
+// version 1 in bits 46-47.  lbo: byte step between the two 16-byte K chunks of one
+// MMA; sbo: byte step between 8-row groups.
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+  return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::tf32: D in F32, A and B TF32, both K-major.
+__host__ __device__ constexpr uint32_t tf32_idesc(int M, int N)
+{
+  return (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+// Round to TF32 (10 mantissa bits), nearest with ties away from zero, with the
+// 13 dropped bits cleared so that x - tf32(x) is the exact remainder.
+__device__ __forceinline__ float tf32_rna(float x)
+{
+  uint32_t b = __float_as_uint(x);
+  if ((b & 0x7F800000u) != 0x7F800000u) b = (b + 0x1000u) & 0xFFFFE000u;
+  return __uint_as_float(b);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+  asm volatile(
+    "{\n\t"
+    ".reg .pred p;\n\t"
+    "setp.ne.b32 p, %4, 0;\n\t"
+    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+    "}\n" ::"r"(tmem_d),
+    "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+    "{\n\t"
+    ".reg .pred P1;\n\t"
+    "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+    "selp.b32 %0, 1, 0, P1;\n\t"
+    "}\n"
+    : "=r"(ok)
+    : "r"(addr), "r"(parity)
+    : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Gives up after kWaitLimit polls or 2 s of wall time, whichever comes first.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity)
+{
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    if (mbar_try_wait(addr, parity)) return true;
+    if ((it & 255u) == 255u && global_ns() - t0 > 2000000000ull) return false;
+  }
+  return false;
+}
+
+// Byte offset of element (row, kk) in a K-major operand buffer with kc K-elements per row.
+__device__ __forceinline__ uint32_t kmajor_offset(uint32_t row, uint32_t kk, uint32_t kc)
+{
+  return (row >> 3) * (kc / 4) * 128u + (kk >> 2) * 128u + (row & 7u) * 16u + (kk & 3u) * 4u;
+}
+
+template <int KB>  // KB = k + 1: K = N = 2^KB floats per row
+__global__ void __launch_bounds__(kTcThreads, 1)
+unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __restrict__ w_split, int* error_flag)
+{
+  constexpr uint32_t K = 1u << KB, N = K, KH = K / 2;
+  constexpr uint32_t B_BYTES = N * K * 4, A_BYTES = kTcM * KH * 4;
+  constexpr uint32_t SBO_A = (KH / 4) * 128u, SBO_B = (K / 4) * 128u;
+  constexpr uint32_t NCOLS = N;  // FP32 accumulator: 128 lanes x N columns
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* b_hi = smem;
+  unsigned char* b_lo = smem + B_BYTES;
+  unsigned char* a_hi = smem + 2 * B_BYTES;
+  unsigned char* a_lo = a_hi + A_BYTES;
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+
+  if (warp == 0)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                 "r"(NCOLS));
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1u));
+    abort_flag = 0;
+  }
+  // W_hi, W_lo: precomputed in the operand layout, copied as-is.
+  {
+    float4* dst = reinterpret_cast<float4*>(smem);
+    for (uint32_t i = tid; i < 2 * B_BYTES / 16; i += kTcThreads) dst[i] = w_split[i];
+  }
+  async_proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  if (warp == 0) asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  const uint32_t idesc = tf32_idesc(kTcM, N);
+  const uint32_t mbar_addr = smem_addr(&mbar);
+  uint32_t phase = 0;
+  const uint64_t tiles = rows / kTcM;
+
+  for (uint64_t tile = blockIdx.x; tile < tiles && !abort_flag; tile += gridDim.x) {
+    float* tile_rows = state + tile * kTcM * K;
+    for (uint32_t h = 0; h < 2; ++h) {
+      // Load the K half h of the 128 rows, split into hi / lo, store in the operand layout.
+      // A warp moves 8 rows x 4 float4: 512 contiguous shared-memory bytes.
+      constexpr uint32_t CG = KH / 16;  // groups of 4 float4 per row half
+      for (uint32_t blk = warp; blk < (kTcM / 8) * CG; blk += kTcThreads / 32) {
+        const uint32_t rg = blk / CG, cg = blk % CG;
+        const uint32_t r = rg * 8 + (lane & 7u), c4 = cg * 4 + (lane >> 3);
+        const float4 v = *reinterpret_cast<const float4*>(tile_rows + size_t(r) * K + h * KH + c4 * 4);
+        float4 hi, lo;
+        hi.x = tf32_rna(v.x); lo.x = tf32_rna(v.x - hi.x);
+        hi.y = tf32_rna(v.y); lo.y = tf32_rna(v.y - hi.y);
+        hi.z = tf32_rna(v.z); lo.z = tf32_rna(v.z - hi.z);
+        hi.w = tf32_rna(v.w); lo.w = tf32_rna(v.w - hi.w);
+        const uint32_t off = kmajor_offset(r, c4 * 4, KH);
+        *reinterpret_cast<float4*>(a_hi + off) = hi;
+        *reinterpret_cast<float4*>(a_lo + off) = lo;
+      }
+      async_proxy_fence();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      if (tid == 0) {
+        const uint32_t ah = smem_addr(a_hi), al = smem_addr(a_lo), bh = smem_addr(b_hi), bl = smem_addr(b_lo);
+#pragma unroll
+        for (uint32_t s = 0; s < KH / 8; ++s) {
+          const uint32_t g = h * (KH / 8) + s;  // K step within the full K of W
+          const uint64_t da_hi = kmajor_desc(ah + s * 256u, 128u, SBO_A), da_lo = kmajor_desc(al + s * 256u, 128u, SBO_A);
+          const uint64_t db_hi = kmajor_desc(bh + g * 256u, 128u, SBO_B), db_lo = kmajor_desc(bl + g * 256u, 128u, SBO_B);
+          umma_tf32(tmem, da_hi, db_hi, idesc, (h | s) != 0 ? 1u : 0u);
+          umma_tf32(tmem, da_hi, db_lo, idesc, 1u);
+          umma_tf32(tmem, da_lo, db_hi, idesc, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_addr)
+                     : "memory");
+      }
+      // The half's MMAs must finish before A is overwritten or the accumulator read.
+      if (!mbar_wait_bounded(mbar_addr, phase)) {
+        if (tid == 0) { atomicExch(error_flag, 1); abort_flag = 1; }
+      }
+      phase ^= 1u;
+      tc_fence_after();
+      __syncthreads();
+      if (abort_flag) break;
+    }
+    if (abort_flag) break;
+    // Epilogue: warp w reads TMEM lanes 32w.. (rows), 32 columns at a time.
+    float* out_row = tile_rows + size_t(warp * 32 + lane) * K;
+#pragma unroll 1
+    for (uint32_t c = 0; c < N / 32; ++c) {
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((warp * 32u) << 16) + c * 32u;
+      asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float4* dst = reinterpret_cast<float4*>(out_row + c * 32);
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                             __uint_as_float(v[4 * q + 3]));
+    }
+    // The next tile's MMAs overwrite the accumulator: every warp must have read it.
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  // After a timed-out wait, let the MMAs of that half finish (bounded) before the accumulator is freed.
+  if (abort_flag) mbar_wait_bounded(mbar_addr, phase ^ 1u);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS));
+}
+
+// Dense k-qubit unitary on CUDA cores (any precision; the targets on the low k
+// physical bits): one CTA per row of 2^k amplitudes, thread b computes output b.
+template <typename Real>
+__global__ void dense_rows_kernel(typename ctype<Real>::c* __restrict__ state, uint64_t rows, int k,
+                                  const double* __restrict__ U)
+{
+  using C = typename ctype<Real>::c;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* in = reinterpret_cast<C*>(smem_raw);
+  const uint32_t dim = 1u << k;
+  for (uint64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    C* row = state + r * dim;
+    for (uint32_t i = threadIdx.x; i < dim; i += blockDim.x) in[i] = row[i];
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < dim; b += blockDim.x) {
+      double re = 0, im = 0;
+      for (uint32_t a = 0; a < dim; ++a) {
+        const double ur = U[2 * (size_t(b) * dim + a)], ui = U[2 * (size_t(b) * dim + a) + 1];
+        const double xr = double(in[a].x), xi = double(in[a].y);
+        re += ur * xr - ui * xi;
+        im += ur * xi + ui * xr;
+      }
+      row[b] = C{(Real)re, (Real)im};
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+size_t tc_w_split_floats(int k) { return size_t(2) << (2 * (k + 1)); }
+
+size_t tc_shared_bytes(int k)
+{
+  const size_t K = size_t(1) << (k + 1);
+  return 2 * K * K * 4 + 2 * size_t(kTcM) * (K / 2) * 4;
+}
+
+cudaError_t launch_unitary_tf32x3(float* state, int n, int k, const float* w_split, int* error_flag, int grid,
+                                  cudaStream_t stream)
+{
+  if ((k != 5 && k != 6) || n < k + 7) return cudaErrorInvalidValue;
+  const uint64_t rows = 1ull << (n - k);
+  const size_t smem = tc_shared_bytes(k);
+  cudaError_t e;
+  if (k == 6) {
+    e = cudaFuncSetAttribute(unitary_tf32x3_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    unitary_tf32x3_kernel<7><<<grid, kTcThreads, smem, stream>>>(state, rows, reinterpret_cast<const float4*>(w_split),
+                                                                  error_flag);
+  } else {
+    e = cudaFuncSetAttribute(unitary_tf32x3_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    unitary_tf32x3_kernel<6><<<grid, kTcThreads, smem, stream>>>(state, rows, reinterpret_cast<const float4*>(w_split),
+                                                                  error_flag);
+  }
+  return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_dense_rows(void* state, int n, int k, const double* U, cudaStream_t stream)
+{
+  const uint64_t rows = 1ull << (n - k);
+  const int threads = (1 << k) < 256 ? (1 << k) < 32 ? 32 : (1 << k) : 256;
+  const unsigned grid = unsigned(rows < 148 * 16 ? rows : 148 * 16);
+  dense_rows_kernel<Real><<<grid, threads, sizeof(typename ctype<Real>::c) << k, stream>>>(
+    static_cast<typename ctype<Real>::c*>(state), rows, k, U);
+  return cudaGetLastError();
+}
+template cudaError_t launch_dense_rows<double>(void*, int, int, const double*, cudaStream_t);
+template cudaError_t launch_dense_rows<float>(void*, int, int, const double*, cudaStream_t);
+
+}  // namespace rbk

@@ -95,6 +95,8 @@ _SIGNATURES = {
     "rbk_clear": ([_P, _U32], _I),
     "rbk_set": ([_P, _U32], _I),
     "rbk_shor_box": ([_P, _U32, _U64, _U64], _I),
+    "rbk_apply_unitary": ([_P, ctypes.POINTER(_D), _U32P, _I], _I),
+    "rbk_state_set_fusion_mode": ([_P, _I], _I),
     "rbk_state_seed": ([_P, _U64], _I),
     "rbk_generate_events": ([_P, _I, ctypes.c_int64, _P], _I),
     "rbk_measure": ([_P, ctypes.POINTER(_U64)], _I),
@@ -367,6 +369,17 @@ class State:
     def exponential_swap(self, phase, q1, q2, controls=()):
         c, nc = _qarr(controls)
         _check(lib().rbk_exponential_swap(self.h, phase, q1, q2, c, nc))
+
+    def apply_unitary(self, u, qubits):
+        """Dense 2^k x 2^k unitary u[r][c] = <r|U|c>, bit i of the index = qubits[i]."""
+        u = np.ascontiguousarray(u, dtype=np.complex128)
+        q, nq = _qarr(qubits)
+        assert u.shape == (1 << nq, 1 << nq)
+        _check(lib().rbk_apply_unitary(self.h, u.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), q, nq))
+
+    def set_fusion_mode(self, mode):
+        """1: complex<float> fusion blocks of 5-6 qubits run as tensor-core unitaries."""
+        _check(lib().rbk_state_set_fusion_mode(self.h, mode))
 
     def clear(self, q):
         _check(lib().rbk_clear(self.h, q))
