@@ -472,6 +472,74 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_qft(args):
+    """Config 3: H on qubit j then U m j (m-j+1) for every m > j (all n(n-1)/2
+    controlled phases), then 5 seeded brick layers, in fusion blocks of 6 qubits.
+    complex<float> at 32 qubits (gate-by-gate fused passes, and the tensor-core
+    mode that runs 5-6 qubit blocks as 3xTF32 GEMMs), complex<double> at 33
+    qubits (128 GiB), and the complex<float> accuracy against complex<double> at
+    30 qubits."""
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    C = pkg.circuits
+    out = {}
+
+    def timed(n, prec, mode, ops):
+        s = pkg.State(n, prec)
+        s.set_fusion_mode(mode)
+        for _ in range(args.warmup):
+            s.reset(0)
+            s.apply(ops)
+            s.synchronize()
+        times, st = [], None
+        for _ in range(args.steps):
+            s.reset(0)
+            s.synchronize()
+            s.reset_stats()
+            s.apply(ops)
+            s.synchronize()
+            times.append(s.device_ms())
+            st = s.stats()
+        return s, statistics.median(times), st
+
+    n = 30
+    ops = C.qft_brick(n, 5, seed=SEED, fuse_k=6)
+    s, ms, st = timed(n, pkg.C128, 0, ops)
+    ref = s.amplitudes()
+    s.close()
+    acc = {}
+    for mode, name in ((0, "fused passes"), (1, "tensor-core blocks")):
+        s, ms32, st32 = timed(n, pkg.C64, mode, ops)
+        got = s.amplitudes().astype(np.complex128)
+        s.close()
+        fid = abs(np.vdot(ref, got)) ** 2 / (np.vdot(got, got).real * np.vdot(ref, ref).real)
+        acc[name] = {"max_abs_error": float(np.abs(got - ref).max()), "one_minus_fidelity": float(1 - fid),
+                     "ms": ms32}
+    del ref, got
+    big = {}
+    ops32 = C.qft_brick(32, 5, seed=SEED, fuse_k=6)
+    for mode, name in ((0, "fused passes"), (1, "tensor-core blocks")):
+        s, ms32, st32 = timed(32, pkg.C64, mode, ops32)
+        s.close()
+        big[name] = {"ms": ms32, "passes": st32["passes"], "relabel_passes": st32["relabel_passes"]}
+    ops33 = C.qft_brick(33, 5, seed=SEED, fuse_k=6)
+    s, ms33, st33 = timed(33, pkg.C128, 0, ops33)
+    s.close()
+    bytes33 = 2 * (1 << 33) * 16
+    line = {
+        "metric": "circuit time, 33-qubit complex<double> QFT + 5 brick layers", "value": ms33, "unit": "ms",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms33, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "H j + U m j (m-j+1) for all m > j, then 5 seeded brick layers, fusion blocks of 6",
+                   "c128_33q": {"ms": ms33, "passes": st33["passes"],
+                                "gb_per_s_per_pass": st33["passes"] * bytes33 / ms33 / 1e6},
+                   "c64_32q": big, "c64_vs_c128_at_30q": acc,
+                   "timing": "CUDA events on the state's stream (rbk_state_device_ms), median of steps"},
+        "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,9 +553,10 @@ def main():
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--shape", type=int, default=None, help="tile shape (rbk_state_set_tile_shape)")
     ap.add_argument("--budget", type=int, default=None, help="dense gates per pass (rbk_state_set_pass_budget)")
-    ap.add_argument("--workload", default="brick", choices=["brick", "adjoint", "batch"],
+    ap.add_argument("--workload", default="brick", choices=["brick", "adjoint", "batch", "qft"],
                     help="brick: the 30-qubit circuit (default); adjoint: energy + gradient of the 20-qubit ansatz; "
-                         "batch: energies + gradients of a batch of ansatz instances")
+                         "batch: energies + gradients of a batch of ansatz instances; "
+                         "qft: the QFT + brick circuit at 32 (c64) and 33 (c128) qubits")
     ap.add_argument("--instances", type=int, default=4096, help="batch workload: number of instances")
     args = ap.parse_args()
     globals()["N_QUBITS"], globals()["DEPTH"] = args.qubits, args.depth
@@ -495,6 +564,8 @@ def main():
         run_adjoint(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "qft":
+        run_qft(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -75,15 +75,36 @@ def brick(n, depth, seed=1, fuse_k=0):
     return ops
 
 
-def qft_brick(n, brick_layers=5, seed=1):
+def qft_brick(n, brick_layers=5, seed=1, fuse_k=0):
     """For j = 0..n-1: H j, then U m j k with k = m - j + 1 for every m > j
-    (phase 2 pi / 2^k on |1_m 1_j>, all n(n-1)/2 pairs), then seeded brick layers."""
+    (phase 2 pi / 2^k on |1_m 1_j>, all n(n-1)/2 pairs), then seeded brick layers.
+
+    fuse_k > 0 groups the qubits in consecutive blocks of fuse_k: each block's H
+    and in-block phases form one BEGIN/END FUSION block, followed by the block's
+    phases towards later qubits (diagonal, so they commute with the rest of the
+    block and may leave it); the brick layers come in fusion blocks as in brick()."""
     ops = []
-    for j in range(n):
-        ops.append(("H", (j,), ()))
-        for m in range(j + 1, n):
-            ops.append(("U", (m, j), (m - j + 1,)))
-    ops += [op for op in brick(n, brick_layers, seed=seed)[n:]]
+    if not fuse_k:
+        for j in range(n):
+            ops.append(("H", (j,), ()))
+            for m in range(j + 1, n):
+                ops.append(("U", (m, j), (m - j + 1,)))
+        ops += [op for op in brick(n, brick_layers, seed=seed)[n:]]
+        return ops
+    for a in range(0, n, fuse_k):
+        b = min(n, a + fuse_k)
+        ops.append(("BEGIN FUSION", (), ()))
+        for j in range(a, b):
+            ops.append(("H", (j,), ()))
+            for m in range(j + 1, b):
+                ops.append(("U", (m, j), (m - j + 1,)))
+        ops.append(("END FUSION", (), ()))
+        for j in range(a, b):
+            for m in range(b, n):
+                ops.append(("U", (m, j), (m - j + 1,)))
+    layers = brick(n, brick_layers, seed=seed, fuse_k=fuse_k)
+    first_layer = next(i for i, op in enumerate(layers) if op[0] == "U3") - 1  # skip the H blocks
+    ops += layers[first_layer:]
     return ops
 
 
