@@ -121,16 +121,22 @@ template <int KB>  // KB = k + 1: K = N = 2^KB floats per row
 __global__ void __launch_bounds__(kTcThreads, 1)
 unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __restrict__ w_split, int* error_flag)
 {
-  constexpr uint32_t K = 1u << KB, N = K, KH = K / 2;
-  constexpr uint32_t B_BYTES = N * K * 4, A_BYTES = kTcM * KH * 4;
-  constexpr uint32_t SBO_A = (KH / 4) * 128u, SBO_B = (K / 4) * 128u;
-  constexpr uint32_t NCOLS = N;  // FP32 accumulator: 128 lanes x N columns
+  // Software pipeline over "stages" = K quarters of this CTA's tiles.  Stage s
+  // is split into A buffer s % 2 while the registers already fetch stage s + 1
+  // from HBM and the tensor cores still run stage s - 1; a tile's four stages
+  // accumulate into TMEM accumulator (tile % 2), so one tile's epilogue also
+  // overlaps the next tile's loads.
+  constexpr uint32_t K = 1u << KB, N = K, KQ = K / 4;
+  constexpr uint32_t B_BYTES = N * K * 4, AQ_BYTES = kTcM * KQ * 4;
+  constexpr uint32_t SBO_A = (KQ / 4) * 128u, SBO_B = (K / 4) * 128u;
+  constexpr uint32_t NCOLS = 2 * N;  // two FP32 accumulators of 128 lanes x N columns
+  constexpr uint32_t CG = KQ / 16;   // groups of 4 float4 per row quarter
+  constexpr uint32_t PER_THREAD = (kTcM / 8) * CG / (kTcThreads / 32);  // float4 per thread per stage
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* b_hi = smem;
   unsigned char* b_lo = smem + B_BYTES;
-  unsigned char* a_hi = smem + 2 * B_BYTES;
-  unsigned char* a_lo = a_hi + A_BYTES;
-  __shared__ __align__(8) uint64_t mbar;
+  unsigned char* a_base = smem + 2 * B_BYTES;  // buffer b: hi at a_base + 2b AQ, lo at + (2b + 1) AQ
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
@@ -139,10 +145,10 @@ unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
                  "r"(NCOLS));
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1u));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar[0])), "r"(1u));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar[1])), "r"(1u));
     abort_flag = 0;
   }
-  // W_hi, W_lo: precomputed in the operand layout, copied as-is.
   {
     float4* dst = reinterpret_cast<float4*>(smem);
     for (uint32_t i = tid; i < 2 * B_BYTES / 16; i += kTcThreads) dst[i] = w_split[i];
@@ -154,86 +160,115 @@ unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __
   const uint32_t tmem = tmem_slot;
   if (warp == 0) asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   const uint32_t idesc = tf32_idesc(kTcM, N);
-  const uint32_t mbar_addr = smem_addr(&mbar);
-  uint32_t phase = 0;
   const uint64_t tiles = rows / kTcM;
+  const uint64_t my_tiles = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint64_t stages = my_tiles * 4;
 
-  for (uint64_t tile = blockIdx.x; tile < tiles && !abort_flag; tile += gridDim.x) {
-    float* tile_rows = state + tile * kTcM * K;
-    for (uint32_t h = 0; h < 2; ++h) {
-      // Load the K half h of the 128 rows, split into hi / lo, store in the operand layout.
-      // A warp moves 8 rows x 4 float4: 512 contiguous shared-memory bytes.
-      constexpr uint32_t CG = KH / 16;  // groups of 4 float4 per row half
-      for (uint32_t blk = warp; blk < (kTcM / 8) * CG; blk += kTcThreads / 32) {
-        const uint32_t rg = blk / CG, cg = blk % CG;
-        const uint32_t r = rg * 8 + (lane & 7u), c4 = cg * 4 + (lane >> 3);
-        const float4 v = *reinterpret_cast<const float4*>(tile_rows + size_t(r) * K + h * KH + c4 * 4);
-        float4 hi, lo;
-        hi.x = tf32_rna(v.x); lo.x = tf32_rna(v.x - hi.x);
-        hi.y = tf32_rna(v.y); lo.y = tf32_rna(v.y - hi.y);
-        hi.z = tf32_rna(v.z); lo.z = tf32_rna(v.z - hi.z);
-        hi.w = tf32_rna(v.w); lo.w = tf32_rna(v.w - hi.w);
-        const uint32_t off = kmajor_offset(r, c4 * 4, KH);
-        *reinterpret_cast<float4*>(a_hi + off) = hi;
-        *reinterpret_cast<float4*>(a_lo + off) = lo;
-      }
-      async_proxy_fence();
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
-      if (tid == 0) {
-        const uint32_t ah = smem_addr(a_hi), al = smem_addr(a_lo), bh = smem_addr(b_hi), bl = smem_addr(b_lo);
+  // Where thread tid's float4 number i of a stage lives: row r, float column c (within the quarter).
+  auto slot = [&](uint32_t i, uint32_t& r, uint32_t& c) {
+    const uint32_t blk = warp + i * (kTcThreads / 32);
+    const uint32_t rg = blk / CG, cg = blk % CG;
+    r = rg * 8 + (lane & 7u);
+    c = (cg * 4 + (lane >> 3)) * 4;
+  };
+  auto stage_rows = [&](uint64_t st) { return state + (blockIdx.x + (st >> 2) * gridDim.x) * kTcM * K; };
+  float4 regs[PER_THREAD];
+  auto fetch = [&](uint64_t st) {
+    const float* base = stage_rows(st) + (st & 3u) * KQ;
 #pragma unroll
-        for (uint32_t s = 0; s < KH / 8; ++s) {
-          const uint32_t g = h * (KH / 8) + s;  // K step within the full K of W
-          const uint64_t da_hi = kmajor_desc(ah + s * 256u, 128u, SBO_A), da_lo = kmajor_desc(al + s * 256u, 128u, SBO_A);
-          const uint64_t db_hi = kmajor_desc(bh + g * 256u, 128u, SBO_B), db_lo = kmajor_desc(bl + g * 256u, 128u, SBO_B);
-          umma_tf32(tmem, da_hi, db_hi, idesc, (h | s) != 0 ? 1u : 0u);
-          umma_tf32(tmem, da_hi, db_lo, idesc, 1u);
-          umma_tf32(tmem, da_lo, db_hi, idesc, 1u);
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_addr)
-                     : "memory");
-      }
-      // The half's MMAs must finish before A is overwritten or the accumulator read.
-      if (!mbar_wait_bounded(mbar_addr, phase)) {
-        if (tid == 0) { atomicExch(error_flag, 1); abort_flag = 1; }
-      }
-      phase ^= 1u;
-      tc_fence_after();
-      __syncthreads();
-      if (abort_flag) break;
+    for (uint32_t i = 0; i < PER_THREAD; ++i) {
+      uint32_t r, c;
+      slot(i, r, c);
+      regs[i] = *reinterpret_cast<const float4*>(base + size_t(r) * K + c);
     }
-    if (abort_flag) break;
-    // Epilogue: warp w reads TMEM lanes 32w.. (rows), 32 columns at a time.
-    float* out_row = tile_rows + size_t(warp * 32 + lane) * K;
-#pragma unroll 1
-    for (uint32_t c = 0; c < N / 32; ++c) {
-      uint32_t v[32];
-      const uint32_t taddr = tmem + ((warp * 32u) << 16) + c * 32u;
-      asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      float4* dst = reinterpret_cast<float4*>(out_row + c * 32);
+  };
+  auto bounded_wait = [&](uint64_t st) {  // the MMAs of stage st have completed
+    if (!mbar_wait_bounded(smem_addr(&mbar[st & 1u]), uint32_t(st >> 1) & 1u)) {
+      atomicExch(error_flag, 1);
+      abort_flag = 1;
+    }
+  };
+
+  if (stages) fetch(0);
+  for (uint64_t st = 0; st < stages; ++st) {
+    const uint32_t buf = uint32_t(st & 1u);
+    unsigned char* a_hi = a_base + (2 * buf) * AQ_BYTES;
+    unsigned char* a_lo = a_hi + AQ_BYTES;
+    if (st >= 2) bounded_wait(st - 2);  // the tensor cores are done with this buffer
 #pragma unroll
-      for (int q = 0; q < 8; ++q)
-        dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
-                             __uint_as_float(v[4 * q + 3]));
+    for (uint32_t i = 0; i < PER_THREAD; ++i) {
+      uint32_t r, c;
+      slot(i, r, c);
+      const float4 v = regs[i];
+      float4 hi, lo;
+      hi.x = tf32_rna(v.x); lo.x = tf32_rna(v.x - hi.x);
+      hi.y = tf32_rna(v.y); lo.y = tf32_rna(v.y - hi.y);
+      hi.z = tf32_rna(v.z); lo.z = tf32_rna(v.z - hi.z);
+      hi.w = tf32_rna(v.w); lo.w = tf32_rna(v.w - hi.w);
+      const uint32_t off = kmajor_offset(r, c, KQ);
+      *reinterpret_cast<float4*>(a_hi + off) = hi;
+      *reinterpret_cast<float4*>(a_lo + off) = lo;
     }
-    // The next tile's MMAs overwrite the accumulator: every warp must have read it.
+    if (st + 1 < stages) fetch(st + 1);  // in flight while the tensor cores work
+    async_proxy_fence();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    if (abort_flag) break;
+    const uint32_t q = uint32_t(st & 3u);
+    const uint32_t acc = tmem + uint32_t((st >> 2) & 1u) * N;
+    if (tid == 0) {
+      const uint32_t ah = smem_addr(a_hi), al = smem_addr(a_lo), bh = smem_addr(b_hi), bl = smem_addr(b_lo);
+#pragma unroll
+      for (uint32_t j = 0; j < KQ / 8; ++j) {
+        const uint32_t g = q * (KQ / 8) + j;
+        const uint64_t da_hi = kmajor_desc(ah + j * 256u, 128u, SBO_A), da_lo = kmajor_desc(al + j * 256u, 128u, SBO_A);
+        const uint64_t db_hi = kmajor_desc(bh + g * 256u, 128u, SBO_B), db_lo = kmajor_desc(bl + g * 256u, 128u, SBO_B);
+        umma_tf32(acc, da_hi, db_hi, idesc, (q | j) != 0 ? 1u : 0u);
+        umma_tf32(acc, da_hi, db_lo, idesc, 1u);
+        umma_tf32(acc, da_lo, db_hi, idesc, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(&mbar[buf]))
+                   : "memory");
+    }
+    if (q == 3) {
+      // Tile complete once this stage's MMAs are: read the accumulator, write the rows back.
+      bounded_wait(st);
+      tc_fence_after();
+      __syncthreads();
+      if (abort_flag) break;
+      float* out_row = stage_rows(st) + size_t(warp * 32 + lane) * K;
+#pragma unroll 1
+      for (uint32_t c = 0; c < N / 32; ++c) {
+        uint32_t v[32];
+        const uint32_t taddr = acc + ((warp * 32u) << 16) + c * 32u;
+        asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+          "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+          "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        float4* dst = reinterpret_cast<float4*>(out_row + c * 32);
+#pragma unroll
+        for (int w = 0; w < 8; ++w)
+          dst[w] = make_float4(__uint_as_float(v[4 * w]), __uint_as_float(v[4 * w + 1]), __uint_as_float(v[4 * w + 2]),
+                               __uint_as_float(v[4 * w + 3]));
+      }
+      tc_fence_before();  // this accumulator is written again two tiles later
+    }
   }
-  // After a timed-out wait, let the MMAs of that half finish (bounded) before the accumulator is freed.
-  if (abort_flag) mbar_wait_bounded(mbar_addr, phase ^ 1u);
+  // Let every MMA this CTA issued finish (bounded) before the accumulators are freed.
+  if (stages) {
+    const uint64_t last = stages - 1;
+    if (!mbar_wait_bounded(smem_addr(&mbar[last & 1u]), uint32_t(last >> 1) & 1u)) atomicExch(error_flag, 1);
+    if (last >= 1 && !mbar_wait_bounded(smem_addr(&mbar[(last - 1) & 1u]), uint32_t((last - 1) >> 1) & 1u))
+      atomicExch(error_flag, 1);
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -275,7 +310,7 @@ size_t tc_w_split_floats(int k) { return size_t(2) << (2 * (k + 1)); }
 size_t tc_shared_bytes(int k)
 {
   const size_t K = size_t(1) << (k + 1);
-  return 2 * K * K * 4 + 2 * size_t(kTcM) * (K / 2) * 4;
+  return 2 * K * K * 4 + 4 * size_t(kTcM) * (K / 4) * 4;  // W hi/lo + two A stages (hi/lo) of K/4 columns
 }
 
 cudaError_t launch_unitary_tf32x3(float* state, int n, int k, const float* w_split, int* error_flag, int grid,
