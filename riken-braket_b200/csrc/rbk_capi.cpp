@@ -1768,12 +1768,20 @@ int move_to_low(rbk_state* s, const uint32_t* q, int k)
 {
   if (int rc = flush(s)) return rc;
   const int n = s->n;
+  // Virtual names chosen so that canonicalising moves as little as possible:
+  // target i is named i; every other qubit keeps the name of its physical bit,
+  // except those sitting on bits 0..k-1, which take the bits the targets leave.
   std::vector<int> sigma(n, -1);  // real logical -> virtual logical
-  std::vector<char> used(n, 0);
-  for (int i = 0; i < k; ++i) { sigma[q[i]] = i; used[q[i]] = 1; }
-  int next = k;
-  for (int l = 0; l < n; ++l)
-    if (!used[l]) sigma[l] = next++;
+  std::vector<char> is_target(n, 0);
+  for (int i = 0; i < k; ++i) { sigma[q[i]] = i; is_target[q[i]] = 1; }
+  std::vector<int> freed;
+  for (int i = 0; i < k; ++i)
+    if (s->perm[q[i]] >= k) freed.push_back(s->perm[q[i]]);
+  size_t f = 0;
+  for (int l = 0; l < n; ++l) {
+    if (is_target[l]) continue;
+    sigma[l] = s->perm[l] >= k ? s->perm[l] : freed.at(f++);
+  }
   bool in_place = true;
   for (int i = 0; i < k; ++i) in_place = in_place && s->perm[q[i]] == i;
   if (in_place) return RBK_OK;
