@@ -145,6 +145,32 @@ def ansatz_hamiltonian(n):
     return terms
 
 
+def inverse(ops):
+    """The exact inverse of an instruction list: gates reversed and each
+    replaced by its adjoint (U3(t, p, l)^-1 = U3(-t, -l, -p), U m j k -> U m j -k,
+    EX/EY/EZ and U1 with the negated angle; H, X, Y, Z, CNOT, CZ, SWAP are their
+    own inverses).  Fusion markers keep their places around the reversed gates."""
+    out = []
+    for mnem, q, p in reversed(ops):
+        if mnem == "BEGIN FUSION":
+            out.append(("END FUSION", (), ()))
+        elif mnem == "END FUSION":
+            out.append(("BEGIN FUSION", (), ()))
+        elif mnem == "U3":
+            out.append(("U3", q, (-p[0], -p[2], -p[1])))
+        elif mnem == "U":
+            out.append(("U", q, (-p[0],)))
+        elif mnem in ("U1", "EX", "EY", "EZ"):
+            out.append((mnem, q, (-p[0],)))
+        elif mnem == "U2":
+            out.append(("U3", q, (-math.pi / 2, -p[1], -p[0])))
+        elif mnem in ("H", "X", "Y", "Z", "CNOT", "CZ", "SWAP"):
+            out.append((mnem, q, p))
+        else:
+            raise ValueError(f"no inverse for {mnem}")
+    return out
+
+
 def batch_instances(count=4096, n_min=10, n_max=24, depth_min=4, depth_max=16, seed_base=1):
     """Config-5 style batch: instance i draws, from its own generator seeded
     seed_base + i, a qubit count n = round(exp(U[ln n_min, ln n_max])), a depth
