@@ -1839,11 +1839,37 @@ std::vector<float> build_w_split(const std::vector<cplx>& U, int k)
 int apply_unitary(rbk_state* s, const std::vector<cplx>& U, const uint32_t* q, int k)
 {
   device_guard g(s->device);
-  if (int rc = move_to_low(s, q, k)) return rc;
-  if (int rc = mark_launch_start(s)) return rc;
-  ++s->stats.gates_issued;
   const bool tensor = s->precision == RBK_C64 && (k == 5 || k == 6) && s->n >= k + 7;
   if (tensor) {
+    if (int rc = flush(s)) return rc;
+  } else if (int rc = move_to_low(s, q, k)) {
+    return rc;
+  }
+  if (int rc = mark_launch_start(s)) return rc;
+  ++s->stats.gates_issued;
+  if (tensor) {
+    // The kernel gathers rows at the targets' current physical bits: no relabelling pass.
+    rbk::tc_layout lay{};
+    uint64_t used = 0;
+    for (int i = 0; i < k; ++i) {
+      lay.target_bit[i] = static_cast<uint8_t>(s->perm[q[i]]);
+      used |= 1ull << s->perm[q[i]];
+    }
+    int j = 0;
+    for (int b = 0; b < s->n && j < 7; ++b)
+      if (!(used & (1ull << b))) { lay.row_bit[j++] = static_cast<uint8_t>(b); used |= 1ull << b; }
+    int src = 0;
+    for (int b = 0; b < s->n;) {
+      if (used & (1ull << b)) { ++b; continue; }
+      int len = 0;
+      while (b + len < s->n && !(used & (1ull << (b + len)))) ++len;
+      lay.run_src[lay.num_runs] = static_cast<uint8_t>(src);
+      lay.run_len[lay.num_runs] = static_cast<uint8_t>(len);
+      lay.run_dst[lay.num_runs] = static_cast<uint8_t>(b);
+      ++lay.num_runs;
+      src += len;
+      b += len;
+    }
     const std::vector<float> w = build_w_split(U, k);
     device_buffer dw;
     RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&dw.p), sizeof(float) * w.size()));
@@ -1854,8 +1880,8 @@ int apply_unitary(rbk_state* s, const std::vector<cplx>& U, const uint32_t* q, i
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     const uint64_t tiles = (1ull << (s->n - k)) / 128;
     const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(sms)));
-    const cudaError_t e = rbk::launch_unitary_tf32x3(static_cast<float*>(s->amps), s->n, k,
-                                                    reinterpret_cast<const float*>(dw.p), flag, grid, s->stream);
+    const cudaError_t e = rbk::launch_unitary_tf32x3(s->amps, s->n, k, reinterpret_cast<const float*>(dw.p), flag, grid,
+                                                    lay, s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "tensor-core unitary");
     ++s->stats.kernel_launches;
     ++s->stats.passes;

@@ -91,15 +91,25 @@ template <typename Real> cudaError_t launch_prob_scan(const void* amps, uint64_t
 cudaError_t launch_upper_bound(const double* prefix, uint64_t count, const double* r, int num, uint64_t* events,
                                cudaStream_t stream);
 
-// Dense k-qubit unitaries with the targets on the low k physical bits.
+// Dense k-qubit unitaries.
 // Tensor cores (complex<float>, k = 5 or 6, n >= k + 7): w_split holds W_hi then
 // W_lo (tc_w_split_floats(k) floats) in the kernel's operand layout; the kernel
 // needs tc_shared_bytes(k) of shared memory and sets *error_flag on a timeout.
+// Physical bits of the tensor-core kernel's rows: target_bit[i] is target i, row_bit[j]
+// row-index bit j of a 128-row tile, and the tile index is deposited run by run
+// into the remaining bits (n >= k + 7).
+struct tc_layout {
+  uint8_t target_bit[6];
+  uint8_t row_bit[7];
+  uint8_t num_runs;
+  uint8_t run_src[16], run_len[16], run_dst[16];
+};
 size_t tc_w_split_floats(int k);
 size_t tc_shared_bytes(int k);
-cudaError_t launch_unitary_tf32x3(float* state, int n, int k, const float* w_split, int* error_flag, int grid,
-                                  cudaStream_t stream);
-// CUDA cores, any precision, k <= 10: U is 2^k x 2^k complex (re, im) in row-major order on the device.
+cudaError_t launch_unitary_tf32x3(void* state, int n, int k, const float* w_split, int* error_flag, int grid,
+                                  const tc_layout& layout, cudaStream_t stream);
+// CUDA cores, any precision, k <= 10, targets on the low k physical bits: U is 2^k x 2^k
+// complex (re, im) in row-major order on the device.
 template <typename Real> cudaError_t launch_dense_rows(void* state, int n, int k, const double* U, cudaStream_t stream);
 
 }  // namespace rbk

@@ -1,9 +1,11 @@
 // rbk_tc.cu -- dense k-qubit unitaries (k = 5, 6) on a complex<float> state as
 // tensor-core GEMMs with 3xTF32 split products (tcgen05, accumulator in TMEM).
 //
-// With the k target qubits on the low k physical bits, the state is a matrix
-// of R = 2^(n-k) rows of 2^k complex amplitudes, stored as 2K = 2^(k+1)
-// interleaved floats.  Applying U is out_row = in_row . W with the real
+// Rows are the 2^(n-k) groups of 2^k amplitudes that differ only in the k
+// target bits; a row, read as 2K = 2^(k+1) interleaved floats, is one GEMM row.
+// The loads and stores gather rows through offset tables, so the targets may sit
+// on any physical bits; a CTA tile is 128 rows spread over the 7 lowest
+// non-target bits (contiguous 64-byte or longer runs in HBM).  Applying U is out_row = in_row . W with the real
 // 2K x 2K matrix
 //   W[2a][2b] = Re U[b][a],  W[2a+1][2b] = -Im U[b][a],
 //   W[2a][2b+1] = Im U[b][a], W[2a+1][2b+1] = Re U[b][a],
@@ -119,7 +121,8 @@ __device__ __forceinline__ uint32_t kmajor_offset(uint32_t row, uint32_t kk, uin
 
 template <int KB>  // KB = k + 1: K = N = 2^KB floats per row
 __global__ void __launch_bounds__(kTcThreads, 1)
-unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __restrict__ w_split, int* error_flag)
+unitary_tf32x3_kernel(float2* __restrict__ state, uint64_t rows, const float4* __restrict__ w_split, int* error_flag,
+                      const __grid_constant__ tc_layout L)
 {
   // Software pipeline over "stages" = K quarters of this CTA's tiles.  Stage s
   // is split into A buffer s % 2 while the registers already fetch stage s + 1
@@ -139,7 +142,19 @@ unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
+  __shared__ uint64_t row_off[kTcM], elem_off[N / 2];  // physical offsets of row bits / target bits
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  for (uint32_t i = tid; i < kTcM; i += kTcThreads) {
+    uint64_t o = 0;
+    for (int b = 0; b < 7; ++b) o |= uint64_t((i >> b) & 1u) << L.row_bit[b];
+    row_off[i] = o;
+  }
+  for (uint32_t i = tid; i < N / 2; i += kTcThreads) {
+    uint64_t o = 0;
+    for (int b = 0; b < KB - 1; ++b) o |= uint64_t((i >> b) & 1u) << L.target_bit[b];
+    elem_off[i] = o;
+  }
+  const bool pair = L.target_bit[0] == 0;  // then element pairs (2m, 2m+1) are 16-byte aligned neighbours
 
   if (warp == 0)
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
@@ -171,15 +186,28 @@ unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __
     r = rg * 8 + (lane & 7u);
     c = (cg * 4 + (lane >> 3)) * 4;
   };
-  auto stage_rows = [&](uint64_t st) { return state + (blockIdx.x + (st >> 2) * gridDim.x) * kTcM * K; };
+  // Tile t: its 2^(n-k-7) index deposited into the bits that are neither row nor target bits.
+  auto tile_base = [&](uint64_t st) {
+    const uint64_t t = blockIdx.x + (st >> 2) * gridDim.x;
+    uint64_t v = 0;
+    for (int r = 0; r < L.num_runs; ++r) v |= ((t >> L.run_src[r]) & ((1ull << L.run_len[r]) - 1)) << L.run_dst[r];
+    return v;
+  };
   float4 regs[PER_THREAD];
   auto fetch = [&](uint64_t st) {
-    const float* base = stage_rows(st) + (st & 3u) * KQ;
+    const uint64_t base = tile_base(st);
+    const uint32_t e0 = (uint32_t(st & 3u) * KQ) >> 1;  // first complex element of the quarter
 #pragma unroll
     for (uint32_t i = 0; i < PER_THREAD; ++i) {
       uint32_t r, c;
       slot(i, r, c);
-      regs[i] = *reinterpret_cast<const float4*>(base + size_t(r) * K + c);
+      const uint64_t rb = base | row_off[r];
+      if (pair) {  // elements 2m and 2m+1 are neighbours in memory: one 16-byte load
+        regs[i] = *reinterpret_cast<const float4*>(state + (rb | elem_off[e0 + (c >> 1)]));
+      } else {
+        const float2 x0 = state[rb | elem_off[e0 + (c >> 1)]], x1 = state[rb | elem_off[e0 + (c >> 1) + 1]];
+        regs[i] = make_float4(x0.x, x0.y, x1.x, x1.y);
+      }
     }
   };
   auto bounded_wait = [&](uint64_t st) {  // the MMAs of stage st have completed
@@ -238,7 +266,7 @@ unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __
       tc_fence_after();
       __syncthreads();
       if (abort_flag) break;
-      float* out_row = stage_rows(st) + size_t(warp * 32 + lane) * K;
+      const uint64_t out_row = tile_base(st) | row_off[warp * 32 + lane];
 #pragma unroll 1
       for (uint32_t c = 0; c < N / 32; ++c) {
         uint32_t v[32];
@@ -253,11 +281,17 @@ unitary_tf32x3_kernel(float* __restrict__ state, uint64_t rows, const float4* __
             "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
           : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        float4* dst = reinterpret_cast<float4*>(out_row + c * 32);
+        if (pair) {
 #pragma unroll
-        for (int w = 0; w < 8; ++w)
-          dst[w] = make_float4(__uint_as_float(v[4 * w]), __uint_as_float(v[4 * w + 1]), __uint_as_float(v[4 * w + 2]),
-                               __uint_as_float(v[4 * w + 3]));
+          for (int e = 0; e < 8; ++e)
+            *reinterpret_cast<float4*>(state + (out_row | elem_off[c * 16 + 2 * e])) =
+              make_float4(__uint_as_float(v[4 * e]), __uint_as_float(v[4 * e + 1]), __uint_as_float(v[4 * e + 2]),
+                          __uint_as_float(v[4 * e + 3]));
+        } else {
+#pragma unroll
+          for (int e = 0; e < 16; ++e)
+            state[out_row | elem_off[c * 16 + e]] = make_float2(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]));
+        }
       }
       tc_fence_before();  // this accumulator is written again two tiles later
     }
@@ -313,8 +347,8 @@ size_t tc_shared_bytes(int k)
   return 2 * K * K * 4 + 4 * size_t(kTcM) * (K / 4) * 4;  // W hi/lo + two A stages (hi/lo) of K/4 columns
 }
 
-cudaError_t launch_unitary_tf32x3(float* state, int n, int k, const float* w_split, int* error_flag, int grid,
-                                  cudaStream_t stream)
+cudaError_t launch_unitary_tf32x3(void* state, int n, int k, const float* w_split, int* error_flag, int grid,
+                                  const tc_layout& layout, cudaStream_t stream)
 {
   if ((k != 5 && k != 6) || n < k + 7) return cudaErrorInvalidValue;
   const uint64_t rows = 1ull << (n - k);
@@ -323,13 +357,13 @@ cudaError_t launch_unitary_tf32x3(float* state, int n, int k, const float* w_spl
   if (k == 6) {
     e = cudaFuncSetAttribute(unitary_tf32x3_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    unitary_tf32x3_kernel<7><<<grid, kTcThreads, smem, stream>>>(state, rows, reinterpret_cast<const float4*>(w_split),
-                                                                  error_flag);
+    unitary_tf32x3_kernel<7><<<grid, kTcThreads, smem, stream>>>(static_cast<float2*>(state), rows,
+                                                                  reinterpret_cast<const float4*>(w_split), error_flag, layout);
   } else {
     e = cudaFuncSetAttribute(unitary_tf32x3_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    unitary_tf32x3_kernel<6><<<grid, kTcThreads, smem, stream>>>(state, rows, reinterpret_cast<const float4*>(w_split),
-                                                                  error_flag);
+    unitary_tf32x3_kernel<6><<<grid, kTcThreads, smem, stream>>>(static_cast<float2*>(state), rows,
+                                                                  reinterpret_cast<const float4*>(w_split), error_flag, layout);
   }
   return cudaGetLastError();
 }
