@@ -88,8 +88,11 @@ int rbk_state_set_deferred(rbk_state* s, int deferred);
 /* Upper bound on dense 2x2 gates per fused pass (0 = built-in default). */
 int rbk_state_set_pass_budget(rbk_state* s, int max_dense_gates_per_pass);
 /* Tile shape of the fused passes: 0 = 2^12 amplitudes (c128; 2^13 for c64)
- * with 16 per thread, 1 = the same tile with 8 per thread, 2 = 2^11 (c128;
- * 2^12 for c64) with 16 per thread (the default).  Results do not depend on it. */
+ * with 16 (c64: 32) per thread, 2 = 2^11 (c128; 2^12 for c64) with 16 (32)
+ * per thread (the default), 3 = the tile of shape 2 in persistent CTAs that
+ * copy their next tile into shared memory while they work on the current one.
+ * Shape 1 (the tile of shape 0 with half the amplitudes per thread) is not
+ * built: RBK_ERR_INVALID.  Results do not depend on the shape. */
 int rbk_state_set_tile_shape(rbk_state* s, int shape);
 int rbk_state_get_stats(const rbk_state* s, rbk_stats* out);
 int rbk_state_reset_stats(rbk_state* s);

@@ -541,6 +541,7 @@ int rbk_state_set_tile_shape(rbk_state* s, int shape)
 {
   if (int rc = check_state(s)) return rc;
   if (shape < 0 || shape >= rbk::kNumShapes) return fail(RBK_ERR_INVALID, "unknown tile shape");
+  if (shape == 1) return fail(RBK_ERR_INVALID, "tile shape 1 is not built");
   if (int rc = guarded([&] { return canonicalize(s); })) return rc;
   s->shape = shape;
   return RBK_OK;

@@ -20,26 +20,30 @@ namespace rbk {
 // the register bits R (2^R amplitudes per thread, 2^(K-R) threads); LOW low
 // physical bits are always tile bits (512-byte contiguous runs in HBM).
 //   shape 0: K = 12 (c128) / 13 (c64), 256 threads, 2 CTAs per SM
-//   shape 1: same tile, half the registers per thread, 512 threads
+//   shape 1: same tile, half the registers per thread, 512 threads (planned
+//            on the host only; no kernel is built for it)
 //   shape 2: K = 11 (c128) / 12 (c64), 128 threads, 4 CTAs per SM
-constexpr int kNumShapes = 3;
+//   shape 3: the tile of shape 2 in a persistent CTA (3 per SM) that copies
+//            its next tile into a second shared-memory buffer with cp.async
+//            while it works on the current one
+constexpr int kNumShapes = 4;
 template <typename Real> struct precision_traits;
 template <> struct precision_traits<double> { static constexpr int VEC = 1, VB = 0, LOW = 5; };
 template <> struct precision_traits<float> { static constexpr int VEC = 2, VB = 1, LOW = 6; };
 
 template <typename Real, int SHAPE> struct tile_shape;
-template <> struct tile_shape<double, 0> { static constexpr int K = 12, R = 4, CTAS = 2; };
-template <> struct tile_shape<double, 1> { static constexpr int K = 12, R = 3, CTAS = 2; };
-template <> struct tile_shape<double, 2> { static constexpr int K = 11, R = 4, CTAS = 4; };
-template <> struct tile_shape<float, 0> { static constexpr int K = 13, R = 5, CTAS = 2; };
-template <> struct tile_shape<float, 1> { static constexpr int K = 13, R = 4, CTAS = 2; };
-template <> struct tile_shape<float, 2> { static constexpr int K = 12, R = 5, CTAS = 4; };
+template <> struct tile_shape<double, 0> { static constexpr int K = 12, R = 4, CTAS = 2; static constexpr bool PIPE = false; };
+template <> struct tile_shape<double, 2> { static constexpr int K = 11, R = 4, CTAS = 4; static constexpr bool PIPE = false; };
+template <> struct tile_shape<double, 3> { static constexpr int K = 11, R = 4, CTAS = 3; static constexpr bool PIPE = true; };
+template <> struct tile_shape<float, 0> { static constexpr int K = 13, R = 5, CTAS = 2; static constexpr bool PIPE = false; };
+template <> struct tile_shape<float, 2> { static constexpr int K = 12, R = 5, CTAS = 4; static constexpr bool PIPE = false; };
+template <> struct tile_shape<float, 3> { static constexpr int K = 12, R = 5, CTAS = 3; static constexpr bool PIPE = true; };
 
 // Host view of a tile shape: tile bits, register bits (precision 0 = c128, 1 = c64).
 inline void shape_bits(int precision, int shape, int* K, int* R)
 {
-  static const int k128[kNumShapes] = {12, 12, 11}, r128[kNumShapes] = {4, 3, 4};
-  static const int k64[kNumShapes] = {13, 13, 12}, r64[kNumShapes] = {5, 4, 5};
+  static const int k128[kNumShapes] = {12, 12, 11, 11}, r128[kNumShapes] = {4, 3, 4, 4};
+  static const int k64[kNumShapes] = {13, 13, 12, 12}, r64[kNumShapes] = {5, 4, 5, 5};
   *K = precision == 0 ? k128[shape] : k64[shape];
   *R = precision == 0 ? r128[shape] : r64[shape];
 }

@@ -154,6 +154,34 @@ def test_pass_budget_and_immediate_mode_agree(pkg, budget):
     assert s2.stats()["passes"] >= len([op for op in ops if op[0] != "SWAP"])
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("shape", [0, 2, 3])
+def test_every_tile_shape_vs_oracle(pkg, shape, precision):
+    """Each tile shape (3: the persistent CTAs that copy their next tile with
+    cp.async) on a brick plus random gates, at sizes from one tile to many
+    tiles per CTA, in both precisions."""
+    tol = TOL64 if precision == 0 else TOL32
+    for n in (13, 17, 21):
+        ops = pkg.circuits.brick(n, 4, seed=n + shape) + pkg.circuits.random_circuit(n, 150, seed=n + 10 * shape)
+        init = random_state(n, n + shape)
+        s = pkg.State(n, precision)
+        s.set_tile_shape(shape)
+        s.upload(init)
+        o = oracle.COracle(n)
+        o.set_amplitudes(init)
+        s.apply(ops)
+        o.apply(ops)
+        assert np.abs(s.amplitudes().astype(np.complex128) - o.amplitudes()).max() <= tol, (n, shape, precision)
+        assert s.stats()["passes"] >= 1
+        s.close()
+
+
+def test_tile_shape_1_is_rejected(pkg):
+    with pkg.State(13) as s:
+        with pytest.raises(pkg.RbkError):
+            s.set_tile_shape(1)
+
+
 def test_layout_map_swaps_and_canonicalize(pkg):
     n = 18
     rng = np.random.default_rng(8)
