@@ -68,13 +68,16 @@ enum op_kind : uint8_t {
 #else
 #define RBK_HOST_DEVICE
 #endif
+// Dense codes 0 .. kNumOpCodes-1 (register bits 0..4), so that the kernel's
+// switch over them can be a jump table.
 RBK_HOST_DEVICE constexpr uint32_t op_code(int kind, int form, bool controlled, int treg)
 {
-  return kind == OPK_MAT ? uint32_t((form * 2 + (controlled ? 1 : 0)) * 8 + treg)
-       : kind == OPK_X ? 48u + uint32_t(treg)
-       : kind == OPK_Y ? 56u + uint32_t(treg)
-       : kind == OPK_NEG ? 64u : 65u;
+  return kind == OPK_MAT ? uint32_t((form * 2 + (controlled ? 1 : 0)) * 5 + treg)
+       : kind == OPK_X ? 30u + uint32_t(treg)
+       : kind == OPK_Y ? 35u + uint32_t(treg)
+       : kind == OPK_NEG ? 40u : 41u;
 }
+constexpr uint32_t kNumOpCodes = 42;
 
 // One gate inside a pass, in the coordinates of the phase it belongs to.
 struct alignas(8) dev_op {

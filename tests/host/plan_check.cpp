@@ -119,7 +119,7 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
           const uint32_t want_code = op.kind == OPK_MAT ? op_code(OPK_MAT, op.real, op.creg != 0, op.treg)
                                    : (op.kind == OPK_X || op.kind == OPK_Y) ? op_code(op.kind, 0, true, op.treg)
                                    : op_code(op.kind, 0, true, 0);
-          if (op.code != want_code || op.treg >= R) { std::fprintf(stderr, "bad dispatch code\n"); std::exit(8); }
+          if (op.code != want_code || op.code >= kNumOpCodes || op.treg >= R) { std::fprintf(stderr, "bad dispatch code\n"); std::exit(8); }
           if ((uint32_t(tid) & op.cthr) != op.cthr || (base & op.cout) != op.cout) continue;
           const cplx m00{op.m[0], op.m[1]}, m01{op.m[2], op.m[3]}, m10{op.m[4], op.m[5]}, m11{op.m[6], op.m[7]};
           for (int i = 0; i < NR; ++i) {
