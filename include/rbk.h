@@ -225,6 +225,13 @@ int rbk_expectation_pauli(rbk_state* s, int num_terms, const char* strings, cons
 int rbk_inner_product(rbk_state* a, rbk_state* b, double* out);
 /* ket::fidelity: |<b|a>|^2 (fidelity.hpp) */
 int rbk_fidelity(rbk_state* a, rbk_state* b, double* out);
+/* <b| H |a> for H = sum_t coeffs[t] P_t given like rbk_expectation_pauli:
+ * ket::inner_product(a, b, observable) as bra's INNERPROD n <operator> calls it
+ * (bra/src/nompi_state.cpp:2602-2648; the observable's Pauli action follows
+ * pauli_index_coeff.hpp:17-59).  Same state requirements as rbk_inner_product. */
+int rbk_inner_product_pauli(rbk_state* a, rbk_state* b, int num_terms, const char* strings, const double* coeffs, double* out);
+/* |<b| H |a>|^2 (ket::fidelity with an observable; bra's FIDELITY n <operator>). */
+int rbk_fidelity_pauli(rbk_state* a, rbk_state* b, int num_terms, const char* strings, const double* coeffs, double* out);
 
 /* ---- sampling and measurement -------------------------------------------
  * Random numbers come from a std::mt19937_64 per state, seeded with 1 at

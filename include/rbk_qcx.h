@@ -9,16 +9,25 @@
  * qubits are unsigned integers, angles are decimal literals or the constants
  * :PI :HALF_PI :TWO_PI :ROOT_TWO :HALF_ROOT_TWO (also :REAL:<literal>).
  *
- * Supported: QUBITS, CIRCUITS 1, INITIAL STATE, BIT ASSIGNMENT (accepted; the
- * nompi build ignores it), MPIPROCESSES / MPISWAPBUFFER (ignored), the gate set
- * of docs/bra.md (I.., H, NOT, X/Y/Z and their multi-qubit forms, SWAP, S/T,
- * SX/SY/SZ.., U1/U2/U3, R, U, +X/-X/+Y/-Y, EX/EY/EZ.., ESWAP, TOFFOLI, with "+"
- * adjoints and C../Cn control prefixes), M, CLEAR, SET, SHORBOX, BEGIN/END
- * FUSION, BEGIN MEASUREMENT, DO MEASUREMENT [p], DO AMPLITUDES [i ...],
- * GENERATE EVENTS n seed, EXPECTATION :PAULIS:<s> q..., PRINT / PRINTLN of
- * literals and built-in symbols (:RESULT, :OUTCOME, :OUTCOMES:i, ...), EXIT.
- * Not supported (RBK_ERR_UNSUPPORTED naming the line): several circuits
- * (CIRCUITS n > 1, BEGIN CIRCUIT, INNERPROD, FIDELITY), classical variables and
+ * Supported: QUBITS, CIRCUITS n, BEGIN CIRCUIT k / END CIRCUIT, INITIAL STATE,
+ * BIT ASSIGNMENT (accepted; the nompi build ignores it), MPIPROCESSES /
+ * MPISWAPBUFFER (ignored), the gate set of docs/bra.md (I.., H, NOT, X/Y/Z and
+ * their multi-qubit forms, SWAP, S/T, SX/SY/SZ.., U1/U2/U3, R, U,
+ * +X/-X/+Y/-Y, EX/EY/EZ.., ESWAP, TOFFOLI, with "+" adjoints and C../Cn control
+ * prefixes), M, CLEAR, SET, SHORBOX, BEGIN/END FUSION, BEGIN MEASUREMENT, DO
+ * MEASUREMENT [p], DO AMPLITUDES [i ...], GENERATE EVENTS n seed, EXPECTATION
+ * :PAULIS:<s> q..., INNERPROD / FIDELITY (k | ALL) [:PAULIS:<s> q...], PRINT /
+ * PRINTLN of literals and built-in symbols (:RESULT, :OUTCOME, :OUTCOMES:i,
+ * ...), EXIT.
+ * Several circuits run as bra's nompi build runs them (bra/src/bra.cpp:299-760):
+ * one state each, circuit 0 seeded with the given seed and circuit k >= 1 with
+ * the k-th draw of std::mt19937_64(seed); each circuit runs until it finishes or
+ * reaches an INNERPROD / FIDELITY, and those are evaluated when their partner
+ * (or, for ALL, every circuit) waits on the matching instruction.  Their value
+ * goes to :RESULT: <Psi_k|Psi_c> (c the running circuit, k the partner; circuit
+ * 0 for ALL), with <Psi_k| H |Psi_c> when an operator is given, and the squared
+ * modulus for FIDELITY.
+ * Not supported (RBK_ERR_UNSUPPORTED naming the line): classical variables and
  * control flow (VAR, LET, @label, JUMP, JUMPIF, SEND, RECEIVE, BROADCAST,
  * GATHER, SCATTER), DEPOLARIZING, PERMUTATION, RANDOM PERMUTATION.
  */
@@ -52,8 +61,17 @@ enum {
   RBK_QCX_PROJECTIVE = 8,       /* M t */
   RBK_QCX_EXPECTATION = 9,      /* text = Pauli string, targets = operated qubits */
   RBK_QCX_PRINT = 10,           /* text = arguments separated by one space; ints[0] = 1 for PRINTLN */
-  RBK_QCX_NOOP = 11             /* I, IC, C..I: MPI-only identities */
+  RBK_QCX_NOOP = 11,            /* I, IC, C..I: MPI-only identities */
+  RBK_QCX_INNERPROD = 12,       /* ints[0] = partner circuit, RBK_QCX_ALL or RBK_QCX_NONE; text = Pauli
+                                   string (empty: no operator), targets = operated qubits */
+  RBK_QCX_FIDELITY = 13         /* as RBK_QCX_INNERPROD */
 };
+
+/* Partner of INNERPROD / FIDELITY: every circuit (ALL), or none -- bra does
+ * nothing for the running circuit's own index or a column that is neither a
+ * number nor ALL (bra/src/nompi_state.cpp:1204-1220). */
+#define RBK_QCX_ALL (-1)
+#define RBK_QCX_NONE (-2)
 
 /* Gate kinds (the numbering of the oracle's reference leg, for tests). */
 enum {
@@ -79,6 +97,7 @@ typedef struct rbk_qcx_instruction {
   int32_t num_targets;
   int32_t num_controls;
   int32_t num_values;
+  int32_t circuit;     /* circuit the instruction belongs to (BEGIN CIRCUIT k; 0 outside) */
   uint32_t targets[RBK_QCX_MAX_QUBITS];
   uint32_t controls[RBK_QCX_MAX_QUBITS];
   double params[3];
@@ -103,15 +122,17 @@ void rbk_qcx_default_options(rbk_qcx_options* options);
 int rbk_qcx_parse(const char* text, size_t length, rbk_qcx_program** out);
 int rbk_qcx_destroy(rbk_qcx_program* program);
 int rbk_qcx_num_qubits(const rbk_qcx_program* program, int* out);
+int rbk_qcx_num_circuits(const rbk_qcx_program* program, int* out);
 int rbk_qcx_initial_state(const rbk_qcx_program* program, uint64_t* out);
 int rbk_qcx_num_instructions(const rbk_qcx_program* program, int* out);
 int rbk_qcx_get_instruction(const rbk_qcx_program* program, int index, rbk_qcx_instruction* out);
 
-/* Runs the program on a new state and returns bra's standard output in *text
- * (NUL-terminated; release with rbk_qcx_free_text).  state_out, if not NULL,
- * receives the final state (release with rbk_state_destroy); if the program
- * ends with GENERATE EVENTS the state is intact (bra leaves prefix sums in its
- * buffer). */
+/* Runs the program on new states (one per circuit) and returns bra's standard
+ * output in *text (NUL-terminated; release with rbk_qcx_free_text).
+ * state_out, if not NULL, receives circuit 0's final state (release with
+ * rbk_state_destroy); if the program ends with GENERATE EVENTS the state is
+ * intact (bra leaves prefix sums in its buffer).  Circuits that wait on each
+ * other in a way that never resolves (bra loops forever) give RBK_ERR_STATE. */
 int rbk_qcx_run(const rbk_qcx_program* program, const rbk_qcx_options* options, char** text, rbk_state** state_out);
 void rbk_qcx_free_text(char* text);
 

@@ -26,7 +26,8 @@ KG = dict(H=1, NOT=2, X=3, Y=4, Z=5, SWAP=6, SX=7, SX_ADJ=8, SY=9, SY_ADJ=10, SZ
           EX_ADJ=26, EY=27, EY_ADJ=28, EZ=29, EZ_ADJ=30, ESWAP=31, ESWAP_ADJ=32, TOFFOLI=33, CLEAR=34, SET=35,
           SHORBOX=36)
 OP = dict(GATE=1, BEGIN_FUSION=2, END_FUSION=3, MEASUREMENT=4, AMPLITUDES=5, GENERATE_EVENTS=6, EXIT=7,
-          PROJECTIVE=8, EXPECTATION=9, PRINT=10, NOOP=11)
+          PROJECTIVE=8, EXPECTATION=9, PRINT=10, NOOP=11, INNERPROD=12, FIDELITY=13)
+ALL, NONE = -1, -2  # INNERPROD / FIDELITY partner: every circuit, or nothing to do
 
 CONSTANTS = {":REAL": 0.0, ":IMAG": 0.0, ":PI": math.pi, ":HALF_PI": math.pi / 2, ":TWO_PI": 2 * math.pi,
              ":ROOT_TWO": math.sqrt(2.0), ":HALF_ROOT_TWO": math.sqrt(0.5)}
@@ -59,12 +60,18 @@ def _count(body, letter):
 
 def parse(text):
     """Returns (num_qubits, initial_state, instructions); each instruction is a
-    dict with op, kind, targets, controls, params, ints, values, text, line."""
+    dict with op, kind, targets, controls, params, ints, values, text, line, circuit."""
+    return parse_program(text)[:3]
+
+
+def parse_program(text):
+    """parse() plus the number of circuits (CIRCUITS n)."""
     n, init, code = None, 0, []
+    state = dict(circuit=0, in_circuit=False, num_circuits=1)
 
     def ins(op, line, **kw):
         d = dict(op=OP[op], kind=0, targets=[], controls=[], params=[0.0, 0.0, 0.0], ints=[0, 0], values=[], text="",
-                 line=line)
+                 line=line, circuit=state["circuit"])
         d.update(kw)
         code.append(d)
 
@@ -167,8 +174,7 @@ def parse(text):
             n = int(cols[1])
             continue
         if m == "CIRCUITS":
-            if int(cols[1]) != 1:
-                raise QcxError("several circuits")
+            state["num_circuits"] = int(cols[1])
             continue
         if m == "INITIAL":
             init = int(cols[2])
@@ -183,12 +189,25 @@ def parse(text):
                 ins("MEASUREMENT", line_no, ints=[3, 0])
             elif word(1) == "FUSION":
                 ins("BEGIN_FUSION", line_no)
+            elif word(1) == "CIRCUIT":
+                state["circuit"], state["in_circuit"] = int(cols[2]), True
             else:
                 raise QcxError("BEGIN")
         elif m == "END":
-            if word(1) != "FUSION":
+            if word(1) == "CIRCUIT":
+                state["circuit"], state["in_circuit"] = 0, False
+            elif word(1) == "FUSION":
+                ins("END_FUSION", line_no)
+            else:
                 raise QcxError("END")
-            ins("END_FUSION", line_no)
+        elif m in ("INNERPROD", "FIDELITY"):
+            who = cols[1]
+            if who[0].isdigit():
+                partner = NONE if int(who) == state["circuit"] else int(who)
+            else:
+                partner = ALL if who.upper() == "ALL" else NONE
+            pauli = cols[2][len(":PAULIS:"):].upper() if len(cols) >= 4 else ""
+            ins(m, line_no, ints=[partner, 0], text=pauli, targets=[qubit(t) for t in cols[3:]])
         elif m == "DO":
             if word(1) == "MEASUREMENT":
                 ins("MEASUREMENT", line_no, ints=[int(cols[2]) if len(cols) == 3 else 3, 0])
@@ -234,7 +253,7 @@ def parse(text):
             raise QcxError(f"line {line_no}: unknown mnemonic {m}")
     if n is None:
         raise QcxError("no QUBITS")
-    return n, init, code
+    return n, init, code, state["num_circuits"]
 
 
 # ---- execution on the reference ----------------------------------------------
@@ -279,19 +298,50 @@ def _bits(v, n):
     return format(v, "0%db" % n) if n else ""
 
 
-def run(text, seed=1, threads=1):
-    """Returns (output text without timing lines, final amplitudes, reference state)."""
-    n, init, code = parse(text)
-    r = oracle.KetRef(n, initial_index=init, threads=threads)
-    r.seed(seed)
-    out = []
-    outcomes = [-1] * n
-    last_measured = 0
-    result = 0j
-    i = 0
-    while i < len(code):
+class _MT64:
+    """std::mt19937_64 (the published MT19937-64 of Nishimura and Matsumoto:
+    w = 64, n = 312, m = 156, r = 31), for the per-circuit seeds bra draws."""
+    N, M = 312, 156
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed):
+        self.mt = [seed & self.MASK]
+        for i in range(1, self.N):
+            prev = self.mt[-1]
+            self.mt.append((6364136223846793005 * (prev ^ (prev >> 62)) + i) & self.MASK)
+        self.i = self.N
+
+    def __call__(self):
+        if self.i >= self.N:
+            upper, lower = 0xFFFFFFFF80000000, 0x7FFFFFFF
+            for k in range(self.N):
+                x = (self.mt[k] & upper) | (self.mt[(k + 1) % self.N] & lower)
+                xa = (x >> 1) ^ (0xB5026F5AA96619E9 if x & 1 else 0)
+                self.mt[k] = self.mt[(k + self.M) % self.N] ^ xa
+            self.i = 0
+        y = self.mt[self.i]
+        self.i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & self.MASK
+
+
+def _overlap(a, b, ins):
+    """ket::inner_product(a, b[, P]) = <b| [P] |a> (squared modulus for FIDELITY) on the reference."""
+    v = a.inner_product_on(b, ins["text"], ins["targets"]) if ins["text"] else a.inner_product(b)
+    return complex(abs(v) ** 2, 0.0) if ins["op"] == OP["FIDELITY"] else v
+
+
+def _run_circuit(c, n, out):
+    """Runs circuit context c until it finishes or waits (bra::interpreter::apply_circuit)."""
+    r, code = c["r"], c["code"]
+    while c["pc"] < len(code) and c["wait"] is None:
+        i = c["pc"]
         ins = code[i]
         op = ins["op"]
+        c["pc"] = i + 1
         if op == OP["BEGIN_FUSION"]:
             j = i + 1
             while j < len(code) and code[j]["op"] != OP["END_FUSION"]:
@@ -300,9 +350,7 @@ def run(text, seed=1, threads=1):
             cores = [_as_core(g) if g["op"] == OP["GATE"] else None for g in block]
             if block and all(cores):
                 r.apply([("BEGIN FUSION", (), ())] + cores + [("END FUSION", (), ())])
-                i = j + 1
-                continue
-            i += 1
+                c["pc"] = j + 1
             continue
         if op == OP["END_FUSION"] or op == OP["NOOP"]:
             pass
@@ -335,23 +383,84 @@ def run(text, seed=1, threads=1):
             out.append("Measurement result: %d\n" % r.measure())
         elif op == OP["PROJECTIVE"]:
             q = ins["targets"][0]
-            outcomes[q] = r.projective_measurement(q)
-            last_measured = q
+            c["outcomes"][q] = r.projective_measurement(q)
+            c["last"] = q
         elif op == OP["EXPECTATION"]:
-            result = r.expectation_on(ins["text"], ins["targets"])
+            c["result"] = r.expectation_on(ins["text"], ins["targets"])
+        elif op in (OP["INNERPROD"], OP["FIDELITY"]):
+            if ins["ints"][0] != NONE:
+                c["wait"] = ins
         elif op == OP["PRINT"]:
             parts = []
+            result = c["result"]
             for a in ins["text"].split():
                 if a[0].isdigit() or a[0] in "+-.":
                     parts.append(a)
                 elif a == ":RESULT":
                     parts.append("(%s,%s)" % (_g(result.real), _g(result.imag)))
                 elif a == ":OUTCOME":
-                    parts.append(str(outcomes[last_measured]))
+                    parts.append(str(c["outcomes"][c["last"]]))
                 elif a.startswith(":OUTCOMES:"):
-                    parts.append(str(outcomes[int(a[10:])]))
+                    parts.append(str(c["outcomes"][int(a[10:])]))
                 elif a in CONSTANTS:
                     parts.append(_g(CONSTANTS[a]))
             out.append(" ".join(parts) + ("\n" if ins["ints"][0] else ""))
-        i += 1
-    return "".join(out), r.amplitudes(), r
+
+
+def _kind(w):
+    return (2 if w["op"] == OP["FIDELITY"] else 0) + (1 if w["text"] else 0) + (4 if w["ints"][0] == ALL else 0)
+
+
+def run(text, seed=1, threads=1):
+    """Returns (output text without timing lines, circuit 0's final amplitudes,
+    circuit 0's reference state).  Several circuits run as bra's nompi
+    scheduler runs them (bra/src/bra.cpp:299-760): circuit 0 seeded with
+    `seed`, circuit k >= 1 with the k-th draw of std::mt19937_64(seed); each
+    runs until it waits on an INNERPROD / FIDELITY, then the pairs that wait
+    on each other are evaluated in circuit order, or the ALL form once every
+    circuit waits on it."""
+    n, init, code, nc = parse_program(text)
+    draws = _MT64(seed)
+    ctx = []
+    for k in range(nc):
+        r = oracle.KetRef(n, initial_index=init, threads=threads)
+        r.seed(seed if k == 0 else draws())
+        ctx.append(dict(r=r, code=[i for i in code if i["circuit"] == k], pc=0, outcomes=[-1] * n, last=0,
+                        result=0j, wait=None))
+    out = []
+    while True:
+        for c in ctx:
+            if c["wait"] is None:
+                _run_circuit(c, n, out)
+        if all(c["wait"] is None for c in ctx):
+            break
+        progress, all_kind, all_same = False, None, True
+        for k, c in enumerate(ctx):
+            if c["wait"] is None:
+                all_same = False
+                continue
+            kind = _kind(c["wait"])
+            if kind >= 4:
+                if all_kind is None:
+                    all_kind = kind
+                elif all_kind != kind:
+                    all_same = False
+                continue
+            all_same = False
+            o = ctx[c["wait"]["ints"][0]]
+            if o["wait"] is None or _kind(o["wait"]) != kind or o["wait"]["ints"][0] != k:
+                continue
+            v = _overlap(c["r"], o["r"], c["wait"])
+            c["result"], o["result"] = v, v.conjugate()
+            c["wait"] = o["wait"] = None
+            progress = True
+        if not progress and all_same and all_kind is not None:
+            w = ctx[0]["wait"]
+            for c in ctx:
+                c["result"] = _overlap(ctx[0]["r"], c["r"], w)
+            for c in ctx:
+                c["wait"] = None
+            progress = True
+        if not progress:
+            raise QcxError("circuits wait on partners that never arrive")
+    return "".join(out), ctx[0]["r"].amplitudes(), ctx[0]["r"]

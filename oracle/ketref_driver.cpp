@@ -667,6 +667,45 @@ void ketref_expectation_on(void* h, char const* pauli, int num_qubits, int const
   out[1] = value.imag();
 }
 
+// INNERPROD n :PAULIS:<s> q_0 ... q_{m-1} with one Pauli string of coefficient 1:
+// bra::inner_product_op (bra/src/nompi_state.cpp:2602-2648) through
+// ket::runtime::ranges::inner_product(state_a, state_b, observable, qubits)
+// = <b| P |a> (ket/include/ket/inner_product.hpp:223-258).
+void ketref_inner_product_on(void* a, void* b, char const* pauli, int num_qubits, int const* qubits, double* out)
+{
+  auto& sa = *static_cast<ref_state*>(a);
+  auto& sb = *static_cast<ref_state*>(b);
+  std::string const str(pauli, static_cast<std::size_t>(num_qubits));
+  std::vector<qubit_t> operated;
+  for (int i = 0; i < num_qubits; ++i) operated.push_back(qb(qubits[i]));
+  auto const nq = operated.size();
+  auto const value = ket::runtime::ranges::inner_product(
+    sa.policy, sa.data, sb.data,
+    [&str, nq](auto const ket_first, auto const bra_first, auto const index_wo_qubits,
+               auto const& unsorted_qubits_or_masks, auto const& sorted_qubits_or_index_masks)
+    {
+      complex_t acc{};
+      auto const last_index = bra::state_integer_type{1} << nq;
+      for (auto bra_index = bra::state_integer_type{0}; bra_index < last_index; ++bra_index)
+      {
+        auto const bra_it = bra_first + ket::gate::utility::index_with_qubits(
+          index_wo_qubits, bra_index,
+          std::begin(unsorted_qubits_or_masks), std::end(unsorted_qubits_or_masks),
+          std::begin(sorted_qubits_or_index_masks), std::end(sorted_qubits_or_index_masks));
+        auto const ket_index_coeff = ket::gate::utility::pauli_index_coeff<complex_t>(str, bra_index);
+        auto const ket_it = ket_first + ket::gate::utility::index_with_qubits(
+          index_wo_qubits, ket_index_coeff.first,
+          std::begin(unsorted_qubits_or_masks), std::end(unsorted_qubits_or_masks),
+          std::begin(sorted_qubits_or_index_masks), std::end(sorted_qubits_or_index_masks));
+        acc += std::conj(*bra_it) * (ket_index_coeff.second * *ket_it);
+      }
+      return acc;
+    },
+    operated);
+  out[0] = value.real();
+  out[1] = value.imag();
+}
+
 // One gate of the wider instruction set (kinds in oracle_ops.h).
 int ketref_gate(void* h, int kind, int num_targets, int const* targets, int num_controls, int const* controls,
                 double const* params)

@@ -83,6 +83,8 @@ class KetRef:
                                     ctypes.c_void_p, ctypes.c_void_p]
         lib.ketref_expectation_on.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_void_p]
+        lib.ketref_inner_product_on.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p]
         lib.ketref_generate_events.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p]
         lib.ketref_measure.argtypes = [ctypes.c_void_p]
         lib.ketref_measure.restype = ctypes.c_uint64
@@ -154,6 +156,13 @@ class KetRef:
         q = np.ascontiguousarray(list(qubits), dtype=np.int32)
         out = np.empty(2, dtype=np.float64)
         self.lib.ketref_expectation_on(self.h, pauli.encode(), len(qubits), q.ctypes.data, out.ctypes.data)
+        return complex(out[0], out[1])
+
+    def inner_product_on(self, other, pauli, qubits):
+        """<other| P |self> with the Pauli string `pauli` on `qubits` (bra's INNERPROD n :PAULIS:<pauli> q ...)."""
+        q = np.ascontiguousarray(list(qubits), dtype=np.int32)
+        out = np.empty(2, dtype=np.float64)
+        self.lib.ketref_inner_product_on(self.h, other.h, pauli.encode(), len(qubits), q.ctypes.data, out.ctypes.data)
         return complex(out[0], out[1])
 
     def generate_events(self, num, seed=-1):

@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <iomanip>
+#include <random>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -28,6 +29,7 @@ int set_last_error(int code, const char* msg);
 
 struct rbk_qcx_program {
   int num_qubits = -1;
+  int num_circuits = 1;
   uint64_t initial_state = 0;
   std::vector<rbk_qcx_instruction> code;
   std::vector<std::vector<uint64_t>> amplitude_lists;  // DO AMPLITUDES index lists, by instruction
@@ -128,6 +130,8 @@ struct parser {
   rbk_qcx_program& prog;
   int line = 0;
   bool done = false;
+  int circuit = 0;          // BEGIN CIRCUIT k ... END CIRCUIT (bra/src/interpreter.cpp:672-745)
+  bool in_circuit = false;
 
   uint32_t qubit(const std::string& s)
   {
@@ -279,9 +283,12 @@ struct parser {
       prog.num_qubits = static_cast<int>(n);
       return;
     }
-    if (m == "CIRCUITS") {
+    if (m == "CIRCUITS") {  // bra resizes its circuit list (interpreter.cpp:411-419)
       expect(c, 2);
-      if (to_unsigned(c[1]) != 1) unsupported("several circuits (CIRCUITS > 1) are not supported");
+      const uint64_t n = to_unsigned(c[1]);
+      if (n < 1 || n > 64) bad("CIRCUITS must be between 1 and 64");
+      if (static_cast<int>(n) <= circuit) bad("CIRCUITS leaves out the current circuit");
+      prog.num_circuits = static_cast<int>(n);
       return;
     }
     if (m == "INITIAL") {  // INITIAL STATE v
@@ -299,7 +306,7 @@ struct parser {
     if (m == "MPIPROCESSES" || m == "MPISWAPBUFFER") return;
     if (m == "DEPOLARIZING" || m == "PERMUTATION" || m == "RANDOM" || m == "VAR" || m == "LET" || m == "SEND" ||
         m == "RECEIVE" || m == "BROADCAST" || m == "GATHER" || m == "SCATTER" || m == "JUMP" || m == "JUMPIF" ||
-        m == "INNERPROD" || m == "FIDELITY" || m.front() == '@')
+        m.front() == '@')
       unsupported("'" + m + "' is not supported");
     if (prog.num_qubits < 0) bad("QUBITS must come first");
     if (m == "EXIT") {
@@ -316,7 +323,13 @@ struct parser {
         prog.code.push_back(in);
       } else if (w == "FUSION") {
         prog.code.push_back(blank(RBK_QCX_BEGIN_FUSION, line));
-      } else if (w == "CIRCUIT" || w == "LEARNING") {
+      } else if (w == "CIRCUIT") {
+        if (c.size() != 3 || in_circuit) bad("expected BEGIN CIRCUIT <index> outside another circuit block");
+        const uint64_t k = to_unsigned(c[2]);
+        if (k >= static_cast<uint64_t>(prog.num_circuits)) bad("circuit index " + c[2] + " is not below CIRCUITS");
+        circuit = static_cast<int>(k);
+        in_circuit = true;
+      } else if (w == "LEARNING") {
         unsupported("BEGIN " + w + " is not supported");
       } else {
         bad("unknown BEGIN statement");
@@ -326,7 +339,11 @@ struct parser {
     if (m == "END") {
       const std::string w = word(1);
       if (w == "FUSION") prog.code.push_back(blank(RBK_QCX_END_FUSION, line));
-      else if (w == "CIRCUIT") unsupported("END CIRCUIT is not supported");
+      else if (w == "CIRCUIT") {
+        if (!in_circuit) bad("END CIRCUIT without BEGIN CIRCUIT");
+        circuit = 0;
+        in_circuit = false;
+      }
       else bad("unknown END statement");
       return;
     }
@@ -382,6 +399,37 @@ struct parser {
         if (std::find(seen.begin(), seen.end(), q) != seen.end()) bad("qubit " + c[i] + " appears twice");
         seen.push_back(q);
         in.targets[in.num_targets++] = q;
+      }
+      prog.code.push_back(in);
+      return;
+    }
+    if (m == "INNERPROD" || m == "FIDELITY") {  // interpreter.cpp:3253-3330
+      if (c.size() != 2 && c.size() < 4) bad("expected " + m + " (<circuit> | ALL) [<operator> <qubits>]");
+      auto in = blank(m == "INNERPROD" ? RBK_QCX_INNERPROD : RBK_QCX_FIDELITY, line);
+      const std::string& who = c[1];
+      if (std::isdigit(static_cast<unsigned char>(who.front()))) {
+        const uint64_t k = to_unsigned(who);
+        if (k >= static_cast<uint64_t>(prog.num_circuits)) bad("circuit " + who + " is not below CIRCUITS");
+        in.ints[0] = static_cast<int>(k) == circuit ? RBK_QCX_NONE : static_cast<int64_t>(k);
+      } else {
+        in.ints[0] = upper(who) == "ALL" ? RBK_QCX_ALL : RBK_QCX_NONE;
+      }
+      if (c.size() >= 4) {
+        const std::string& op = c[2];
+        if (op.rfind(":PAULIS:", 0) != 0 || op.size() <= 8) unsupported(m + " takes a :PAULIS:<string> literal");
+        const std::string str = upper(op.substr(8));
+        if (str.size() != c.size() - 3) bad("the Pauli string length must equal the number of qubits");
+        if (str.size() >= sizeof(in.text) || str.size() > RBK_QCX_MAX_QUBITS) bad("Pauli string too long");
+        for (char ch : str)
+          if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z') bad("Pauli strings use I, X, Y, Z");
+        std::memcpy(in.text, str.c_str(), str.size() + 1);
+        std::vector<uint32_t> seen;
+        for (size_t i = 3; i < c.size(); ++i) {
+          const uint32_t q = qubit(c[i]);
+          if (std::find(seen.begin(), seen.end(), q) != seen.end()) bad("qubit " + c[i] + " appears twice");
+          seen.push_back(q);
+          in.targets[in.num_targets++] = q;
+        }
       }
       prog.code.push_back(in);
       return;
@@ -447,13 +495,18 @@ struct parser {
       while (ls >> tok) c.push_back(tok);
       if (c.empty()) continue;
       try {
+        const size_t before = prog.code.size();
         statement(std::move(c));
+        for (size_t i = before; i < prog.code.size(); ++i) prog.code[i].circuit = circuit;
       } catch (qcx_error const& e) {
         throw qcx_error(e.code, "line " + std::to_string(line) + ": " + e.what());
       }
     }
     if (prog.num_qubits < 0) bad("no QUBITS statement");
     if (prog.initial_state >= (1ull << prog.num_qubits)) bad("INITIAL STATE is out of range");
+    for (const auto& in : prog.code)
+      if ((in.op == RBK_QCX_INNERPROD || in.op == RBK_QCX_FIDELITY) && in.ints[0] >= prog.num_circuits)
+        throw qcx_error(RBK_ERR_INVALID, "line " + std::to_string(in.line) + ": circuit index is not below CIRCUITS");
   }
 };
 
@@ -501,24 +554,42 @@ void check(int rc)
   if (rc != RBK_OK) throw qcx_error(rc, rbk_last_error());
 }
 
-struct runner {
-  const rbk_qcx_program& prog;
-  const rbk_qcx_options& opt;
+// One circuit of the program: bra's nompi_state with its wait reason
+// (bra/include/bra/state.hpp wait_reason; bra/src/nompi_state.cpp:1204-1275).
+struct circuit_ctx {
   rbk_state* s = nullptr;
-  std::ostringstream out;
+  std::vector<size_t> code;  // indices into the program, in order
+  size_t pc = 0;             // next instruction
   clock_type::time_point start, last;
   std::vector<int> last_outcomes;
   int last_measured = 0;
   cplx result{0.0, 0.0};
+  bool in_fusion = false;
+  const rbk_qcx_instruction* wait = nullptr;  // INNERPROD / FIDELITY this circuit waits on
+};
+
+struct runner {
+  const rbk_qcx_program& prog;
+  const rbk_qcx_options& opt;
+  std::ostringstream out;
+  std::vector<circuit_ctx> circ;
+  circuit_ctx* cur = nullptr;  // the running circuit
+  rbk_state* s = nullptr;      // its state
 
   runner(const rbk_qcx_program& p, const rbk_qcx_options& o) : prog(p), opt(o) {}
+
+  void select(circuit_ctx& c)
+  {
+    cur = &c;
+    s = c.s;
+  }
 
   void mark(const char* what)
   {
     check(rbk_state_synchronize(s));
     const auto now = clock_type::now();
-    if (opt.print_timing) out << what << " finished: " << seconds(start, now) << " (" << seconds(last, now) << ")\n";
-    last = now;
+    if (opt.print_timing) out << what << " finished: " << seconds(cur->start, now) << " (" << seconds(cur->last, now) << ")\n";
+    cur->last = now;
   }
 
   void gate(const rbk_qcx_instruction& g)
@@ -694,7 +765,7 @@ struct runner {
     const double coeff[2] = {1.0, 0.0};
     double r[2];
     check(rbk_expectation_pauli(s, 1, full.c_str(), coeff, r));
-    result = cplx{r[0], r[1]};
+    cur->result = cplx{r[0], r[1]};
   }
 
   // bra::state::generate_print_string (bra/src/state.cpp:495-538) for literals and built-ins.
@@ -709,17 +780,17 @@ struct runner {
       const char f = a.front();
       if (std::isdigit(static_cast<unsigned char>(f)) || f == '+' || f == '-' || f == '.') { out << a; continue; }
       if (f != ':') continue;  // classical variables do not exist here
-      if (a == ":RESULT") out << result;
+      if (a == ":RESULT") out << cur->result;
       else if (a == ":I") out << cplx{0.0, 1.0};
       else if (a == ":MINUS_I") out << cplx{0.0, -1.0};
       else if (a == ":COMPLEX") out << cplx{0.0, 0.0};
       else if (a == ":INT") out << 0;
-      else if (a == ":OUTCOME") out << last_outcomes[static_cast<size_t>(last_measured)];
-      else if (a == ":OUTCOMES") out << last_outcomes.front();
+      else if (a == ":OUTCOME") out << cur->last_outcomes[static_cast<size_t>(cur->last_measured)];
+      else if (a == ":OUTCOMES") out << cur->last_outcomes.front();
       else if (a.rfind(":OUTCOMES:", 0) == 0) {
         const int64_t q = to_int(a.substr(10));
         if (q < 0 || q >= prog.num_qubits) throw qcx_error(RBK_ERR_INVALID, "line " + std::to_string(in.line) + ": qubit out of range");
-        out << last_outcomes[static_cast<size_t>(q)];
+        out << cur->last_outcomes[static_cast<size_t>(q)];
       } else {
         out << to_real(a);
       }
@@ -727,16 +798,42 @@ struct runner {
     if (in.ints[0]) out << '\n';
   }
 
-  void execute()
+  // The Pauli string of an INNERPROD / FIDELITY operator over all qubits.
+  std::string operator_string(const rbk_qcx_instruction& in) const
   {
-    const size_t count = prog.code.size();
-    for (size_t i = 0; i < count; ++i) {
+    std::string full(static_cast<size_t>(prog.num_qubits), 'I');
+    for (int k = 0; k < in.num_targets; ++k) full[in.targets[k]] = in.text[k];
+    return full;
+  }
+
+  // ket::inner_product(a, b[, H]) = <b| [H] |a>, or its squared modulus.
+  cplx overlap(rbk_state* a, rbk_state* b, const rbk_qcx_instruction& in)
+  {
+    double r[2] = {0.0, 0.0};
+    if (in.text[0]) {
+      const std::string full = operator_string(in);
+      const double coeff[2] = {1.0, 0.0};
+      check(rbk_inner_product_pauli(a, b, 1, full.c_str(), coeff, r));
+    } else {
+      check(rbk_inner_product(a, b, r));
+    }
+    if (in.op == RBK_QCX_FIDELITY) return cplx{r[0] * r[0] + r[1] * r[1], 0.0};
+    return cplx{r[0], r[1]};
+  }
+
+  // Runs the selected circuit until it finishes or waits (bra::interpreter::apply_circuit,
+  // bra/src/interpreter.cpp:851-871).
+  void run_circuit()
+  {
+    circuit_ctx& c = *cur;
+    while (c.pc < c.code.size() && !c.wait) {
+      const size_t i = c.code[c.pc++];
       const auto& in = prog.code[i];
       try {
         switch (in.op) {
           case RBK_QCX_GATE: gate(in); break;
-          case RBK_QCX_BEGIN_FUSION: check(rbk_begin_fusion(s)); break;
-          case RBK_QCX_END_FUSION: check(rbk_end_fusion(s)); break;
+          case RBK_QCX_BEGIN_FUSION: check(rbk_begin_fusion(s)); c.in_fusion = true; break;
+          case RBK_QCX_END_FUSION: check(rbk_end_fusion(s)); c.in_fusion = false; break;
           case RBK_QCX_MEASUREMENT: measurement(static_cast<int>(in.ints[0])); break;
           case RBK_QCX_AMPLITUDES:
             amplitudes(i < prog.amplitude_lists.size() ? prog.amplitude_lists[i] : std::vector<uint64_t>{});
@@ -746,18 +843,73 @@ struct runner {
           case RBK_QCX_PROJECTIVE: {
             int outcome = 0;
             check(rbk_projective_measurement(s, in.targets[0], &outcome));
-            last_outcomes[in.targets[0]] = outcome;
-            last_measured = static_cast<int>(in.targets[0]);
+            c.last_outcomes[in.targets[0]] = outcome;
+            c.last_measured = static_cast<int>(in.targets[0]);
             break;
           }
           case RBK_QCX_EXPECTATION: expectation(in); break;
           case RBK_QCX_PRINT: print(in); break;
+          case RBK_QCX_INNERPROD: case RBK_QCX_FIDELITY:
+            // bra::state::inner_product / fidelity refuse a fused block (bra/src/state.cpp:2133-2170)
+            if (c.in_fusion) throw qcx_error(RBK_ERR_UNSUPPORTED, "INNERPROD / FIDELITY inside BEGIN/END FUSION");
+            if (in.ints[0] != RBK_QCX_NONE) c.wait = &in;
+            break;
           case RBK_QCX_NOOP: break;
           default: throw qcx_error(RBK_ERR_INVALID, "unknown instruction");
         }
       } catch (qcx_error const& e) {
         throw qcx_error(e.code, "line " + std::to_string(in.line) + ": " + e.what());
       }
+    }
+  }
+
+  // bra's nompi scheduler (bra/src/bra.cpp:329-760): run every circuit that is
+  // not waiting; then evaluate the pairs that wait on each other (the lower
+  // circuit index first, as the scan meets it), or, when every circuit waits
+  // on the same ALL instruction, that collective.
+  void execute()
+  {
+    const int nc = static_cast<int>(circ.size());
+    auto kind_of = [](const rbk_qcx_instruction* w) {
+      // 0: pair INNERPROD, 1: pair INNERPROD with operator, 2/3: FIDELITY; +4: ALL
+      return (w->op == RBK_QCX_FIDELITY ? 2 : 0) + (w->text[0] ? 1 : 0) + (w->ints[0] == RBK_QCX_ALL ? 4 : 0);
+    };
+    while (true) {
+      for (auto& c : circ)
+        if (!c.wait) {
+          select(c);
+          run_circuit();
+        }
+      if (std::none_of(circ.begin(), circ.end(), [](const circuit_ctx& c) { return c.wait != nullptr; })) break;
+      bool progress = false;
+      int all_kind = -1;  // the ALL kind every circuit waits on, if any
+      bool all_same = true;
+      for (int k = 0; k < nc; ++k) {
+        circuit_ctx& c = circ[static_cast<size_t>(k)];
+        if (!c.wait) { all_same = false; continue; }
+        const int kind = kind_of(c.wait);
+        if (kind >= 4) {
+          if (all_kind < 0) all_kind = kind;
+          else if (all_kind != kind) all_same = false;
+          continue;
+        }
+        all_same = false;
+        const int other = static_cast<int>(c.wait->ints[0]);
+        circuit_ctx& o = circ[static_cast<size_t>(other)];
+        if (!o.wait || kind_of(o.wait) != kind || o.wait->ints[0] != k) continue;
+        const cplx r = overlap(c.s, o.s, *c.wait);  // <Psi_other| [H] |Psi_k>
+        c.result = r;
+        o.result = std::conj(r);
+        c.wait = o.wait = nullptr;
+        progress = true;
+      }
+      if (!progress && all_same && all_kind >= 0) {
+        const rbk_qcx_instruction& in = *circ.front().wait;  // the operator comes from circuit 0
+        for (auto& c : circ) c.result = overlap(circ.front().s, c.s, in);  // <Psi_c| [H] |Psi_0>
+        for (auto& c : circ) c.wait = nullptr;
+        progress = true;
+      }
+      if (!progress) throw qcx_error(RBK_ERR_STATE, "circuits wait on INNERPROD / FIDELITY partners that never arrive");
     }
   }
 };
@@ -822,6 +974,13 @@ int rbk_qcx_num_qubits(const rbk_qcx_program* p, int* out)
   return RBK_OK;
 }
 
+int rbk_qcx_num_circuits(const rbk_qcx_program* p, int* out)
+{
+  if (!p || !out) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
+  *out = p->num_circuits;
+  return RBK_OK;
+}
+
 int rbk_qcx_initial_state(const rbk_qcx_program* p, uint64_t* out)
 {
   if (!p || !out) return rbk::set_last_error(RBK_ERR_INVALID, "null argument");
@@ -854,28 +1013,44 @@ int rbk_qcx_run(const rbk_qcx_program* p, const rbk_qcx_options* options, char**
     rbk_qcx_default_options(&opt);
     if (options) opt = *options;
     runner r(*p, opt);
-    r.last_outcomes.assign(static_cast<size_t>(p->num_qubits), -1);  // ket::gate::outcome::unspecified
-    r.start = r.last = clock_type::now();
-    check(rbk_state_create(p->num_qubits, opt.precision, p->initial_state, opt.device, &r.s));
+    r.circ.resize(static_cast<size_t>(p->num_circuits));
+    for (size_t i = 0; i < p->code.size(); ++i) r.circ[static_cast<size_t>(p->code[i].circuit)].code.push_back(i);
+    auto release = [&] {
+      for (auto& c : r.circ)
+        if (c.s) rbk_state_destroy(c.s);
+    };
     try {
-      check(rbk_state_seed(r.s, opt.seed));
-      check(rbk_state_set_deferred(r.s, opt.deferred));
+      // Circuit 0 takes the given seed, circuit k >= 1 the k-th draw of
+      // std::mt19937_64(seed) (bra/src/bra.cpp:300-326).
+      std::mt19937_64 seeds(opt.seed);
+      const auto now = clock_type::now();
+      for (size_t k = 0; k < r.circ.size(); ++k) {
+        auto& c = r.circ[k];
+        c.last_outcomes.assign(static_cast<size_t>(p->num_qubits), -1);  // ket::gate::outcome::unspecified
+        c.start = c.last = now;
+        check(rbk_state_create(p->num_qubits, opt.precision, p->initial_state, opt.device, &c.s));
+        check(rbk_state_seed(c.s, k == 0 ? opt.seed : seeds()));
+        check(rbk_state_set_deferred(c.s, opt.deferred));
+      }
       r.execute();
-      check(rbk_state_synchronize(r.s));
+      for (auto& c : r.circ) check(rbk_state_synchronize(c.s));
     } catch (...) {
-      rbk_state_destroy(r.s);
+      release();
       throw;
     }
     const std::string o = r.out.str();
     char* buf = static_cast<char*>(std::malloc(o.size() + 1));
     if (!buf) {
-      rbk_state_destroy(r.s);
+      release();
       return rbk::set_last_error(RBK_ERR_OOM, "host memory exhausted");
     }
     std::memcpy(buf, o.c_str(), o.size() + 1);
     *text = buf;
-    if (state_out) *state_out = r.s;
-    else rbk_state_destroy(r.s);
+    if (state_out) {
+      *state_out = r.circ.front().s;
+      r.circ.front().s = nullptr;
+    }
+    release();
     return RBK_OK;
   });
 }

@@ -348,6 +348,49 @@ int read_out(rbk_state* s, int count)
   return bounded_sync(s);
 }
 
+// Pauli strings (one character per logical qubit) as physical flip/sign masks,
+// grouped by flip mask:  (P psi)(i) = (-i)^{#Y} (-1)^{popcount(i & (Y|Z))} psi(i ^ (X|Y))
+// (ket/include/ket/gate/utility/pauli_index_coeff.hpp:17-59).  Uses s->perm:
+// call after the queued gates have run.
+struct pauli_group_terms { uint64_t flip; rbk::pauli_terms terms; };
+
+int group_pauli_terms(const rbk_state* s, int num_terms, const char* strings, const double* coeffs,
+                      std::vector<pauli_group_terms>& groups)
+{
+  struct term { uint64_t flip, sign; cplx w; };
+  std::vector<term> terms;
+  for (int t = 0; t < num_terms; ++t) {
+    uint64_t x = 0, y = 0, z = 0;
+    for (int k = 0; k < s->n; ++k) {
+      const char c = strings[static_cast<size_t>(t) * s->n + k];
+      const uint64_t b = 1ull << s->perm[k];
+      if (c == 'X') x |= b;
+      else if (c == 'Y') y |= b;
+      else if (c == 'Z') z |= b;
+      else if (c != 'I') return fail(RBK_ERR_INVALID, "Pauli strings use the characters I, X, Y, Z");
+    }
+    static const cplx pow_mi[4] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}};
+    const cplx w = cplx{coeffs[2 * t], coeffs[2 * t + 1]} * pow_mi[__builtin_popcountll(y) & 3];
+    terms.push_back({x | y, y | z, w});
+  }
+  std::vector<char> done(terms.size(), 0);
+  for (size_t i = 0; i < terms.size(); ++i) {
+    if (done[i]) continue;
+    pauli_group_terms g{};
+    g.flip = terms[i].flip;
+    for (size_t j = i; j < terms.size() && g.terms.count < rbk::kMaxPauliTerms; ++j) {
+      if (done[j] || terms[j].flip != terms[i].flip) continue;
+      g.terms.sign[g.terms.count] = terms[j].sign;
+      g.terms.w[g.terms.count][0] = terms[j].w.real();
+      g.terms.w[g.terms.count][1] = terms[j].w.imag();
+      ++g.terms.count;
+      done[j] = 1;
+    }
+    groups.push_back(g);
+  }
+  return RBK_OK;
+}
+
 // sum over one flip-mask group of Pauli terms (physical masks).
 int pauli_group(rbk_state* s, uint64_t flip, const rbk::pauli_terms& t, double* out2)
 {
@@ -887,38 +930,12 @@ int rbk_expectation_pauli(rbk_state* s, int num_terms, const char* strings, cons
     // The queued gates may move qubits (SWAPs, relabelling): map logical
     // qubits to physical bits only after they have run.
     if (int rc = flush(s)) return rc;
-    struct term { uint64_t flip, sign; cplx w; };
-    std::vector<term> terms;
-    for (int t = 0; t < num_terms; ++t) {
-      uint64_t x = 0, y = 0, z = 0;
-      for (int k = 0; k < s->n; ++k) {
-        const char c = strings[static_cast<size_t>(t) * s->n + k];
-        const uint64_t b = 1ull << s->perm[k];
-        if (c == 'X') x |= b;
-        else if (c == 'Y') y |= b;
-        else if (c == 'Z') z |= b;
-        else if (c != 'I') return fail(RBK_ERR_INVALID, "Pauli strings use the characters I, X, Y, Z");
-      }
-      // (P psi)(i) = (-i)^{#Y} (-1)^{popcount(i & (Y|Z))} psi(i ^ (X|Y))  (pauli_index_coeff.hpp:17-59)
-      static const cplx pow_mi[4] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}};
-      const cplx w = cplx{coeffs[2 * t], coeffs[2 * t + 1]} * pow_mi[__builtin_popcountll(y) & 3];
-      terms.push_back({x | y, y | z, w});
-    }
-    std::vector<char> done(terms.size(), 0);
+    std::vector<pauli_group_terms> groups;
+    if (int rc = group_pauli_terms(s, num_terms, strings, coeffs, groups)) return rc;
     double acc_re = 0, acc_im = 0;
-    for (size_t i = 0; i < terms.size(); ++i) {
-      if (done[i]) continue;
-      rbk::pauli_terms pt{};
-      for (size_t j = i; j < terms.size() && pt.count < rbk::kMaxPauliTerms; ++j) {
-        if (done[j] || terms[j].flip != terms[i].flip) continue;
-        pt.sign[pt.count] = terms[j].sign;
-        pt.w[pt.count][0] = terms[j].w.real();
-        pt.w[pt.count][1] = terms[j].w.imag();
-        ++pt.count;
-        done[j] = 1;
-      }
+    for (const auto& g : groups) {
       double r[2];
-      if (int rc = pauli_group(s, terms[i].flip, pt, r)) return rc;
+      if (int rc = pauli_group(s, g.flip, g.terms, r)) return rc;
       acc_re += r[0];
       acc_im += r[1];
     }
@@ -964,6 +981,55 @@ int rbk_fidelity(rbk_state* a, rbk_state* b, double* out)
   if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
   double ip[2];
   if (int rc = rbk_inner_product(a, b, ip)) return rc;
+  *out = ip[0] * ip[0] + ip[1] * ip[1];
+  return RBK_OK;
+}
+
+int rbk_inner_product_pauli(rbk_state* a, rbk_state* b, int num_terms, const char* strings, const double* coeffs, double* out)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(a)) return rc;
+    if (int rc = check_state(b)) return rc;
+    if (num_terms < 0 || (num_terms > 0 && (!strings || !coeffs)) || !out)
+      return fail(RBK_ERR_INVALID, "bad Pauli term arguments");
+    if (a->n != b->n || a->precision != b->precision) return fail(RBK_ERR_INVALID, "states differ in size or precision");
+    if (a->device != b->device) return fail(RBK_ERR_UNSUPPORTED, "states live on different devices");
+    if (int rc = flush(a)) return rc;
+    if (int rc = flush(b)) return rc;
+    if (a->perm != b->perm) {
+      if (int rc = canonicalize(a)) return rc;
+      if (int rc = canonicalize(b)) return rc;
+    }
+    if (int rc = flush(b)) return rc;
+    {
+      device_guard g(b->device);
+      if (int rc = bounded_sync(b)) return rc;
+    }
+    std::vector<pauli_group_terms> groups;
+    if (int rc = group_pauli_terms(a, num_terms, strings, coeffs, groups)) return rc;
+    double acc_re = 0, acc_im = 0;
+    for (const auto& g : groups) {
+      int rc = launch_reduction(a, [&] {
+        return a->precision == RBK_C128
+          ? rbk::launch_pauli2<double>(a->amps, b->amps, a->n, g.flip, g.terms, a->d_partials, a->d_out, a->stream)
+          : rbk::launch_pauli2<float>(a->amps, b->amps, a->n, g.flip, g.terms, a->d_partials, a->d_out, a->stream);
+      });
+      if (rc) return rc;
+      if ((rc = read_out(a, 2))) return rc;
+      acc_re += a->h_out[0];
+      acc_im += a->h_out[1];
+    }
+    out[0] = acc_re;
+    out[1] = acc_im;
+    return RBK_OK;
+  });
+}
+
+int rbk_fidelity_pauli(rbk_state* a, rbk_state* b, int num_terms, const char* strings, const double* coeffs, double* out)
+{
+  if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
+  double ip[2];
+  if (int rc = rbk_inner_product_pauli(a, b, num_terms, strings, coeffs, ip)) return rc;
   *out = ip[0] * ip[0] + ip[1] * ip[1];
   return RBK_OK;
 }

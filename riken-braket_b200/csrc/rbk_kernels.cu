@@ -214,6 +214,35 @@ pauli_kernel(const typename ctype<Real>::c* __restrict__ a, int n, uint64_t flip
   block_sum_store<2>(vals, 2, partials + size_t(blockIdx.x) * 2);
 }
 
+// <b| P |a> summed over Pauli strings sharing one flip mask F:
+//   out = sum_i conj(b_i) a_{i^F} W(i),  W(i) = sum_t w_t (-1)^popcount(i & s_t)
+// ((P a)_i = coeff(i) a_{i^F}, ket/include/ket/gate/utility/pauli_index_coeff.hpp:17-59).
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads)
+pauli2_kernel(const typename ctype<Real>::c* __restrict__ a, const typename ctype<Real>::c* __restrict__ b, int n,
+              uint64_t flip, const pauli_terms T, double* partials)
+{
+  const uint64_t size = 1ull << n;
+  double re = 0, im = 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += stride) {
+    const auto x = a[i ^ flip], y = b[i];
+    // c = conj(b_i) a_{i^F}
+    const double cr = double(y.x) * double(x.x) + double(y.y) * double(x.y);
+    const double ci = double(y.x) * double(x.y) - double(y.y) * double(x.x);
+    double wr = 0, wi = 0;
+    for (int t = 0; t < T.count; ++t) {
+      const double s = (__popcll(i & T.sign[t]) & 1) ? -1.0 : 1.0;
+      wr += s * T.w[t][0];
+      wi += s * T.w[t][1];
+    }
+    re += cr * wr - ci * wi;
+    im += cr * wi + ci * wr;
+  }
+  double vals[2] = {re, im};
+  block_sum_store<2>(vals, 2, partials + size_t(blockIdx.x) * 2);
+}
+
 // <b|a> = sum conj(b_i) a_i
 template <typename Real>
 __global__ void __launch_bounds__(kRedThreads)
@@ -263,6 +292,17 @@ cudaError_t launch_pauli(const void* state, int n, uint64_t flip, const pauli_te
 }
 
 template <typename Real>
+cudaError_t launch_pauli2(const void* a, const void* b, int n, uint64_t flip, const pauli_terms& terms, double* partials,
+                          double* out, cudaStream_t stream)
+{
+  const int blocks = reduction_blocks();
+  pauli2_kernel<Real><<<blocks, kRedThreads, 0, stream>>>(static_cast<const typename ctype<Real>::c*>(a),
+                                                          static_cast<const typename ctype<Real>::c*>(b), n, flip, terms, partials);
+  finish_partials_kernel<<<1, 32, 0, stream>>>(partials, blocks, 2, out);
+  return cudaGetLastError();
+}
+
+template <typename Real>
 cudaError_t launch_inner(const void* a, const void* b, int n, double* partials, double* out, cudaStream_t stream)
 {
   const int blocks = reduction_blocks();
@@ -283,6 +323,8 @@ template cudaError_t launch_zsum<double>(const void*, int, double*, double*, cud
 template cudaError_t launch_zsum<float>(const void*, int, double*, double*, cudaStream_t);
 template cudaError_t launch_pauli<double>(const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
 template cudaError_t launch_pauli<float>(const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
+template cudaError_t launch_pauli2<double>(const void*, const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
+template cudaError_t launch_pauli2<float>(const void*, const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
 template cudaError_t launch_inner<double>(const void*, const void*, int, double*, double*, cudaStream_t);
 template cudaError_t launch_inner<float>(const void*, const void*, int, double*, double*, cudaStream_t);
 template cudaError_t launch_probs<double>(const void*, uint64_t, uint64_t, double*, cudaStream_t);

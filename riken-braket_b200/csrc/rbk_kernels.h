@@ -38,6 +38,9 @@ inline size_t reduction_scratch_doubles() { return size_t(1 << 12) * (1 + kMaxQu
 template <typename Real> cudaError_t launch_zsum(const void* state, int n, double* partials, double* out, cudaStream_t stream);
 template <typename Real> cudaError_t launch_pauli(const void* state, int n, uint64_t flip, const pauli_terms& terms,
                                                   double* partials, double* out, cudaStream_t stream);
+// <b| sum_t w_t P_t |a> for strings sharing the flip mask `flip`.
+template <typename Real> cudaError_t launch_pauli2(const void* a, const void* b, int n, uint64_t flip, const pauli_terms& terms,
+                                                   double* partials, double* out, cudaStream_t stream);
 template <typename Real> cudaError_t launch_inner(const void* a, const void* b, int n, double* partials, double* out,
                                                   cudaStream_t stream);
 template <typename Real> cudaError_t launch_probs(const void* state, uint64_t offset, uint64_t count, double* out,

@@ -19,12 +19,13 @@ MAX_VALUES = 40
 class Instruction(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int32), ("kind", ctypes.c_int32), ("line", ctypes.c_int32),
                 ("num_targets", ctypes.c_int32), ("num_controls", ctypes.c_int32), ("num_values", ctypes.c_int32),
-                ("targets", ctypes.c_uint32 * MAX_QUBITS), ("controls", ctypes.c_uint32 * MAX_QUBITS),
+                ("circuit", ctypes.c_int32), ("targets", ctypes.c_uint32 * MAX_QUBITS), ("controls", ctypes.c_uint32 * MAX_QUBITS),
                 ("params", ctypes.c_double * 3), ("ints", ctypes.c_int64 * 2),
                 ("values", ctypes.c_uint64 * MAX_VALUES), ("text", ctypes.c_char * 256)]
 
     def as_dict(self):
-        return dict(op=self.op, kind=self.kind, line=self.line, targets=list(self.targets[:self.num_targets]),
+        return dict(op=self.op, kind=self.kind, line=self.line, circuit=self.circuit,
+                    targets=list(self.targets[:self.num_targets]),
                     controls=list(self.controls[:self.num_controls]), params=list(self.params),
                     ints=list(self.ints), values=list(self.values[:min(self.num_values, MAX_VALUES)]),
                     text=self.text.decode())
@@ -48,13 +49,14 @@ def _lib():
         L.rbk_qcx_parse.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(P)]
         L.rbk_qcx_destroy.argtypes = [P]
         L.rbk_qcx_num_qubits.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
+        L.rbk_qcx_num_circuits.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         L.rbk_qcx_initial_state.argtypes = [P, ctypes.POINTER(ctypes.c_uint64)]
         L.rbk_qcx_num_instructions.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
         L.rbk_qcx_get_instruction.argtypes = [P, ctypes.c_int, ctypes.POINTER(Instruction)]
         L.rbk_qcx_run.argtypes = [P, ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(P)]
         L.rbk_qcx_free_text.argtypes = [ctypes.c_void_p]
         L.rbk_qcx_free_text.restype = None
-        for f in ("rbk_qcx_parse", "rbk_qcx_destroy", "rbk_qcx_num_qubits", "rbk_qcx_initial_state",
+        for f in ("rbk_qcx_parse", "rbk_qcx_destroy", "rbk_qcx_num_qubits", "rbk_qcx_num_circuits", "rbk_qcx_initial_state",
                   "rbk_qcx_num_instructions", "rbk_qcx_get_instruction", "rbk_qcx_run"):
             getattr(L, f).restype = ctypes.c_int
         _bound = True
@@ -94,6 +96,12 @@ class Program:
         return v.value
 
     @property
+    def num_circuits(self):
+        v = ctypes.c_int()
+        _check(_lib().rbk_qcx_num_circuits(self.h, ctypes.byref(v)))
+        return v.value
+
+    @property
     def initial_state(self):
         v = ctypes.c_uint64()
         _check(_lib().rbk_qcx_initial_state(self.h, ctypes.byref(v)))
@@ -111,7 +119,7 @@ class Program:
         return out
 
     def run(self, precision=rbk.C128, seed=1, deferred=True, timing=False, device=0, keep_state=False):
-        """Returns (bra's output text, final State or None)."""
+        """Returns (bra's output text, circuit 0's final State or None)."""
         L = _lib()
         opt = Options()
         L.rbk_qcx_default_options(ctypes.byref(opt))

@@ -84,6 +84,8 @@ _SIGNATURES = {
     "rbk_expectation_pauli": ([_P, _I, ctypes.c_char_p, _P, _P], _I),
     "rbk_inner_product": ([_P, _P, _P], _I),
     "rbk_fidelity": ([_P, _P, ctypes.POINTER(_D)], _I),
+    "rbk_inner_product_pauli": ([_P, _P, _I, ctypes.c_char_p, _P, _P], _I),
+    "rbk_fidelity_pauli": ([_P, _P, _I, ctypes.c_char_p, _P, ctypes.POINTER(_D)], _I),
     "rbk_x_rotation_half_pi": ([_P, _I, _U32, _U32P, _I], _I),
     "rbk_y_rotation_half_pi": ([_P, _I, _U32, _U32P, _I], _I),
     "rbk_sqrt_pauli_x": ([_P, _I, _U32, _U32P, _I], _I),
@@ -423,6 +425,22 @@ class State:
     def fidelity(self, other):
         v = ctypes.c_double()
         _check(lib().rbk_fidelity(self.h, other.h, ctypes.byref(v)))
+        return v.value
+
+    def inner_product_pauli(self, other, terms):
+        """<other| H |self> for H = sum of (string, coeff) terms (strings over all qubits)."""
+        strings = b"".join(s.encode() for s, _ in terms)
+        coeffs = np.array([[complex(c).real, complex(c).imag] for _, c in terms], dtype=np.float64).ravel()
+        out = np.empty(2, dtype=np.float64)
+        _check(lib().rbk_inner_product_pauli(self.h, other.h, len(terms), strings, coeffs.ctypes.data, out.ctypes.data))
+        return complex(out[0], out[1])
+
+    def fidelity_pauli(self, other, terms):
+        """|<other| H |self>|^2."""
+        strings = b"".join(s.encode() for s, _ in terms)
+        coeffs = np.array([[complex(c).real, complex(c).imag] for _, c in terms], dtype=np.float64).ravel()
+        v = ctypes.c_double()
+        _check(lib().rbk_fidelity_pauli(self.h, other.h, len(terms), strings, coeffs.ctypes.data, ctypes.byref(v)))
         return v.value
 
     # -- sampling and measurement ------------------------------------------------

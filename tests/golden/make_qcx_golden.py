@@ -185,6 +185,56 @@ def bigger_mixed(n=15, seed=7):
     return "\n".join(L) + "\n"
 
 
+def circuits_overlaps(n=9, seed=8):
+    """Three circuits (CIRCUITS 3): pairwise and ALL inner products and fidelities,
+    with and without a Pauli operator, a measurement with circuit 2's own seed."""
+    rng = np.random.default_rng(seed)
+
+    def layer(L, k):
+        for q in range(n):
+            L.append("U3 %d %s %s %s" % (q, a(rng), a(rng), a(rng)))
+        for q in range(k % 2, n - 1, 2):
+            L.append("CNOT %d %d" % (q, q + 1))
+
+    L = ["! several circuits and their overlaps", "CIRCUITS 3", "QUBITS %d" % n]
+    L += ["H %d" % q for q in range(n)]
+    layer(L, 0)
+    L += ["INNERPROD 1", "PRINTLN :RESULT", "INNERPROD 0", "FIDELITY ALL", "PRINTLN :RESULT",
+          "INNERPROD 2 :PAULIS:XZY 0 4 8", "PRINTLN :RESULT", "FIDELITY ALL :PAULIS:ZZ 1 2", "PRINTLN :RESULT"]
+    L += ["BEGIN CIRCUIT 1"] + ["H %d" % q for q in range(n)]
+    layer(L, 1)
+    L += ["DO MEASUREMENT 4", "INNERPROD 0", "PRINTLN :RESULT", "FIDELITY ALL", "PRINTLN :RESULT",
+          "FIDELITY ALL :PAULIS:ZZ 1 2", "PRINTLN :RESULT", "END CIRCUIT"]
+    L += ["BEGIN CIRCUIT 2"] + ["H %d" % q for q in range(0, n, 2)]
+    layer(L, 0)
+    layer(L, 1)
+    L += ["M 3", "PRINTLN :OUTCOME", "FIDELITY ALL", "PRINTLN :RESULT", "INNERPROD 0 :PAULIS:XZY 0 4 8",
+          "PRINTLN :RESULT", "FIDELITY ALL :PAULIS:ZZ 1 2", "PRINTLN :RESULT", "DO AMPLITUDES 0 5 77", "END CIRCUIT"]
+    return "\n".join(L) + "\n"
+
+
+def circuits_tiles(n=14, seed=9):
+    """Two 14-qubit circuits (tile passes, fusion blocks) compared by FIDELITY and INNERPROD."""
+    rng = np.random.default_rng(seed)
+    L = ["CIRCUITS 2", "QUBITS %d" % n]
+    for k in (0, 1):
+        if k:
+            L.append("BEGIN CIRCUIT 1")
+        L += ["H %d" % q for q in range(n)]
+        for layer in range(3):
+            L.append("BEGIN FUSION")
+            for q in range(n):
+                L.append("U3 %d %s %s %s" % (q, a(rng), a(rng), a(rng)))
+            L.append("END FUSION")
+            for q in range(layer % 2, n - 1, 2):
+                L.append("CNOT %d %d" % (q, q + 1))
+        L += ["FIDELITY %d" % (1 - k), "PRINTLN :RESULT", "INNERPROD ALL :PAULIS:XYZX 0 3 9 13", "PRINTLN :RESULT",
+              "INNERPROD %d" % k, "DO MEASUREMENT 6"]
+        if k:
+            L.append("END CIRCUIT")
+    return "\n".join(L) + "\n"
+
+
 PROGRAMS = {
     "every_gate": every_gate,
     "fused_brick": fused_brick,
@@ -194,6 +244,8 @@ PROGRAMS = {
     "shor_program": shor_program,
     "rotations_adder": rotations_adder,
     "bigger_mixed": bigger_mixed,
+    "circuits_overlaps": circuits_overlaps,
+    "circuits_tiles": circuits_tiles,
     "hadamards8": lambda: "QUBITS 8\n" + "".join("H %d\n" % q for q in range(8)) + "DO MEASUREMENT\n",
 }
 

@@ -45,8 +45,11 @@ def same_output(got, want):
         wt = re.split(r"([\s(),]+)", w)
         assert len(gt) == len(wt), (g, w)
         for a, b in zip(gt, wt):
-            if NUM.match(b) and NUM.match(a) and not re.match(r"^[01]+$", b):
-                assert abs(float(a) - float(b)) <= max(1e-12, 1.01 * last_digit(b)), (g, w)
+            if NUM.match(b) and NUM.match(a):
+                if re.match(r"^[-+]?\d+$", b):  # integers (indices, bit strings, outcomes, a zero): equal values
+                    assert (a == b) if len(b) > 1 and set(b) <= {"0", "1"} else float(a) == float(b), (g, w)
+                else:
+                    assert abs(float(a) - float(b)) <= max(1e-12, 1.01 * last_digit(b)), (g, w)
             elif a.strip() != b.strip():
                 assert a == b, (g, w)
 
@@ -112,3 +115,56 @@ def test_seed_option_changes_the_state_generator(pkg):
     b, _ = pkg.qcx.run(text, seed=2)
     c, _ = pkg.qcx.run(text, seed=1)
     assert a == c and a != b
+
+
+def test_waits_that_never_resolve_are_an_error(pkg):
+    """bra's scheduler would loop forever here (circuit 1 finishes without the
+    INNERPROD circuit 0 waits for); the engine reports it instead."""
+    text = "CIRCUITS 2\nQUBITS 3\nH 0\nINNERPROD 1\nBEGIN CIRCUIT 1\nH 1\nEND CIRCUIT\n"
+    with pytest.raises(pkg.RbkError) as e:
+        pkg.qcx.run(text)
+    assert e.value.code == 6
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("n", [5, 12, 17])
+def test_inner_product_pauli_vs_reference(pkg, n, precision):
+    """<b| P |a> through rbk_inner_product_pauli against ket::runtime::ranges::inner_product
+    with bra's observable (oracle KetRef.inner_product_on); sums of terms by linearity."""
+    import oracle
+    rng = np.random.default_rng(n + 10 * precision)
+    va = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    vb = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    va /= np.linalg.norm(va)
+    vb /= np.linalg.norm(vb)
+    ra, rb = oracle.KetRef(n), oracle.KetRef(n)
+    ra.set_amplitudes(va)
+    rb.set_amplitudes(vb)
+    a, b = pkg.State(n, precision), pkg.State(n, precision)
+    a.upload(va)
+    b.upload(vb)
+    # queued gates on both (a SWAP relabels a's layout only) before the overlap
+    a.apply([("H", (1,), ()), ("SWAP", (0, n - 1), ()), ("CNOT", (2, 3), ())])
+    b.apply([("U3", (n - 2,), (0.3, 0.7, -1.1))])
+    ra.apply([("H", (1,), ()), ("SWAP", (0, n - 1), ()), ("CNOT", (2, 3), ())])
+    rb.apply([("U3", (n - 2,), (0.3, 0.7, -1.1))])
+    tol = 1e-12 if precision == 0 else 1e-5
+    total_ref, terms = 0j, []
+    for k in range(4):
+        m = int(rng.integers(1, min(n, 6) + 1))
+        qubits = [int(q) for q in rng.choice(n, size=m, replace=False)]
+        pauli = "".join(rng.choice(list("IXYZ"), size=m))
+        want = ra.inner_product_on(rb, pauli, qubits)
+        full = ["I"] * n
+        for q, ch in zip(qubits, pauli):
+            full[q] = ch
+        full = "".join(full)
+        got = a.inner_product_pauli(b, [(full, 1.0)])
+        assert abs(got - want) <= tol, (pauli, qubits)
+        assert abs(a.fidelity_pauli(b, [(full, 1.0)]) - abs(want) ** 2) <= tol
+        c = complex(rng.standard_normal(), rng.standard_normal())
+        terms.append((full, c))
+        total_ref += c * want
+    assert abs(a.inner_product_pauli(b, terms) - total_ref) <= 4 * tol
+    a.close()
+    b.close()

@@ -16,7 +16,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 PROGRAMS = sorted(glob.glob(os.path.join(GOLDEN, "qcx", "*.qcx")))
 REF_BUILT = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libketref.so"))
 REF_SAMPLES = "/root/reference/bra/qcx"
-FIELDS = ("op", "kind", "line", "targets", "controls", "params", "text")
+FIELDS = ("op", "kind", "line", "circuit", "targets", "controls", "params", "text")
 
 
 def same_program(cpp, py):
@@ -26,14 +26,16 @@ def same_program(cpp, py):
             assert a[k] == b[k], (k, a, b)
         if a["op"] == bra_ref.OP["AMPLITUDES"]:
             assert a["values"] == b["values"][:40]
+        if a["op"] in (bra_ref.OP["INNERPROD"], bra_ref.OP["FIDELITY"]):
+            assert a["ints"][0] == b["ints"][0]
 
 
 @pytest.mark.parametrize("path", PROGRAMS, ids=os.path.basename)
 def test_cpp_parser_equals_python_restatement(pkg, path):
     text = open(path).read()
     prog = pkg.qcx.parse(text)
-    n, init, code = bra_ref.parse(text)
-    assert prog.num_qubits == n and prog.initial_state == init
+    n, init, code, circuits = bra_ref.parse_program(text)
+    assert prog.num_qubits == n and prog.initial_state == init and prog.num_circuits == circuits
     same_program(prog.instructions(), code)
 
 
@@ -58,8 +60,12 @@ def test_every_gate_program_covers_the_gate_set(pkg):
     ("H 0\n", 1, "line 1"),
     ("QUBITS 3\nU3 0 1.0 2.0 x\n", 5, "line 2"),
     ("QUBITS 3\nVAR A INT\n", 5, "line 2"),
-    ("CIRCUITS 2\nQUBITS 3\n", 5, "line 1"),
-    ("QUBITS 3\nINNERPROD 0\n", 5, "line 2"),
+    ("CIRCUITS 2\nQUBITS 3\nBEGIN CIRCUIT 2\n", 1, "line 3"),
+    ("CIRCUITS 2\nQUBITS 3\nBEGIN CIRCUIT 1\nBEGIN CIRCUIT 0\n", 1, "line 4"),
+    ("QUBITS 3\nEND CIRCUIT\n", 1, "line 2"),
+    ("QUBITS 3\nINNERPROD 1\n", 1, "line 2"),
+    ("CIRCUITS 2\nQUBITS 3\nFIDELITY 1 :PAULIS:ZZ 0\n", 1, "line 3"),
+    ("CIRCUITS 2\nQUBITS 3\nINNERPROD ALL H 0 1\n", 5, "line 3"),
     ("QUBITS 3\nDEPOLARIZING CHANNEL P_X=0.1\n", 5, "line 2"),
     ("QUBITS 3\nEXPECTATION :PAULIS:ZZ 0\n", 1, "line 2"),
     ("", 1, "QUBITS"),
@@ -77,6 +83,18 @@ def test_comments_case_and_stops(pkg):
     assert ins[1]["controls"] == [0] and ins[1]["targets"] == [1]
     ins = pkg.qcx.parse("QUBITS 3\nGENERATE EVENTS 5 -1\nH 0\n").instructions()
     assert len(ins) == 1 and ins[0]["ints"] == [5, -1]
+
+
+def test_circuit_blocks_and_partners(pkg):
+    text = ("CIRCUITS 3\nQUBITS 4\nH 0\nINNERPROD 0\nBEGIN CIRCUIT 2\nX 1\nFIDELITY ALL\nINNERPROD 2\n"
+            "INNERPROD 0 :PAULIS:XZ 3 1\nEND CIRCUIT\nINNERPROD foo\nFIDELITY 2\n")
+    prog = pkg.qcx.parse(text)
+    ins = prog.instructions()
+    assert prog.num_circuits == 3
+    assert [i["circuit"] for i in ins] == [0, 0, 2, 2, 2, 2, 0, 0]
+    # own index and a column that is neither a number nor ALL: nothing to wait for
+    assert [i["ints"][0] for i in ins if i["op"] in (12, 13)] == [-2, -1, -2, 0, -2, 2]
+    assert ins[5]["text"] == "XZ" and ins[5]["targets"] == [3, 1]
 
 
 def test_run_without_gpu_is_a_cuda_error(pkg):
