@@ -188,10 +188,12 @@ def dist_setup():
 
 
 def dist_max(dist, value, local):
+    """The maximum over ranks (NCCL reduces on the rank's GPU; gloo on the host)."""
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    device = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -199,8 +201,11 @@ def dist_max(dist, value, local):
 def barrier(dist, local):
     if dist is not None:
         import torch
-        dist.barrier(device_ids=[local])
-        torch.cuda.synchronize(local)
+        if dist.get_backend() == "nccl":
+            dist.barrier(device_ids=[local])
+            torch.cuda.synchronize(local)
+        else:
+            dist.barrier()
 
 
 def run_gpu(args):

@@ -233,3 +233,28 @@ def test_engine_shards_exchange_on_one_gpu(pkg, precision):
         assert np.abs(got.astype(np.complex128) - ref.amplitudes()).max() <= tol
         assert abs(norm2 - 1.0) <= (1e-12 if precision == 0 else 1e-4)
         assert exchanges > 0
+
+
+def _bench_rank(rank, world, port):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch.distributed as dist
+
+    import bench
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        bench.barrier(dist, 0)
+        assert bench.dist_max(dist, 1.5 * (rank + 1), 0) == 1.5 * world
+        bench.barrier(dist, 0)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_timing_is_the_max_over_gloo_ranks():
+    """bench.py's N > 1 plumbing (barrier, max over ranks) on 2 gloo ranks."""
+    import torch.multiprocessing as mp
+
+    mp.spawn(_bench_rank, args=(2, free_port()), nprocs=2, join=True)
