@@ -95,6 +95,22 @@ struct alignas(8) dev_op {
   double m[8];        // MAT: m00 m01 m10 m11 as (re, im); DIAG: d0 d1
 };
 
+// A CNOT/X folded into the write map of a phase whose control outside the tile
+// makes it hold on some tiles only: where (base & cout) == cout the write
+// position of register slot i of thread t moves by x when the fold's control
+// holds -- always (kind 0), register bit `bit` of i (kind 1), or bit `bit` of t
+// (kind 2).  x is a shared-memory slot, or a physical offset when the phase
+// stores straight to HBM.  Folds with controls inside the tile only are
+// composed into wslot / wtslot (or the store layout) on the host.
+constexpr int kMaxFolds = 8;
+struct dev_fold {
+  uint64_t cout;
+  uint64_t x;
+  uint8_t kind;
+  uint8_t bit;
+  uint8_t pad[6];
+};
+
 // One register layout of the tile.  Tile index j of the amplitude held in
 // register slot i of thread t:  j = sum_b bit_b(i) << reg_pos[b]  |  sum_b bit_b(t) << thr_pos[b].
 // After the phase's gates the registers are written back at positions given by
@@ -102,8 +118,10 @@ struct alignas(8) dev_op {
 // where they carry the pass's relabelling of tile bits).  The host also
 // precomputes the shared-memory slots of these positions: rslot[b] for
 // register bit b, and tslot_lo[t & 15] ^ tslot_hi[t >> 4] for thread t (up to
-// 9 thread bits; the
-// slot map is linear, so a thread XORs them together).
+// 9 thread bits; the slot map is linear, so a thread XORs them together).
+// CNOTs and X gates at the end of a phase need not run: the host composes them
+// into the write slots (they permute tile indices GF(2)-affinely), and folds[]
+// holds those that apply on some tiles only.
 struct dev_phase {
   uint16_t rslot[8];
   uint16_t wslot[8];
@@ -114,10 +132,14 @@ struct dev_phase {
   uint8_t wreg_pos[8];
   uint8_t wthr_pos[16];
   uint16_t op_begin, op_end;
+  uint8_t num_folds;
+  uint8_t pad[3];
+  dev_fold folds[kMaxFolds];
 };
 
 // Physical offsets of a register layout for direct HBM access: register bit b
-// adds rphys[b]; thread t adds tphys_lo[t & 15] | tphys_hi[t >> 4].
+// contributes rphys[b], thread t tphys_lo[t & 15] ^ tphys_hi[t >> 4], all
+// combined with XOR (folded CNOTs can make contributions share bits).
 struct dev_hbm_layout {
   uint64_t rphys[8];
   uint64_t tphys_lo[16], tphys_hi[32];

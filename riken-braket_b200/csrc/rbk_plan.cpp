@@ -189,6 +189,84 @@ std::vector<phase_build> phases_by_dag(const std::vector<pop>& ops, const int* t
   return phases;
 }
 
+// CNOT / X gates at the end of a phase permute the tile's indices GF(2)-affinely:
+// instead of running them, the write-back layout absorbs them.  A gate X_t
+// controlled by one bit c (a register bit, a warp-uniform thread bit, or none)
+// moves the value of register slot i of thread tid by W(e_t) -- the write
+// position of register bit t -- where c holds: register control c adds W(e_t)
+// to wslot[c], a thread control adds it to the thread tables' entries with
+// that bit, no control adds it to every thread.  Gates that also have controls
+// outside the tile hold on some tiles only and go to dp.folds for the kernel.
+// A gate folds when no later kept op of the phase touches its target or acts
+// non-diagonally on its control, and no later folded gate is controlled by its
+// target (so every folded gate reads its control before any fold moved it and
+// their contributions add up).  direct_store: the phase stores straight to HBM
+// and the contributions are physical offsets (store layout); for complex<float>
+// the 16-byte pair (register bit 0) must then stay out of the folds.
+void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_end, bool direct_store)
+{
+  const int begin = dp.op_begin, count = op_end - begin;
+  std::vector<char> folded(static_cast<size_t>(count), 0);
+  uint32_t later_target = 0, later_diag = 0, later_fold_ctl = 0;
+  int conditional = 0;
+  for (int k = op_end - 1; k >= begin; --k) {
+    const dev_op& d = out.ops[k];
+    bool ok = d.kind == OPK_X;
+    if (ok) {
+      const uint32_t t = 1u << d.treg;
+      const int nctl = __builtin_popcount(d.creg) + __builtin_popcount(d.cthr);
+      ok = nctl <= 1 && (d.cthr == 0 || __builtin_ctz(d.cthr) >= 5) &&
+           !((later_target | later_diag | later_fold_ctl) & t) && !(later_target & d.creg);
+      if (ok && direct_store && p.vbits) ok = d.treg != 0 && !(d.creg & 1u);
+      if (ok && d.cout) ok = conditional < kMaxFolds;
+    }
+    if (ok) {
+      folded[static_cast<size_t>(k - begin)] = 1;
+      later_fold_ctl |= d.creg;
+      if (d.cout) ++conditional;
+      continue;
+    }
+    if (is_target_kind(d.kind)) later_target |= 1u << d.treg;
+    later_diag |= d.creg | d.dreg;
+  }
+  // Contributions use the unfolded write positions of the target bits.
+  uint16_t wslot0[8];
+  uint64_t rphys0[8];
+  std::memcpy(wslot0, dp.wslot, sizeof(wslot0));
+  std::memcpy(rphys0, out.store.rphys, sizeof(rphys0));
+  int kept = begin;
+  for (int k = begin; k < op_end; ++k) {
+    const dev_op d = out.ops[k];
+    if (!folded[static_cast<size_t>(k - begin)]) {
+      out.ops[kept++] = d;
+      continue;
+    }
+    const uint64_t x = direct_store ? rphys0[d.treg] : wslot0[d.treg];
+    const uint8_t kind = d.creg ? 1 : d.cthr ? 2 : 0;
+    const uint8_t bitpos = static_cast<uint8_t>(d.creg ? __builtin_ctz(d.creg) : d.cthr ? __builtin_ctz(d.cthr) : 0);
+    if (d.cout) {
+      dev_fold& f = dp.folds[dp.num_folds++];
+      f.cout = d.cout;
+      f.x = x;
+      f.kind = kind;
+      f.bit = bitpos;
+      continue;
+    }
+    if (direct_store) {
+      if (kind == 0) for (int e = 0; e < 16; ++e) out.store.tphys_lo[e] ^= x;
+      else if (kind == 1) out.store.rphys[bitpos] ^= x;
+      else for (int e = 0; e < 32; ++e) if ((e >> (bitpos - 4)) & 1) out.store.tphys_hi[e] ^= x;
+    } else {
+      const uint16_t xs = static_cast<uint16_t>(x);
+      if (kind == 0) for (int e = 0; e < 16; ++e) dp.wtslot_lo[e] ^= xs;
+      else if (kind == 1) dp.wslot[bitpos] ^= xs;
+      else for (int e = 0; e < 32; ++e) if ((e >> (bitpos - 4)) & 1) dp.wtslot_hi[e] ^= xs;
+    }
+  }
+  for (int k = kept; k < op_end; ++k) out.ops[k] = dev_op{};
+  op_end = kept;
+}
+
 void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>& ops,
                 const int* relabel_to, const int* tile_phys, dev_pass& out)
 {
@@ -331,6 +409,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     for (int oi : pb.ops) {
       const pop& o = ops[oi];
       dev_op& d = out.ops[op_index++];
+      d = dev_op{};  // the slot may hold an op of an earlier phase that folding removed
       d.kind = o.kind;
       d.diag_one = o.diag_one;
       std::memcpy(d.m, o.m, sizeof(d.m));
@@ -363,6 +442,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
              : (d.kind == OPK_X || d.kind == OPK_Y) ? op_code(d.kind, 0, true, d.treg)
              : op_code(d.kind, 0, true, 0);
     }
+    if (p.fold_x) fold_trailing_x(p, out, dp, op_index, last && ds);
     dp.op_end = static_cast<uint16_t>(op_index);
   }
   out.num_phases = static_cast<uint8_t>(phases.size());

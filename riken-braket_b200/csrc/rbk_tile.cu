@@ -262,6 +262,27 @@ __device__ __forceinline__ uint64_t tile_base(const dev_pass& P, uint64_t b)
   return base;
 }
 
+// The folded CNOTs of a phase that hold on some tiles only (controls outside
+// the tile): move the write positions of this tile's registers (dev_fold).
+template <int R, typename W>
+__device__ __forceinline__ void apply_folds(const dev_phase& ph, uint64_t base, uint32_t tid, W& thr, W (&reg)[R])
+{
+  const int nf = ph.num_folds;
+  for (int f = 0; f < nf; ++f) {
+    const dev_fold& F = ph.folds[f];
+    if ((base & F.cout) != F.cout) continue;  // the same for the whole CTA
+    const W x = static_cast<W>(F.x);
+    if (F.kind == 0) {
+      thr ^= x;
+    } else if (F.kind == 2) {
+      if ((tid >> F.bit) & 1u) thr ^= x;  // a warp bit: uniform within the warp
+    } else {
+#pragma unroll
+      for (int b = 0; b < R; ++b) reg[b] ^= (b == F.bit) ? x : W(0);
+    }
+  }
+}
+
 // One tile through the pass's phases, ending with the tile stored to HBM.
 // from_hbm: phase 0 loads its registers straight from HBM (the pass's direct
 // load); otherwise the tile is already in `tile` and visible to every thread.
@@ -314,23 +335,27 @@ __device__ __forceinline__ void tile_phases(typename ctype<Real>::c* __restrict_
       // CTA must have read its amplitudes before any warp overwrites the tile
       // in its relabelled order.
       if (p == 0 && from_hbm) __syncthreads();
-      const uint64_t tphys = base | P.store.tphys_lo[tid & 15] | P.store.tphys_hi[tid >> 4];
+      // base holds only bits outside the tile, the tables only tile bits;
+      // folded CNOTs make table contributions overlap, hence XOR.
+      uint64_t tphys = base ^ P.store.tphys_lo[tid & 15] ^ P.store.tphys_hi[tid >> 4];
       uint64_t rphys[R];
 #pragma unroll
       for (int b = 0; b < R; ++b) rphys[b] = P.store.rphys[b];
+      apply_folds<R>(ph, base, tid, tphys, rphys);
 #pragma unroll
       for (int i = 0; i < NR; i += VEC) {
         uint64_t phys = tphys;
 #pragma unroll
-        for (int b = VB; b < R; ++b) if (i & (1 << b)) phys |= rphys[b];
+        for (int b = VB; b < R; ++b) if (i & (1 << b)) phys ^= rphys[b];
         __stcs(gdst + (phys >> VB), vec_io<Real>::pack(&a[i]));
       }
     } else {
       __syncthreads();  // every thread has read this phase's layout
-      const uint32_t ts = ph.wtslot_lo[tid & 15] ^ ph.wtslot_hi[tid >> 4];
+      uint32_t ts = ph.wtslot_lo[tid & 15] ^ ph.wtslot_hi[tid >> 4];
       uint32_t rs[R];
 #pragma unroll
       for (int b = 0; b < R; ++b) rs[b] = ph.wslot[b];
+      apply_folds<R>(ph, base, tid, ts, rs);
 #pragma unroll
       for (int i = 0; i < NR; ++i) {
         uint32_t sidx = ts;

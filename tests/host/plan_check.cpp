@@ -52,6 +52,20 @@ static uint32_t slot_of(uint32_t j, int vbits)
   return (u << vbits) | (j & ((1u << vbits) - 1));
 }
 
+// The kernel's apply_folds: folded CNOTs that hold on this tile move write positions.
+static void apply_folds(const dev_phase& D, uint64_t base, int tid, int R, uint64_t& thr, uint64_t* reg)
+{
+  if (D.num_folds > kMaxFolds) { std::fprintf(stderr, "too many folds\n"); std::exit(11); }
+  for (int f = 0; f < D.num_folds; ++f) {
+    const dev_fold& F = D.folds[f];
+    if ((base & F.cout) != F.cout) continue;
+    if (F.kind == 0) thr ^= F.x;
+    else if (F.kind == 2) { if (F.bit < 5) { std::fprintf(stderr, "fold on a lane bit\n"); std::exit(12); } if ((tid >> F.bit) & 1) thr ^= F.x; }
+    else if (F.bit < R) reg[F.bit] ^= F.x;
+    else { std::fprintf(stderr, "bad fold register\n"); std::exit(13); }
+  }
+}
+
 // Model of tile_pass_kernel for one pass: shared memory is indexed by slot and
 // every address comes from the precomputed tables, as in the kernel.  Each
 // phase completes all threads' reads before any write, which is what the
@@ -144,19 +158,25 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
       for (int tid = 0; tid < NT; ++tid) {
         const cplx* a = &regs[size_t(tid) * NR];
         if (last && P.direct_store) {
-          const uint64_t tp = base | P.store.tphys_lo[tid & 15] | P.store.tphys_hi[tid >> 4];
+          uint64_t tp = base ^ P.store.tphys_lo[tid & 15] ^ P.store.tphys_hi[tid >> 4];
+          uint64_t rp[8];
+          for (int x = 0; x < R; ++x) rp[x] = P.store.rphys[x];
+          apply_folds(D, base, tid, R, tp, rp);
           for (int i = 0; i < NR; ++i) {
             uint64_t phys = tp;
-            for (int x = 0; x < R; ++x) if (i & (1 << x)) phys |= P.store.rphys[x];
+            for (int x = 0; x < R; ++x) if (i & (1 << x)) phys ^= rp[x];
             if (!stored.insert(phys).second) { std::fprintf(stderr, "direct store writes an amplitude twice\n"); std::exit(5); }
             st[in_state(phys)] = a[i];
           }
           continue;
         }
-        const uint32_t ts = D.wtslot_lo[tid & 15] ^ D.wtslot_hi[tid >> 4];
+        uint64_t ts = D.wtslot_lo[tid & 15] ^ D.wtslot_hi[tid >> 4];
+        uint64_t rs[8];
+        for (int x = 0; x < R; ++x) rs[x] = D.wslot[x];
+        apply_folds(D, base, tid, R, ts, rs);
         for (int i = 0; i < NR; ++i) {
-          uint32_t sidx = ts;
-          for (int x = 0; x < R; ++x) if (i & (1 << x)) sidx ^= D.wslot[x];
+          uint32_t sidx = static_cast<uint32_t>(ts);
+          for (int x = 0; x < R; ++x) if (i & (1 << x)) sidx ^= static_cast<uint32_t>(rs[x]);
           if (sidx >= (1u << K) || written[sidx]) { std::fprintf(stderr, "bad write position\n"); std::exit(3); }
           written[sidx] = 1;
           smem[sidx] = a[i];
