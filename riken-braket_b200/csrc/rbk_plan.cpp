@@ -448,6 +448,59 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
   out.num_phases = static_cast<uint8_t>(phases.size());
 }
 
+// Single-qubit gates without controls as 2x2 matrices (row-major, re/im pairs).
+bool single_qubit_matrix(const pop& o, double* m)
+{
+  std::memset(m, 0, 8 * sizeof(double));
+  if (o.kind == OPK_MAT && o.cmask == 0) { std::memcpy(m, o.m, 8 * sizeof(double)); return true; }
+  if (o.kind == OPK_X && o.cmask == 0) { m[2] = 1; m[4] = 1; return true; }
+  if (o.kind == OPK_Y && o.cmask == 0) { m[3] = -1; m[5] = 1; return true; }
+  if (o.kind == OPK_DIAG && o.cmask == 0) { m[0] = o.m[0]; m[1] = o.m[1]; m[6] = o.m[2]; m[7] = o.m[3]; return true; }
+  return false;
+}
+
+bool touches(const pop& o, int q)
+{
+  return o.target == q || ((o.cmask >> q) & 1);
+}
+
+// Merges an uncontrolled single-qubit gate into the last op of the pass that
+// touches its qubit when that op is an uncontrolled single-qubit gate too and
+// one of the two is non-diagonal (so the qubit is a tile bit): the ops between
+// them act on other qubits, so the new gate can move back to it and the two
+// become one 2x2 matrix (later gate times earlier).  allow_dense: the merge may
+// turn two sparse gates (X, Y, diagonal) into a dense one.
+bool merge_single_qubit(std::vector<pop>& ops, const pop& o, bool allow_dense)
+{
+  double b[8];
+  if (o.target < 0 || !single_qubit_matrix(o, b)) return false;
+  for (size_t j = ops.size(); j-- > 0;) {
+    if (!touches(ops[j], o.target)) continue;
+    double a[8];
+    if (ops[j].target != o.target || !single_qubit_matrix(ops[j], a)) return false;
+    if (!is_target_kind(ops[j].kind) && !is_target_kind(o.kind)) return false;
+    if (ops[j].kind != OPK_MAT && o.kind != OPK_MAT && !allow_dense) return false;
+    double c[8];
+    for (int r = 0; r < 2; ++r)
+      for (int k = 0; k < 2; ++k) {
+        double re = 0, im = 0;
+        for (int l = 0; l < 2; ++l) {
+          const double xr = b[2 * (2 * r + l)], xi = b[2 * (2 * r + l) + 1];
+          const double yr = a[2 * (2 * l + k)], yi = a[2 * (2 * l + k) + 1];
+          re += xr * yr - xi * yi;
+          im += xr * yi + xi * yr;
+        }
+        c[2 * (2 * r + k)] = re;
+        c[2 * (2 * r + k) + 1] = im;
+      }
+    ops[j].kind = OPK_MAT;
+    ops[j].diag_one = 0;
+    std::memcpy(ops[j].m, c, sizeof(c));
+    return true;
+  }
+  return false;
+}
+
 // Tile bit order: physical bits 0..LOW-1 first, then the others ascending.
 void tile_order(const plan_params& p, uint64_t tile_mask, int* tile_phys)
 {
@@ -543,8 +596,18 @@ void plan_passes(const plan_params& p, const std::vector<hgate>& gates, std::vec
       o.target = g.target >= 0 ? perm[g.target] : -1;
       o.cmask = map_mask(g.cmask, perm);
       std::memcpy(o.m, g.m, sizeof(o.m));
-      ops.push_back(o);
       taken[i] = 1;
+      if (p.merge_1q) {
+        // the merged op is dense; it adds to the pass's dense count unless the op it replaces was dense
+        bool was_dense = false;
+        for (size_t j = ops.size(); j-- > 0;)
+          if (touches(ops[j], o.target)) { was_dense = ops[j].kind == OPK_MAT; break; }
+        if (merge_single_qubit(ops, o, dense < budget)) {
+          dense += was_dense ? 0 : 1;
+          continue;
+        }
+      }
+      ops.push_back(o);
       dense += is_dense(g) ? 1 : 0;
     }
     if (ops.empty()) continue;  // only swaps were taken: layout map updated, no data moved

@@ -31,6 +31,7 @@ struct plan_params {
   int vbits;     // log2 amplitudes per 16-byte vector
   int dense_budget;  // max dense 2x2 gates per pass
   bool fold_x = true;  // fold CNOT / X gates at the end of a phase into its write layout
+  bool merge_1q = true;  // merge consecutive uncontrolled single-qubit gates on one qubit
 };
 
 // Plans `gates` (in order) into passes, updating the layout map
