@@ -891,31 +891,124 @@ int rbk_spin_expectation_values(rbk_state* s, double* out)
   return guarded([&]() -> int {
     if (int rc = check_state(s)) return rc;
     if (!out) return fail(RBK_ERR_INVALID, "null output pointer");
-    // <S_z>: one pass of Z sums over all physical bits.
-    int rc = launch_reduction(s, [&] {
-      return s->precision == RBK_C128 ? rbk::launch_zsum<double>(s->amps, s->n, s->d_partials, s->d_out, s->stream)
-                                      : rbk::launch_zsum<float>(s->amps, s->n, s->d_partials, s->d_out, s->stream);
-    });
-    if (rc) return rc;
-    if ((rc = read_out(s, s->n + 1))) return rc;
-    const double total = s->h_out[0];
-    std::vector<double> ones(s->n);
-    for (int p = 0; p < s->n; ++p) ones[p] = s->h_out[1 + p];
-    for (int q = 0; q < s->n; ++q) {
-      const double one = ones[s->perm[q]];
-      out[3 * q + 2] = 0.5 * ((total - one) - one);
+    if (int rc = flush(s)) return rc;  // the layout map is final only after the queued gates ran
+    const bool c128 = s->precision == RBK_C128;
+    const int n = s->n, RB = rbk::spin_register_bits(c128 ? 0 : 1), KT = 8 + RB;
+    if (n < KT) {
+      // Small states: one Z-sum pass and one pair-sum pass per qubit.
+      int rc = launch_reduction(s, [&] {
+        return c128 ? rbk::launch_zsum<double>(s->amps, n, s->d_partials, s->d_out, s->stream)
+                    : rbk::launch_zsum<float>(s->amps, n, s->d_partials, s->d_out, s->stream);
+      });
+      if (rc) return rc;
+      if ((rc = read_out(s, n + 1))) return rc;
+      const double total = s->h_out[0];
+      std::vector<double> ones(static_cast<size_t>(n));
+      for (int p = 0; p < n; ++p) ones[static_cast<size_t>(p)] = s->h_out[1 + p];
+      for (int q = 0; q < n; ++q) {
+        const double one = ones[static_cast<size_t>(s->perm[q])];
+        out[3 * q + 2] = 0.5 * ((total - one) - one);
+        rbk::pauli_terms t{};
+        t.count = 1;
+        t.w[0][0] = 1.0;
+        t.one_sided = 1;  // <S_x> + i <S_y> = sum over pairs with the qubit clear of conj(a0) a1
+        double r[2];
+        if ((rc = pauli_group(s, 1ull << s->perm[q], t, r))) return rc;
+        out[3 * q + 0] = r[0];
+        out[3 * q + 1] = r[1];
+      }
+      return RBK_OK;
     }
-    // <S_x> + i <S_y> = sum over pairs with the qubit clear of conj(a0) a1.
-    for (int q = 0; q < s->n; ++q) {
-      rbk::pauli_terms t{};
-      t.count = 1;
-      t.w[0][0] = 1.0;
-      t.one_sided = 1;
-      const uint64_t flip = 1ull << s->perm[q];
-      double r[2];
-      if ((rc = pauli_group(s, flip, t, r))) return rc;
-      out[3 * q + 0] = r[0];
-      out[3 * q + 1] = r[1];
+    // Tile layouts of KT bits whose flips cover every physical bit once: the
+    // low KT bits, then the coalescing bits 0..LOW-1 with up to KT - LOW
+    // further bits (filled up with other bits when fewer remain).  Each layout
+    // is one read of the state (spins_kernel) for all its flips.
+    const int LOW = c128 ? rbk::precision_traits<double>::LOW : rbk::precision_traits<float>::LOW;
+    std::vector<rbk::spin_group> groups;
+    std::vector<std::vector<int>> group_flips;  // physical bits flipped by each group, in flip order
+    auto add_group = [&](const std::vector<int>& tile_bits, const std::vector<int>& flips_local) {
+      rbk::spin_group g{};
+      g.K = KT;
+      uint64_t mask = 0;
+      for (int b = 0; b < KT; ++b) { g.tile_phys[b] = static_cast<uint8_t>(tile_bits[b]); mask |= 1ull << tile_bits[b]; }
+      g.nflips = static_cast<int>(flips_local.size());
+      g.nphases = (g.nflips + RB - 1) / RB;
+      std::vector<int> phys;
+      for (int p = 0; p < g.nphases; ++p) {
+        std::vector<int> regs;
+        for (int k = 0; k < RB; ++k) {
+          const int f = p * RB + k;
+          if (f < g.nflips) regs.push_back(flips_local[static_cast<size_t>(f)]);
+        }
+        for (int b = 0; static_cast<int>(regs.size()) < RB; ++b)  // fillers: other tile bits
+          if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
+        int nt = 0;
+        for (int b = 0; b < KT; ++b)
+          if (std::find(regs.begin(), regs.end(), b) == regs.end()) g.phase_thr[p][nt++] = static_cast<uint8_t>(b);
+        for (int k = 0; k < RB; ++k) g.phase_reg[p][k] = static_cast<uint8_t>(regs[static_cast<size_t>(k)]);
+      }
+      for (int f : flips_local) phys.push_back(tile_bits[static_cast<size_t>(f)]);
+      int runs = 0, src = 0;
+      for (int q = 0; q < n;) {
+        if ((mask >> q) & 1) { ++q; continue; }
+        int len = 0;
+        while (q + len < n && !((mask >> (q + len)) & 1)) ++len;
+        g.run_src[runs] = static_cast<uint8_t>(src);
+        g.run_len[runs] = static_cast<uint8_t>(len);
+        g.run_dst[runs] = static_cast<uint8_t>(q);
+        ++runs;
+        src += len;
+        q += len;
+      }
+      g.num_runs = runs;
+      groups.push_back(g);
+      group_flips.push_back(phys);
+    };
+    {
+      std::vector<int> bits, flips;
+      for (int b = 0; b < KT; ++b) { bits.push_back(b); flips.push_back(b); }
+      add_group(bits, flips);
+      for (int b = KT; b < n; b += KT - LOW) {
+        std::vector<int> tile_bits, local;
+        for (int l = 0; l < LOW; ++l) tile_bits.push_back(l);
+        for (int c = b; c < std::min(n, b + KT - LOW); ++c) {
+          local.push_back(static_cast<int>(tile_bits.size()));
+          tile_bits.push_back(c);
+        }
+        for (int c = KT - 1; static_cast<int>(tile_bits.size()) < KT; --c) tile_bits.push_back(c);  // fillers
+        std::vector<int> order(tile_bits);  // tile bits ascending keeps the 512-byte runs of the low bits
+        std::sort(order.begin(), order.end());
+        std::vector<int> flips;
+        for (int f : local) flips.push_back(static_cast<int>(std::find(order.begin(), order.end(), tile_bits[static_cast<size_t>(f)]) - order.begin()));
+        add_group(order, flips);
+      }
+    }
+    std::vector<int> slot_of_bit(static_cast<size_t>(n), -1);  // d_out offset of a physical bit's (x, y, z)
+    int width = 0;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      for (int f = 0; f < groups[gi].nflips; ++f) slot_of_bit[static_cast<size_t>(group_flips[gi][static_cast<size_t>(f)])] = width + 3 * f;
+      width += 3 * groups[gi].nflips + 1;
+    }
+    if (width > 4 * (rbk::kMaxQubits + 8)) return fail(RBK_ERR_INVALID, "too many qubits for the spin layouts");
+    for (int q = 0; q < n; ++q)
+      if (slot_of_bit[static_cast<size_t>(q)] < 0) return fail(RBK_ERR_STATE, "spin layouts miss a qubit");
+    int offset = 0;
+    for (const auto& g : groups) {
+      int rc = launch_reduction(s, [&] {
+        return c128 ? rbk::launch_spins<double>(s->amps, n, g, s->d_partials, s->d_out + offset, s->stream)
+                    : rbk::launch_spins<float>(s->amps, n, g, s->d_partials, s->d_out + offset, s->stream);
+      });
+      if (rc) return rc;
+      offset += 3 * g.nflips + 1;
+    }
+    if (int rc = read_out(s, width)) return rc;
+    const double total = s->h_out[3 * groups.front().nflips];  // sum |a|^2 of the first layout
+    for (int q = 0; q < n; ++q) {
+      const int k = slot_of_bit[static_cast<size_t>(s->perm[q])];
+      const double one = s->h_out[k + 2];
+      out[3 * q + 0] = s->h_out[k];      // <S_x> = Re sum conj(a0) a1
+      out[3 * q + 1] = s->h_out[k + 1];  // <S_y> = Im sum conj(a0) a1
+      out[3 * q + 2] = 0.5 * ((total - one) - one);
     }
     return RBK_OK;
   });

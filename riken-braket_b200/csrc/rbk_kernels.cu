@@ -9,6 +9,7 @@
 //                      fixed order (deterministic).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 
@@ -214,6 +215,110 @@ pauli_kernel(const typename ctype<Real>::c* __restrict__ a, int n, uint64_t flip
   block_sum_store<2>(vals, 2, partials + size_t(blockIdx.x) * 2);
 }
 
+// spin_group (rbk_kernels.h): persistent CTAs, one tile at a time, two CTAs
+// per SM (one loads while the other sums).  Element j = it * 256 + tid of a
+// tile sits at shared-memory slot smem_slot(j) (the fused pass's XOR swizzle,
+// linear, so a thread composes slots with XORs and every phase reads without
+// bank conflicts).
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads, 2)
+spins_kernel(const typename ctype<Real>::c* __restrict__ a, const __grid_constant__ spin_group S, uint64_t num_tiles,
+             double* partials)
+{
+  using C = typename ctype<Real>::c;
+  constexpr int VB = precision_traits<Real>::VB;
+  constexpr int RB = sizeof(Real) == 8 ? 3 : 4, NE = 1 << RB;  // 256 threads x NE = 2^(8 + RB) = the tile
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  const uint32_t tid = threadIdx.x;
+  // The thread's parts of addresses, the same for every tile.
+  uint64_t tphys = 0;
+  for (int b = 0; b < 8; ++b) tphys |= uint64_t((tid >> b) & 1u) << S.tile_phys[b];
+  const uint32_t st = smem_slot<VB>(tid);
+  uint32_t sbase[kSpinPhases];
+#pragma unroll
+  for (int p = 0; p < kSpinPhases; ++p) {
+    uint32_t j = 0;
+    if (p < S.nphases)
+      for (int b = 0; b < 8; ++b) j |= ((tid >> b) & 1u) << S.phase_thr[p][b];
+    sbase[p] = smem_slot<VB>(j);
+  }
+  double xr[kMaxSpinFlips], xi[kMaxSpinFlips], z[kMaxSpinFlips];
+#pragma unroll
+  for (int f = 0; f < kMaxSpinFlips; ++f) xr[f] = xi[f] = z[f] = 0.0;
+  double total = 0.0;
+  for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+    uint64_t base = tphys;
+    for (int r = 0; r < S.num_runs; ++r) base |= ((t >> S.run_src[r]) & ((1ull << S.run_len[r]) - 1)) << S.run_dst[r];
+    C v[NE];
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      uint64_t p = base;
+#pragma unroll
+      for (int b = 0; b < RB; ++b)
+        if ((it >> b) & 1) p |= 1ull << S.tile_phys[8 + b];
+      v[it] = __ldcs(a + p);
+    }
+    __syncthreads();  // the previous tile is no longer read
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      tile[st ^ smem_slot<VB>(uint32_t(it) << 8)] = v[it];
+      total += double(v[it].x) * double(v[it].x) + double(v[it].y) * double(v[it].y);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kSpinPhases; ++p) {
+      if (p < S.nphases) {
+        uint32_t rs[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) rs[k] = smem_slot<VB>(1u << S.phase_reg[p][k]);
+        C e[NE];
+#pragma unroll
+        for (int i = 0; i < NE; ++i) {
+          uint32_t sidx = sbase[p];
+#pragma unroll
+          for (int k = 0; k < RB; ++k)
+            if ((i >> k) & 1) sidx ^= rs[k];
+          e[i] = tile[sidx];
+        }
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+          const int f = p * RB + k;
+          if (f < kMaxSpinFlips && f < S.nflips) {
+#pragma unroll
+            for (int i = 0; i < NE; ++i) {
+              if ((i >> k) & 1) continue;
+              const C u = e[i], w = e[i | (1 << k)];
+              xr[f] += double(u.x) * double(w.x) + double(u.y) * double(w.y);
+              xi[f] += double(u.x) * double(w.y) - double(u.y) * double(w.x);
+              z[f] += double(w.x) * double(w.x) + double(w.y) * double(w.y);
+            }
+          }
+        }
+      }
+    }
+  }
+  // Block sums, in a fixed order, of 3 nflips + 1 values.
+  __shared__ double red[kRedThreads / 32][3 * kMaxSpinFlips + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int f = 0; f < kMaxSpinFlips; ++f) {
+    if (f < S.nflips) {
+      const double a0 = warp_sum(xr[f]), a1 = warp_sum(xi[f]), a2 = warp_sum(z[f]);
+      if (lane == 0) { red[warp][3 * f] = a0; red[warp][3 * f + 1] = a1; red[warp][3 * f + 2] = a2; }
+    }
+  }
+  const double tt = warp_sum(total);
+  if (lane == 0) red[warp][3 * S.nflips] = tt;
+  __syncthreads();
+  const int width = 3 * S.nflips + 1;
+  for (int k = threadIdx.x; k < width; k += blockDim.x) {
+    double acc = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) acc += red[w][k];
+    partials[size_t(blockIdx.x) * width + k] = acc;
+  }
+}
+
 // <b| P |a> summed over Pauli strings sharing one flip mask F:
 //   out = sum_i conj(b_i) a_{i^F} W(i),  W(i) = sum_t w_t (-1)^popcount(i & s_t)
 // ((P a)_i = coeff(i) a_{i^F}, ket/include/ket/gate/utility/pauli_index_coeff.hpp:17-59).
@@ -292,6 +397,31 @@ cudaError_t launch_pauli(const void* state, int n, uint64_t flip, const pauli_te
 }
 
 template <typename Real>
+cudaError_t launch_spins(const void* state, int n, const spin_group& g, double* partials, double* out, cudaStream_t stream)
+{
+  const int rb = sizeof(Real) == 8 ? 3 : 4;
+  if (g.K != 8 + rb || g.K > n || g.nflips < 1 || g.nflips > kMaxSpinFlips || g.nphases < 1 ||
+      g.nphases > kSpinPhases || g.nphases * rb < g.nflips)
+    return cudaErrorInvalidValue;
+  const size_t smem = sizeof(typename ctype<Real>::c) << g.K;
+  static std::atomic<bool> configured[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!configured[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(spins_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 << 12);
+    if (e != cudaSuccess) return e;
+    configured[dev].store(true, std::memory_order_release);
+  }
+  const uint64_t tiles = 1ull << (n - g.K);
+  const int blocks = static_cast<int>(std::min<uint64_t>(tiles, 148 * 2));
+  spins_kernel<Real><<<blocks, kRedThreads, smem, stream>>>(static_cast<const typename ctype<Real>::c*>(state), g, tiles, partials);
+  finish_partials_kernel<<<1, 64, 0, stream>>>(partials, blocks, 3 * g.nflips + 1, out);
+  return cudaGetLastError();
+}
+
+template <typename Real>
 cudaError_t launch_pauli2(const void* a, const void* b, int n, uint64_t flip, const pauli_terms& terms, double* partials,
                           double* out, cudaStream_t stream)
 {
@@ -323,6 +453,8 @@ template cudaError_t launch_zsum<double>(const void*, int, double*, double*, cud
 template cudaError_t launch_zsum<float>(const void*, int, double*, double*, cudaStream_t);
 template cudaError_t launch_pauli<double>(const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
 template cudaError_t launch_pauli<float>(const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
+template cudaError_t launch_spins<double>(const void*, int, const spin_group&, double*, double*, cudaStream_t);
+template cudaError_t launch_spins<float>(const void*, int, const spin_group&, double*, double*, cudaStream_t);
 template cudaError_t launch_pauli2<double>(const void*, const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
 template cudaError_t launch_pauli2<float>(const void*, const void*, int, uint64_t, const pauli_terms&, double*, double*, cudaStream_t);
 template cudaError_t launch_inner<double>(const void*, const void*, int, double*, double*, cudaStream_t);

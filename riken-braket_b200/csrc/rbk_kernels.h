@@ -86,6 +86,29 @@ size_t tile_overlaps_partials_doubles(int n, int K);
 template <typename Real> cudaError_t launch_tile_overlaps(const void* lam, const void* psi, int n, const tile_overlap_set& set,
                                                           double* partials, double* out, cudaStream_t stream);
 
+// All spins of the flip bits of one tile layout in one read of the state.
+// Tile t (its bits outside tile_phys spell t, deposited run by run) of 2^K
+// amplitudes, K = 8 + RB (RB = 3 for complex<double>, 4 for complex<float>;
+// 256 threads), is staged in shared memory; for each flip f the CTAs sum
+//   x_f = sum over j with tile bit b_f clear of conj(a_j) a_{j | b_f}   (complex)
+//   z_f = sum over j with tile bit b_f set of |a_j|^2
+// and the total of |a|^2.  The flips are read in register phases: in phase p
+// a thread holds the 2^RB amplitudes whose tile bits phase_reg[p][0..RB-1]
+// vary, at the tile bits phase_thr[p][0..7] that its index gives; flip
+// f = p * RB + k is register bit k of phase p (entries past nflips are fillers).
+// out[3f], out[3f+1] = x_f; out[3f+2] = z_f; out[3 nflips] = total.
+constexpr int kMaxSpinFlips = 12;
+constexpr int kSpinPhases = 4;
+struct spin_group {
+  int K, num_runs, nflips, nphases;
+  uint8_t tile_phys[16], run_src[16], run_len[16], run_dst[16];
+  uint8_t phase_reg[kSpinPhases][4];
+  uint8_t phase_thr[kSpinPhases][8];
+};
+inline int spin_register_bits(int precision) { return precision == 0 ? 3 : 4; }
+template <typename Real> cudaError_t launch_spins(const void* state, int n, const spin_group& g, double* partials, double* out,
+                                                  cudaStream_t stream);
+
 // Sampling: prefix = inclusive scan of |a_i|^2 (scratch: scan_scratch_doubles(count)
 // doubles); events[k] = upper_bound(prefix, r[k]).
 size_t scan_scratch_doubles(uint64_t count);

@@ -242,6 +242,18 @@ def test_c64_path_vs_fp64_oracle(pkg, n):
     assert np.abs(s.spins() - o.spins()).max() <= 1e-5
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("n", [3, 11, 12, 17, 23])
+def test_spins_all_layouts_vs_oracle(pkg, n, precision):
+    """Every qubit's spins from the tiled layouts (one read of the state per
+    layout), after queued SWAPs moved logical qubits around the physical bits."""
+    ops = pkg.circuits.random_circuit(n, 80, seed=n + 3) + [("SWAP", (0, n - 1), ()), ("SWAP", (1, n // 2 + 1), ())]
+    init = random_state(n, n + 7)
+    s, o = run_both(pkg, n, ops, init=init, precision=precision)
+    tol = TOL64 if precision == 0 else 2e-6
+    assert np.abs(s.spins() - o.spins()).max() <= tol
+
+
 def test_errors_are_status_codes(pkg):
     s = pkg.State(14)
     with pytest.raises(pkg.RbkError) as e:
