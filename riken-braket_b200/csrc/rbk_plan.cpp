@@ -150,7 +150,7 @@ std::vector<phase_build> phases_in_order(const std::vector<pop>& ops, const int*
 // the ops in order and takes every op whose predecessors are done and whose
 // target is (or can still join) the phase's register set.  Gates that commute
 // are thereby gathered per register set (a light cone inside the registers).
-std::vector<phase_build> phases_by_dag(const std::vector<pop>& ops, const int* tile_of_phys, int R)
+std::vector<phase_build> phases_by_dag(const std::vector<pop>& ops, const int* tile_of_phys, int R, bool defer_x)
 {
   const int m = static_cast<int>(ops.size());
   std::vector<std::vector<int>> preds(m);
@@ -162,11 +162,17 @@ std::vector<phase_build> phases_by_dag(const std::vector<pop>& ops, const int* t
   std::vector<phase_build> phases;
   while (remaining > 0) {
     phase_build pb;
+    // defer_x: the phase first takes every other ready op, then the ready
+    // CNOT / X gates, and closes -- so that those end the phase and fold into
+    // its write layout (fold_trailing_x); their dependents start the next phase.
+    for (int stage = defer_x ? 0 : 1; stage < 2; ++stage) {
     bool progress = true;
     while (progress) {
       progress = false;
       for (int j = 0; j < m; ++j) {
         if (done[j]) continue;
+        if (stage == 0 && ops[j].kind == OPK_X) continue;
+        if (defer_x && stage == 1 && ops[j].kind != OPK_X) continue;
         bool ready = true;
         for (int i : preds[j]) if (!done[i]) { ready = false; break; }
         if (!ready) continue;
@@ -183,7 +189,8 @@ std::vector<phase_build> phases_by_dag(const std::vector<pop>& ops, const int* t
         progress = true;
       }
     }
-    phases.push_back(pb);
+    }
+    phases.push_back(pb);  // never empty: a fresh register set takes at least one ready op
   }
   if (phases.empty()) phases.emplace_back();
   return phases;
@@ -215,7 +222,8 @@ void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op
     if (ok) {
       const uint32_t t = 1u << d.treg;
       const int nctl = __builtin_popcount(d.creg) + __builtin_popcount(d.cthr);
-      ok = nctl <= 1 && (d.cthr == 0 || __builtin_ctz(d.cthr) >= 5) &&
+      // a lane-bit control would split a warp's direct HBM store; shared-memory writes take it
+      ok = nctl <= 1 && (d.cthr == 0 || !direct_store || __builtin_ctz(d.cthr) >= 5) &&
            !((later_target | later_diag | later_fold_ctl) & t) && !(later_target & d.creg);
       if (ok && direct_store && p.vbits) ok = d.treg != 0 && !(d.creg & 1u);
       if (ok && d.cout) ok = conditional < kMaxFolds;
@@ -252,14 +260,17 @@ void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op
       f.bit = bitpos;
       continue;
     }
+    // thread bit b: entry e of the low table (tid & 15) when b < 4, of the high table (tid >> 4) otherwise
     if (direct_store) {
       if (kind == 0) for (int e = 0; e < 16; ++e) out.store.tphys_lo[e] ^= x;
       else if (kind == 1) out.store.rphys[bitpos] ^= x;
+      else if (bitpos < 4) for (int e = 0; e < 16; ++e) { if ((e >> bitpos) & 1) out.store.tphys_lo[e] ^= x; }
       else for (int e = 0; e < 32; ++e) if ((e >> (bitpos - 4)) & 1) out.store.tphys_hi[e] ^= x;
     } else {
       const uint16_t xs = static_cast<uint16_t>(x);
       if (kind == 0) for (int e = 0; e < 16; ++e) dp.wtslot_lo[e] ^= xs;
       else if (kind == 1) dp.wslot[bitpos] ^= xs;
+      else if (bitpos < 4) for (int e = 0; e < 16; ++e) { if ((e >> bitpos) & 1) dp.wtslot_lo[e] ^= xs; }
       else for (int e = 0; e < 32; ++e) if ((e >> (bitpos - 4)) & 1) dp.wtslot_hi[e] ^= xs;
     }
   }
@@ -295,7 +306,11 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     out.num_runs = static_cast<uint8_t>(runs);
   }
 
-  std::vector<phase_build> phases = phases_by_dag(ops, tile_of_phys, R);
+  std::vector<phase_build> phases = phases_by_dag(ops, tile_of_phys, R, false);
+  if (p.defer_x) {  // taking CNOT / X gates last lets them fold; keep it unless it costs register phases
+    std::vector<phase_build> deferred = phases_by_dag(ops, tile_of_phys, R, true);
+    if (deferred.size() <= phases.size()) phases.swap(deferred);
+  }
   if (static_cast<int>(phases.size()) > kMaxPhases) phases = phases_in_order(ops, tile_of_phys, R);
   if (static_cast<int>(phases.size()) > kMaxPhases) throw std::logic_error("planner: too many phases");
 

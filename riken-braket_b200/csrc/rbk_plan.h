@@ -32,6 +32,7 @@ struct plan_params {
   int dense_budget;  // max dense 2x2 gates per pass
   bool fold_x = true;  // fold CNOT / X gates at the end of a phase into its write layout
   bool merge_1q = true;  // merge consecutive uncontrolled single-qubit gates on one qubit
+  bool defer_x = true;   // register phases take CNOT / X gates last (so that they fold)
 };
 
 // Plans `gates` (in order) into passes, updating the layout map

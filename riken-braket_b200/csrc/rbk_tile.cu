@@ -275,7 +275,7 @@ __device__ __forceinline__ void apply_folds(const dev_phase& ph, uint64_t base, 
     if (F.kind == 0) {
       thr ^= x;
     } else if (F.kind == 2) {
-      if ((tid >> F.bit) & 1u) thr ^= x;  // a warp bit: uniform within the warp
+      if ((tid >> F.bit) & 1u) thr ^= x;
     } else {
 #pragma unroll
       for (int b = 0; b < R; ++b) reg[b] ^= (b == F.bit) ? x : W(0);

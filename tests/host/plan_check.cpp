@@ -60,7 +60,7 @@ static void apply_folds(const dev_phase& D, uint64_t base, int tid, int R, uint6
     const dev_fold& F = D.folds[f];
     if ((base & F.cout) != F.cout) continue;
     if (F.kind == 0) thr ^= F.x;
-    else if (F.kind == 2) { if (F.bit < 5) { std::fprintf(stderr, "fold on a lane bit\n"); std::exit(12); } if ((tid >> F.bit) & 1) thr ^= F.x; }
+    else if (F.kind == 2) { if ((tid >> F.bit) & 1) thr ^= F.x; }
     else if (F.bit < R) reg[F.bit] ^= F.x;
     else { std::fprintf(stderr, "bad fold register\n"); std::exit(13); }
   }
