@@ -115,7 +115,7 @@ rbk::plan_params params_of(const rbk_state* s)
   rbk::shape_bits(s->precision, s->shape, &p.K, &p.R);
   p.LOW = s->precision == RBK_C128 ? rbk::precision_traits<double>::LOW : rbk::precision_traits<float>::LOW;
   p.vbits = s->precision == RBK_C128 ? 0 : 1;
-  p.dense_budget = s->dense_budget > 0 ? s->dense_budget : (s->precision == RBK_C128 ? 12 : 16);
+  p.dense_budget = s->dense_budget > 0 ? s->dense_budget : (s->precision == RBK_C128 ? 12 : 14);
   return p;
 }
 
