@@ -278,6 +278,43 @@ void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op
   op_end = kept;
 }
 
+// Runs of phase gates -- DIAG with d0 == 1 exactly, NEG: a factor on the
+// amplitudes whose bits of the gate are all one -- go to the kernel behind one
+// PHASES header: it multiplies each gate's factor into a per-thread
+// accumulator (the whole thread's, or that of one register bit) and applies
+// the products once, instead of running every gate over the registers.
+bool is_phase_op(const dev_op& d)
+{
+  return d.kind == OPK_NEG || (d.kind == OPK_DIAG && d.diag_one && d.m[0] == 1.0 && d.m[1] == 0.0);
+}
+
+// headers_left: headers the pass may still add (kMaxPassOps - kMaxPassGates in
+// all), so that the gates of later phases still fit in the op records.
+void group_phase_runs(dev_pass& out, dev_phase& dp, int& op_end, int& headers_left)
+{
+  const int begin = dp.op_begin;
+  std::vector<dev_op> list(out.ops + begin, out.ops + op_end);
+  std::vector<dev_op> grouped;
+  for (size_t i = 0; i < list.size();) {
+    size_t j = i;
+    while (j < list.size() && is_phase_op(list[j])) ++j;
+    if (j - i >= 2 && headers_left > 0) {
+      dev_op h{};
+      h.kind = OPK_PHASES;
+      h.run = static_cast<uint32_t>(j - i);
+      h.code = op_code(OPK_PHASES, 0, true, 0);
+      grouped.push_back(h);
+      --headers_left;
+    }
+    if (j == i) ++j;  // a gate that is not a phase
+    for (size_t k = i; k < j; ++k) grouped.push_back(list[k]);
+    i = j;
+  }
+  if (begin + static_cast<int>(grouped.size()) > kMaxPassOps) throw std::logic_error("planner: too many op records");
+  for (size_t k = 0; k < grouped.size(); ++k) out.ops[begin + static_cast<int>(k)] = grouped[k];
+  op_end = begin + static_cast<int>(grouped.size());
+}
+
 void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>& ops,
                 const int* relabel_to, const int* tile_phys, dev_pass& out)
 {
@@ -322,6 +359,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
   auto contains = [](const std::vector<int>& v, int x) { return std::find(v.begin(), v.end(), x) != v.end(); };
 
   int op_index = 0;
+  int headers_left = kMaxPassOps - kMaxPassGates;
   for (size_t ph = 0; ph < phases.size(); ++ph) {
     auto& pb = phases[ph];
     const bool first = ph == 0, last = ph + 1 == phases.size();
@@ -423,6 +461,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     dp.op_begin = static_cast<uint16_t>(op_index);
     for (int oi : pb.ops) {
       const pop& o = ops[oi];
+      if (op_index >= kMaxPassOps) throw std::logic_error("planner: too many op records");
       dev_op& d = out.ops[op_index++];
       d = dev_op{};  // the slot may hold an op of an earlier phase that folding removed
       d.kind = o.kind;
@@ -458,6 +497,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
              : op_code(d.kind, 0, true, 0);
     }
     if (p.fold_x) fold_trailing_x(p, out, dp, op_index, last && ds);
+    if (p.phase_runs) group_phase_runs(out, dp, op_index, headers_left);
     dp.op_end = static_cast<uint16_t>(op_index);
   }
   out.num_phases = static_cast<uint8_t>(phases.size());
@@ -594,7 +634,7 @@ void plan_passes(const plan_params& p, const std::vector<hgate>& gates, std::vec
         if (((blockN | blockZ) & all) == all) break;
         continue;
       }
-      bool ok = static_cast<int>(ops.size()) < kMaxPassOps;
+      bool ok = static_cast<int>(ops.size()) < kMaxPassGates;
       const int t = Nq ? perm[g.target] : -1;
       if (ok && t >= 0 && !(tile & bit(t)) && popc(tile) >= p.K) ok = false;
       if (ok && is_dense(g) && dense >= budget) ok = false;

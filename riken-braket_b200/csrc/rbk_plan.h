@@ -33,6 +33,7 @@ struct plan_params {
   bool fold_x = true;  // fold CNOT / X gates at the end of a phase into its write layout
   bool merge_1q = true;  // merge consecutive uncontrolled single-qubit gates on one qubit
   bool defer_x = true;   // register phases take CNOT / X gates last (so that they fold)
+  bool phase_runs = true;  // runs of phase gates behind one PHASES header
 };
 
 // Plans `gates` (in order) into passes, updating the layout map

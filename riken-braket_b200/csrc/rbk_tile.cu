@@ -135,14 +135,78 @@ __device__ __forceinline__ void apply_y(typename ctype<Real>::c* a, uint32_t cre
   }
 }
 
-// One jump per op: the host encodes (kind, matrix form, controls, target bit)
-// into op.code (see op_code in rbk_internal.h).
+// A run of phase gates (PHASES header; rbk_plan.cpp group_phase_runs): gate k
+// multiplies the amplitudes whose bits of the gate are all one by its factor
+// (d1 of a DIAG with d0 == 1, -1 of a NEG).  Gates whose register bits are
+// none or one only multiply a per-thread accumulator -- the thread's, or that
+// of the register bit -- and every amplitude takes the product of its
+// accumulators once at the end; gates on two or more register bits apply
+// directly.  Accumulation in double for both precisions.
 template <typename Real, int R>
-__device__ __forceinline__ void apply_op(typename ctype<Real>::c* a, const dev_op& op, uint32_t tid, uint64_t base)
+__device__ __forceinline__ void apply_phase_run(typename ctype<Real>::c* a, const dev_op* run, int count, uint32_t tid,
+                                                uint64_t base)
+{
+  constexpr int NR = 1 << R;
+  double fr = 1.0, fi = 0.0;
+  double lr[R], li[R];
+#pragma unroll
+  for (int b = 0; b < R; ++b) { lr[b] = 1.0; li[b] = 0.0; }
+  for (int k = 0; k < count; ++k) {
+    const dev_op& g = run[k];
+    const uint32_t mt = g.cthr | g.dthr;
+    const uint64_t mo = g.cout | g.dout;
+    if ((tid & mt) != mt || (base & mo) != mo) continue;
+    const uint32_t mr = g.creg | g.dreg;
+    const double dr = g.kind == OPK_NEG ? -1.0 : g.m[2], di = g.kind == OPK_NEG ? 0.0 : g.m[3];
+    if (mr == 0) {
+      const double t = fr * dr - fi * di;
+      fi = fr * di + fi * dr;
+      fr = t;
+    } else if ((mr & (mr - 1)) == 0) {
+#pragma unroll
+      for (int b = 0; b < R; ++b) {
+        if (mr == (1u << b)) {
+          const double t = lr[b] * dr - li[b] * di;
+          li[b] = lr[b] * di + li[b] * dr;
+          lr[b] = t;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NR; ++i) {
+        if ((uint32_t(i) & mr) != mr) continue;
+        const double xr = double(a[i].x), xi = double(a[i].y);
+        a[i].x = static_cast<Real>(xr * dr - xi * di);
+        a[i].y = static_cast<Real>(xr * di + xi * dr);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    double pr = fr, pi = fi;
+#pragma unroll
+    for (int b = 0; b < R; ++b) {
+      if ((i >> b) & 1) {
+        const double t = pr * lr[b] - pi * li[b];
+        pi = pr * li[b] + pi * lr[b];
+        pr = t;
+      }
+    }
+    const double xr = double(a[i].x), xi = double(a[i].y);
+    a[i].x = static_cast<Real>(xr * pr - xi * pi);
+    a[i].y = static_cast<Real>(xr * pi + xi * pr);
+  }
+}
+
+// One jump per op: the host encodes (kind, matrix form, controls, target bit)
+// into op.code (see op_code in rbk_internal.h).  Returns how many of the
+// following op records the op consumed (a phase run's gates).
+template <typename Real, int R>
+__device__ __forceinline__ int apply_op(typename ctype<Real>::c* a, const dev_op& op, uint32_t tid, uint64_t base)
 {
   using C = typename ctype<Real>::c;
   constexpr int NR = 1 << R;
-  if ((tid & op.cthr) != op.cthr || (base & op.cout) != op.cout) return;
+  if ((tid & op.cthr) != op.cthr || (base & op.cout) != op.cout) return 0;
   const uint32_t creg = op.creg;
 #define RBK_MAT_CASES(FORM, CTRL, B)                                                                    \
   case op_code(OPK_MAT, FORM, CTRL, B):                                                                 \
@@ -191,8 +255,12 @@ __device__ __forceinline__ void apply_op(typename ctype<Real>::c* a, const dev_o
       }
       break;
     }
+    case op_code(OPK_PHASES, 0, true, 0):
+      apply_phase_run<Real, R>(a, &op + 1, static_cast<int>(op.run), tid, base);
+      return static_cast<int>(op.run);
     default: break;
   }
+  return 0;
 #undef RBK_PERM_CASES
 #undef RBK_PERM_CASE
 #undef RBK_MAT_BITS
@@ -328,7 +396,7 @@ __device__ __forceinline__ void tile_phases(typename ctype<Real>::c* __restrict_
       }
     }
 
-    for (int o = ph.op_begin; o < ph.op_end; ++o) apply_op<Real, R>(a, P.ops[o], tid, base);
+    for (int o = ph.op_begin; o < ph.op_end; ++o) o += apply_op<Real, R>(a, P.ops[o], tid, base);
 
     if (p + 1 == nph && P.direct_store) {
       // A one-phase pass that also loaded straight from HBM: every warp of the

@@ -134,6 +134,17 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
                                    : (op.kind == OPK_X || op.kind == OPK_Y) ? op_code(op.kind, 0, true, op.treg)
                                    : op_code(op.kind, 0, true, 0);
           if (op.code != want_code || op.code >= kNumOpCodes || op.treg >= R) { std::fprintf(stderr, "bad dispatch code\n"); std::exit(8); }
+          if (op.kind == OPK_PHASES) {  // a run header: the run's gates follow in this phase, each a pure phase
+            if (op.run < 2 || o + static_cast<int>(op.run) >= D.op_end) { std::fprintf(stderr, "bad phase run\n"); std::exit(14); }
+            for (int k = 1; k <= static_cast<int>(op.run); ++k) {
+              const dev_op& g = P.ops[o + k];
+              if (!(g.kind == OPK_NEG || (g.kind == OPK_DIAG && g.diag_one && g.m[0] == 1.0 && g.m[1] == 0.0))) {
+                std::fprintf(stderr, "phase run holds a gate that is not a phase\n");
+                std::exit(15);
+              }
+            }
+            continue;
+          }
           if ((uint32_t(tid) & op.cthr) != op.cthr || (base & op.cout) != op.cout) continue;
           const cplx m00{op.m[0], op.m[1]}, m01{op.m[2], op.m[3]}, m10{op.m[4], op.m[5]}, m11{op.m[6], op.m[7]};
           for (int i = 0; i < NR; ++i) {
@@ -193,13 +204,16 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
   }
 }
 
-static hgate random_gate(std::mt19937_64& rng, int n)
+// phase_heavy: mostly diagonal gates and sign flips between dense ones, so
+// that register phases hold many short runs of phase gates.
+static hgate random_gate(std::mt19937_64& rng, int n, bool phase_heavy = false)
 {
   hgate g{};
   g.target2 = -1;
   std::uniform_int_distribution<int> kind(0, 9), q(0, n - 1), nc(0, 2);
   std::uniform_real_distribution<double> u(-1, 1);
-  const int k = kind(rng);
+  int k = kind(rng);
+  if (phase_heavy) k = (k < 2) ? 0 : (k < 4) ? 4 : (k < 7) ? 6 : 7;  // MAT, X, DIAG, NEG
   g.target = static_cast<int8_t>(q(rng));
   const int ncontrols = nc(rng) == 2 ? 1 + (rng() % 2) : 0;
   for (int c = 0; c < ncontrols; ++c) {
@@ -240,7 +254,8 @@ int main(int argc, char** argv)
       for (auto& x : init) x = cplx{nd(rng), nd(rng)};
       std::vector<hgate> gates;
       const int count = 50 + static_cast<int>(rng() % 300);
-      for (int i = 0; i < count; ++i) gates.push_back(random_gate(rng, p.n));
+      const bool phase_heavy = seed % 2 == 1;
+      for (int i = 0; i < count; ++i) gates.push_back(random_gate(rng, p.n, phase_heavy));
 
       std::vector<cplx> want = init;
       for (const auto& g : gates) apply_direct(want, g);
