@@ -49,7 +49,7 @@ inline void shape_bits(int precision, int shape, int* K, int* R)
 }
 
 constexpr int kMaxPassGates = 112;  // gates the planner puts in one pass
-constexpr int kMaxPassOps = 128;    // op records of a pass: the gates plus phase-run headers
+constexpr int kMaxPassOps = 128;    // op records of a pass: the gates plus phase-run and layer headers
 constexpr int kMaxPhases = 16;
 constexpr int kMaxQubits = 40;
 
@@ -60,11 +60,15 @@ enum op_kind : uint8_t {
   OPK_DIAG = 4,  // amplitude *= (target bit ? d1 : d0) when the controls are all one
   OPK_NEG = 5,   // amplitude *= -1 when the controls are all one (Z, CZ: exact)
   OPK_PHASES = 6,  // header of a run of `run` phase ops that follow (DIAG with d0 == 1, NEG)
+  OPK_LAYER = 7,   // header of `run` uncontrolled MAT ops that follow, on distinct register bits
+                   // (mask dreg) in ascending bit order; applied as one straight-line block
 };
 
 // Dispatch key of a pass op: MAT ops are keyed by matrix form (0 general,
 // 1 real, 2 real m00), by whether register-bit controls exist and by the target
-// register bit; X and Y by the target bit; NEG, DIAG and PHASES by kind alone.
+// register bit; X and Y by the target bit; NEG, DIAG and PHASES by kind alone;
+// LAYER by the form its matrices are applied in and by whether it covers every
+// register bit (passed as `controlled`).
 #ifdef __CUDACC__
 #define RBK_HOST_DEVICE __host__ __device__
 #else
@@ -77,22 +81,23 @@ RBK_HOST_DEVICE constexpr uint32_t op_code(int kind, int form, bool controlled, 
   return kind == OPK_MAT ? uint32_t((form * 2 + (controlled ? 1 : 0)) * 5 + treg)
        : kind == OPK_X ? 30u + uint32_t(treg)
        : kind == OPK_Y ? 35u + uint32_t(treg)
-       : kind == OPK_NEG ? 40u : kind == OPK_DIAG ? 41u : 42u;
+       : kind == OPK_NEG ? 40u : kind == OPK_DIAG ? 41u : kind == OPK_PHASES ? 42u
+       : 43u + uint32_t(form * 2 + (controlled ? 1 : 0));
 }
-constexpr uint32_t kNumOpCodes = 43;
+constexpr uint32_t kNumOpCodes = 49;
 
 // One gate inside a pass, in the coordinates of the phase it belongs to.
 struct alignas(8) dev_op {
   uint8_t kind;
   uint8_t treg;       // MAT/X/Y: target register bit
   uint8_t diag_one;   // DIAG: d0 == 1 exactly (phase-shift form: only the one-half is touched)
-  uint8_t real;       // MAT: 1 = all four entries real (H, exp(i theta Y)); 2 = m00 real (U3, U2)
+  uint8_t real;       // MAT: 1 = all four entries real (H, exp(i theta Y)); 2 = m00 real (U3, U2); LAYER: the form used
   uint32_t creg;      // controls inside the register bits
   uint32_t cthr;      // controls inside the thread bits
-  uint32_t dreg;      // DIAG target bit among the register bits (mask), 0 if elsewhere
+  uint32_t dreg;      // DIAG target bit among the register bits (mask), 0 if elsewhere; LAYER: its register bits
   uint32_t dthr;      // DIAG target bit among the thread bits (mask)
   uint32_t code;      // op_code(kind, form, controlled, treg): the kernel's single dispatch key
-  uint32_t run;       // PHASES: number of phase ops that follow and belong to the run
+  uint32_t run;       // PHASES, LAYER: number of ops that follow and belong to the header
   uint64_t cout;      // controls on physical bits outside the tile
   uint64_t dout;      // DIAG target on a physical bit outside the tile (mask)
   double m[8];        // MAT: m00 m01 m10 m11 as (re, im); DIAG: d0 d1

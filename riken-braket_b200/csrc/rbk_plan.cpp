@@ -315,6 +315,59 @@ void group_phase_runs(dev_pass& out, dev_phase& dp, int& op_end, int& headers_le
   op_end = begin + static_cast<int>(grouped.size());
 }
 
+// Consecutive uncontrolled MAT ops of a phase on distinct register bits go to
+// the kernel behind one LAYER header, sorted by register bit (gates on distinct
+// qubits commute): the kernel applies them as one straight-line block, with no
+// dispatch between the gates.  Form: the matrices' common form, where m00-real
+// ones may join general ones (the general update computes the same values);
+// real ones join only real ones.
+int layer_form(int a, int b)
+{
+  if (a == b) return a;
+  if ((a == 0 && b == 2) || (a == 2 && b == 0)) return 0;
+  return -1;
+}
+
+void group_layers(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_end, int& headers_left)
+{
+  const int begin = dp.op_begin;
+  std::vector<dev_op> list(out.ops + begin, out.ops + op_end);
+  auto layer_op = [](const dev_op& d) { return d.kind == OPK_MAT && d.creg == 0 && d.cthr == 0 && d.cout == 0; };
+  std::vector<dev_op> grouped;
+  for (size_t i = 0; i < list.size();) {
+    size_t j = i;
+    uint32_t mask = 0;
+    int form = layer_op(list[i]) ? list[i].real : -1;
+    while (j < list.size() && layer_op(list[j]) && !((mask >> list[j].treg) & 1u)) {
+      const int f = layer_form(form, list[j].real);
+      if (f < 0) break;
+      form = f;
+      mask |= 1u << list[j].treg;
+      ++j;
+    }
+    if (j - i >= 2 && headers_left > 0) {
+      dev_op h{};
+      h.kind = OPK_LAYER;
+      h.run = static_cast<uint32_t>(j - i);
+      h.dreg = mask;
+      h.real = static_cast<uint8_t>(form);
+      h.code = op_code(OPK_LAYER, form, mask == (1u << p.R) - 1, 0);
+      grouped.push_back(h);
+      --headers_left;
+      std::vector<dev_op> run(list.begin() + static_cast<long>(i), list.begin() + static_cast<long>(j));
+      std::sort(run.begin(), run.end(), [](const dev_op& x, const dev_op& y) { return x.treg < y.treg; });
+      grouped.insert(grouped.end(), run.begin(), run.end());
+    } else {
+      if (j == i) ++j;
+      for (size_t k = i; k < j; ++k) grouped.push_back(list[k]);
+    }
+    i = j;
+  }
+  if (begin + static_cast<int>(grouped.size()) > kMaxPassOps) throw std::logic_error("planner: too many op records");
+  for (size_t k = 0; k < grouped.size(); ++k) out.ops[begin + static_cast<int>(k)] = grouped[k];
+  op_end = begin + static_cast<int>(grouped.size());
+}
+
 void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>& ops,
                 const int* relabel_to, const int* tile_phys, dev_pass& out)
 {
@@ -498,6 +551,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     }
     if (p.fold_x) fold_trailing_x(p, out, dp, op_index, last && ds);
     if (p.phase_runs) group_phase_runs(out, dp, op_index, headers_left);
+    if (p.layers) group_layers(p, out, dp, op_index, headers_left);
     dp.op_end = static_cast<uint16_t>(op_index);
   }
   out.num_phases = static_cast<uint8_t>(phases.size());

@@ -34,6 +34,7 @@ struct plan_params {
   bool merge_1q = true;  // merge consecutive uncontrolled single-qubit gates on one qubit
   bool defer_x = true;   // register phases take CNOT / X gates last (so that they fold)
   bool phase_runs = true;  // runs of phase gates behind one PHASES header
+  bool layers = true;      // uncontrolled 2x2 gates on distinct register bits behind one LAYER header
 };
 
 // Plans `gates` (in order) into passes, updating the layout map

@@ -198,6 +198,45 @@ __device__ __forceinline__ void apply_phase_run(typename ctype<Real>::c* a, cons
   }
 }
 
+// One gate of a LAYER on register bit B, in the layer's matrix form.
+template <typename Real, int R, int FORM, int B>
+__device__ __forceinline__ void layer_gate(typename ctype<Real>::c* a, const dev_op& g)
+{
+  constexpr int NR = 1 << R;
+  if constexpr (FORM == 1) {
+    apply_real<Real, B, NR, false>(a, 0u, (Real)g.m[0], (Real)g.m[2], (Real)g.m[4], (Real)g.m[6]);
+  } else {
+    const mat2<Real> M{(Real)g.m[0], FORM == 2 ? (Real)0 : (Real)g.m[1], (Real)g.m[2], (Real)g.m[3],
+                       (Real)g.m[4], (Real)g.m[5], (Real)g.m[6], (Real)g.m[7]};
+    if constexpr (FORM == 2) apply_mat_r00<Real, B, NR, false>(a, 0u, M);
+    else apply_mat<Real, B, NR, false>(a, 0u, M);
+  }
+}
+
+// A LAYER (rbk_plan.cpp group_layers): the uncontrolled 2x2 gates that follow
+// the header, one per register bit of `mask` in ascending bit order, with no
+// dispatch between them.  FULL: every register bit has one; for complex<double>
+// (4 register bits) the gates then run as one straight-line block.  For
+// complex<float> (5 register bits) that block made the kernel spill registers
+// and run slower (30-qubit brick: 350 ms against 317 ms with the per-bit form),
+// so it takes the per-bit form for every mask.
+template <typename Real, int R, int FORM, bool FULL, int B = 0>
+__device__ __forceinline__ void apply_layer(typename ctype<Real>::c* a, const dev_op* g, uint32_t mask)
+{
+  if constexpr (B < R) {
+    if constexpr (FULL && sizeof(Real) == 8) {
+      layer_gate<Real, R, FORM, B>(a, g[B]);
+      apply_layer<Real, R, FORM, FULL, B + 1>(a, g, mask);
+    } else {
+      if ((mask >> B) & 1u) {
+        layer_gate<Real, R, FORM, B>(a, *g);
+        ++g;
+      }
+      apply_layer<Real, R, FORM, FULL, B + 1>(a, g, mask);
+    }
+  }
+}
+
 // One jump per op: the host encodes (kind, matrix form, controls, target bit)
 // into op.code (see op_code in rbk_internal.h).  Returns how many of the
 // following op records the op consumed (a phase run's gates).
@@ -258,6 +297,14 @@ __device__ __forceinline__ int apply_op(typename ctype<Real>::c* a, const dev_op
     case op_code(OPK_PHASES, 0, true, 0):
       apply_phase_run<Real, R>(a, &op + 1, static_cast<int>(op.run), tid, base);
       return static_cast<int>(op.run);
+#define RBK_LAYER_CASE(FORM, FULL) \
+    case op_code(OPK_LAYER, FORM, FULL, 0): \
+      apply_layer<Real, R, FORM, FULL>(a, &op + 1, op.dreg); \
+      return static_cast<int>(op.run);
+    RBK_LAYER_CASE(0, false) RBK_LAYER_CASE(0, true)
+    RBK_LAYER_CASE(1, false) RBK_LAYER_CASE(1, true)
+    RBK_LAYER_CASE(2, false) RBK_LAYER_CASE(2, true)
+#undef RBK_LAYER_CASE
     default: break;
   }
   return 0;
@@ -418,7 +465,9 @@ __device__ __forceinline__ void tile_phases(typename ctype<Real>::c* __restrict_
         __stcs(gdst + (phys >> VB), vec_io<Real>::pack(&a[i]));
       }
     } else {
-      __syncthreads();  // every thread has read this phase's layout
+      // Every thread has read this phase's layout from `tile` (a phase that
+      // loaded straight from HBM has not used it).
+      if (!(p == 0 && from_hbm)) __syncthreads();
       uint32_t ts = ph.wtslot_lo[tid & 15] ^ ph.wtslot_hi[tid >> 4];
       uint32_t rs[R];
 #pragma unroll

@@ -132,6 +132,7 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
           const dev_op& op = P.ops[o];
           const uint32_t want_code = op.kind == OPK_MAT ? op_code(OPK_MAT, op.real, op.creg != 0, op.treg)
                                    : (op.kind == OPK_X || op.kind == OPK_Y) ? op_code(op.kind, 0, true, op.treg)
+                                   : op.kind == OPK_LAYER ? op_code(OPK_LAYER, op.real, op.dreg == (1u << R) - 1, 0)
                                    : op_code(op.kind, 0, true, 0);
           if (op.code != want_code || op.code >= kNumOpCodes || op.treg >= R) { std::fprintf(stderr, "bad dispatch code\n"); std::exit(8); }
           if (op.kind == OPK_PHASES) {  // a run header: the run's gates follow in this phase, each a pure phase
@@ -141,6 +142,27 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
               if (!(g.kind == OPK_NEG || (g.kind == OPK_DIAG && g.diag_one && g.m[0] == 1.0 && g.m[1] == 0.0))) {
                 std::fprintf(stderr, "phase run holds a gate that is not a phase\n");
                 std::exit(15);
+              }
+            }
+            continue;
+          }
+          if (op.kind == OPK_LAYER) {  // a layer header: one uncontrolled 2x2 gate per bit of dreg follows, in bit order
+            if (op.run < 2 || o + static_cast<int>(op.run) >= D.op_end || op.real > 2 || op.dreg >= (1u << R) ||
+                __builtin_popcount(op.dreg) != static_cast<int>(op.run) || op.creg || op.cthr || op.cout) {
+              std::fprintf(stderr, "bad layer header\n");
+              std::exit(16);
+            }
+            uint32_t bits = op.dreg;
+            for (int k = 1; k <= static_cast<int>(op.run); ++k) {
+              const dev_op& g = P.ops[o + k];
+              const int want = __builtin_ctz(bits);
+              bits &= bits - 1;
+              // the layer's form must compute each matrix exactly: real only with real,
+              // general with general or m00-real
+              const bool form_ok = op.real == g.real || (op.real == 0 && g.real == 2);
+              if (g.kind != OPK_MAT || g.creg || g.cthr || g.cout || g.treg != want || !form_ok) {
+                std::fprintf(stderr, "layer holds a gate it cannot run\n");
+                std::exit(17);
               }
             }
             continue;
