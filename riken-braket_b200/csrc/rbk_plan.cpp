@@ -83,8 +83,12 @@ struct phase_tracker {
 
 // Orders the thread bits of a phase so that the lowest lanes fall on tile bits
 // that map to distinct shared-memory bank groups (see smem_slot in
-// rbk_kernels.cu: vector-index bit b contributes to slot bit b mod 3).
-void order_thread_bits(std::vector<int>& thr, int vbits)
+// rbk_device.cuh: vector-index bit b contributes to slot bit b mod 3): the
+// lanes of one 128-byte wavefront then touch 8 distinct 16-byte bank groups.
+// wmap (the last phase of a pass, which writes the tile back relabelled): the
+// write puts thread bit b at tile bit wmap[b], so the lanes are chosen to be
+// conflict-free for that write too where the thread bits allow it.
+void order_thread_bits(std::vector<int>& thr, int vbits, const int* wmap)
 {
   std::vector<int> out;
   std::vector<int> rest(thr);
@@ -93,12 +97,35 @@ void order_thread_bits(std::vector<int>& thr, int vbits)
     rest.erase(std::find(rest.begin(), rest.end(), b));
   };
   if (vbits == 1 && std::find(rest.begin(), rest.end(), 0) != rest.end()) take(0);
-  bool used[3] = {false, false, false};
-  for (int pass = 0; pass < 3; ++pass) {
-    for (int b : std::vector<int>(rest)) {
-      if (b < vbits) continue;
-      const int res = (b - vbits) % 3;
-      if (!used[res]) { used[res] = true; take(b); break; }
+  auto residue = [&](int b) { return b < vbits ? -1 : (b - vbits) % 3; };
+  bool done = false;
+  if (wmap) {  // three lanes with distinct residues both where they are read and where they are written
+    const std::vector<int> cand(rest);
+    const size_t m = cand.size();
+    for (size_t i = 0; i < m && !done; ++i)
+      for (size_t j = i + 1; j < m && !done; ++j)
+        for (size_t k = j + 1; k < m && !done; ++k) {
+          const int b[3] = {cand[i], cand[j], cand[k]};
+          bool rd[3] = {false, false, false}, wr[3] = {false, false, false}, ok = true;
+          for (int x : b) {
+            const int r = residue(x), w = residue(wmap[x]);
+            if (r < 0 || w < 0 || rd[r] || wr[w]) { ok = false; break; }
+            rd[r] = wr[w] = true;
+          }
+          if (ok) {
+            for (int x : b) take(x);
+            done = true;
+          }
+        }
+  }
+  if (!done) {
+    bool used[3] = {false, false, false};
+    for (int pass = 0; pass < 3; ++pass) {
+      for (int b : std::vector<int>(rest)) {
+        if (b < vbits) continue;
+        const int res = residue(b);
+        if (!used[res]) { used[res] = true; take(b); break; }
+      }
     }
   }
   std::sort(rest.begin(), rest.end());
@@ -449,15 +476,29 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     }
     std::vector<int> thr;
     for (int b = 0; b < K; ++b) if (!contains(pb.reg, b)) thr.push_back(b);
+    // The five lanes of a direct HBM access may come in any order (a warp
+    // still touches one 512-byte run); the order puts three tile bits with
+    // distinct bank residues on lanes 0-2 where it can, for the phase's
+    // shared-memory accesses in the same layout.
     auto lanes_first = [&](const std::vector<int>& lanes) {
       std::vector<int> o(lanes);
+      if (!p.vbits) {
+        bool used[3] = {false, false, false};
+        std::vector<int> front, back;
+        for (int b : o) {
+          if (front.size() < 3 && !used[b % 3]) { used[b % 3] = true; front.push_back(b); }
+          else back.push_back(b);
+        }
+        o = front;
+        o.insert(o.end(), back.begin(), back.end());
+      }
       for (int b : thr) if (!contains(lanes, b)) o.push_back(b);
       thr = o;
     };
     if (dl) lanes_first({lane0, lane0 + 1, lane0 + 2, lane0 + 3, lane0 + 4});
     else if (ds) lanes_first({relabel_from[lane0], relabel_from[lane0 + 1], relabel_from[lane0 + 2],
                               relabel_from[lane0 + 3], relabel_from[lane0 + 4]});
-    else order_thread_bits(thr, p.vbits);
+    else order_thread_bits(thr, p.vbits, last ? relabel_to : nullptr);
     // c64 vectors: register index bit 0 must be the amplitude pair bit.
     if (p.vbits && (dl || ds)) {
       const int want = dl ? 0 : relabel_from[0];
