@@ -99,7 +99,7 @@ struct alignas(8) dev_op {
   uint32_t code;      // op_code(kind, form, controlled, treg): the kernel's single dispatch key
   uint32_t run;       // PHASES, LAYER: number of ops that follow and belong to the header
   uint64_t cout;      // controls on physical bits outside the tile
-  uint64_t dout;      // DIAG target on a physical bit outside the tile (mask)
+  uint64_t dout;      // DIAG target on a physical bit outside the tile (mask); PHASES: the run's class sizes
   double m[8];        // MAT: m00 m01 m10 m11 as (re, im); DIAG: d0 d1
 };
 

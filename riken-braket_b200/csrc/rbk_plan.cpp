@@ -310,6 +310,13 @@ void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op
 // PHASES header: it multiplies each gate's factor into a per-thread
 // accumulator (the whole thread's, or that of one register bit) and applies
 // the products once, instead of running every gate over the registers.
+// The members are rewritten in the run's own form: all the gate's bits in
+// creg / cthr / cout (controls and target alike), the factor in (m[2], m[3]).
+// They are sorted by accumulator -- no register bit, register bit 0, ..., R-1,
+// then two or more register bits (gates that multiply amplitudes directly) --
+// and the header's dout holds the class sizes, one byte each in that order
+// (the last class takes the rest of `run`).  The gates of a run commute, so
+// their order is free.
 bool is_phase_op(const dev_op& d)
 {
   return d.kind == OPK_NEG || (d.kind == OPK_DIAG && d.diag_one && d.m[0] == 1.0 && d.m[1] == 0.0);
@@ -317,7 +324,7 @@ bool is_phase_op(const dev_op& d)
 
 // headers_left: headers the pass may still add (kMaxPassOps - kMaxPassGates in
 // all), so that the gates of later phases still fit in the op records.
-void group_phase_runs(dev_pass& out, dev_phase& dp, int& op_end, int& headers_left)
+void group_phase_runs(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_end, int& headers_left)
 {
   const int begin = dp.op_begin;
   std::vector<dev_op> list(out.ops + begin, out.ops + op_end);
@@ -326,15 +333,42 @@ void group_phase_runs(dev_pass& out, dev_phase& dp, int& op_end, int& headers_le
     size_t j = i;
     while (j < list.size() && is_phase_op(list[j])) ++j;
     if (j - i >= 2 && headers_left > 0) {
+      std::vector<dev_op> members;
+      for (size_t k = i; k < j; ++k) {
+        dev_op g = list[k];
+        const bool neg = g.kind == OPK_NEG;
+        g.creg |= g.dreg;
+        g.cthr |= g.dthr;
+        g.cout |= g.dout;
+        g.dreg = g.dthr = 0;
+        g.dout = 0;
+        g.kind = OPK_DIAG;
+        g.diag_one = 1;
+        g.m[0] = 1.0;
+        g.m[1] = 0.0;
+        if (neg) { g.m[2] = -1.0; g.m[3] = 0.0; }
+        members.push_back(g);
+      }
+      auto cls = [&](const dev_op& g) {
+        const int c = __builtin_popcount(g.creg);
+        return c == 0 ? 0 : c == 1 ? 1 + __builtin_ctz(g.creg) : 1 + p.R;
+      };
+      std::stable_sort(members.begin(), members.end(), [&](const dev_op& x, const dev_op& y) { return cls(x) < cls(y); });
       dev_op h{};
       h.kind = OPK_PHASES;
       h.run = static_cast<uint32_t>(j - i);
       h.code = op_code(OPK_PHASES, 0, true, 0);
+      for (const dev_op& g : members) {
+        const int c = cls(g);
+        if (c <= p.R) h.dout += 1ull << (8 * c);
+      }
       grouped.push_back(h);
       --headers_left;
+      grouped.insert(grouped.end(), members.begin(), members.end());
+    } else {
+      if (j == i) ++j;  // a gate that is not a phase
+      for (size_t k = i; k < j; ++k) grouped.push_back(list[k]);
     }
-    if (j == i) ++j;  // a gate that is not a phase
-    for (size_t k = i; k < j; ++k) grouped.push_back(list[k]);
     i = j;
   }
   if (begin + static_cast<int>(grouped.size()) > kMaxPassOps) throw std::logic_error("planner: too many op records");
@@ -591,7 +625,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
              : op_code(d.kind, 0, true, 0);
     }
     if (p.fold_x) fold_trailing_x(p, out, dp, op_index, last && ds);
-    if (p.phase_runs) group_phase_runs(out, dp, op_index, headers_left);
+    if (p.phase_runs) group_phase_runs(p, out, dp, op_index, headers_left);
     if (p.layers) group_layers(p, out, dp, op_index, headers_left);
     dp.op_end = static_cast<uint16_t>(op_index);
   }

@@ -135,63 +135,63 @@ __device__ __forceinline__ void apply_y(typename ctype<Real>::c* a, uint32_t cre
   }
 }
 
+// Multiplies (xr, xi) by (dr, di) in place.
+__device__ __forceinline__ void cmul_acc(double& xr, double& xi, double dr, double di)
+{
+  const double t = xr * dr - xi * di;
+  xi = xr * di + xi * dr;
+  xr = t;
+}
+
 // A run of phase gates (PHASES header; rbk_plan.cpp group_phase_runs): gate k
-// multiplies the amplitudes whose bits of the gate are all one by its factor
-// (d1 of a DIAG with d0 == 1, -1 of a NEG).  Gates whose register bits are
-// none or one only multiply a per-thread accumulator -- the thread's, or that
-// of the register bit -- and every amplitude takes the product of its
-// accumulators once at the end; gates on two or more register bits apply
-// directly.  Accumulation in double for both precisions.
+// multiplies the amplitudes whose bits creg / cthr / cout are all one by its
+// factor (m[2], m[3]).  The members come sorted by accumulator, with the class
+// sizes in the header's dout: gates on no register bit multiply the thread's
+// accumulator, gates on one register bit b that of b, and every amplitude takes
+// the product of its accumulators once at the end; gates on two or more
+// register bits (the rest of the run) multiply their amplitudes directly.
+// Accumulation in double for both precisions.
 template <typename Real, int R>
-__device__ __forceinline__ void apply_phase_run(typename ctype<Real>::c* a, const dev_op* run, int count, uint32_t tid,
-                                                uint64_t base)
+__device__ __forceinline__ void apply_phase_run(typename ctype<Real>::c* a, const dev_op* run, int count,
+                                                uint64_t classes, uint32_t tid, uint64_t base)
 {
   constexpr int NR = 1 << R;
   double fr = 1.0, fi = 0.0;
   double lr[R], li[R];
 #pragma unroll
   for (int b = 0; b < R; ++b) { lr[b] = 1.0; li[b] = 0.0; }
-  for (int k = 0; k < count; ++k) {
+  int k = 0;
+  for (const int e = static_cast<int>(classes & 0xff); k < e; ++k) {
     const dev_op& g = run[k];
-    const uint32_t mt = g.cthr | g.dthr;
-    const uint64_t mo = g.cout | g.dout;
-    if ((tid & mt) != mt || (base & mo) != mo) continue;
-    const uint32_t mr = g.creg | g.dreg;
-    const double dr = g.kind == OPK_NEG ? -1.0 : g.m[2], di = g.kind == OPK_NEG ? 0.0 : g.m[3];
-    if (mr == 0) {
-      const double t = fr * dr - fi * di;
-      fi = fr * di + fi * dr;
-      fr = t;
-    } else if ((mr & (mr - 1)) == 0) {
+    if ((tid & g.cthr) == g.cthr && (base & g.cout) == g.cout) cmul_acc(fr, fi, g.m[2], g.m[3]);
+  }
 #pragma unroll
-      for (int b = 0; b < R; ++b) {
-        if (mr == (1u << b)) {
-          const double t = lr[b] * dr - li[b] * di;
-          li[b] = lr[b] * di + li[b] * dr;
-          lr[b] = t;
-        }
-      }
-    } else {
+  for (int b = 0; b < R; ++b) {
+    for (const int e = k + static_cast<int>((classes >> (8 * (b + 1))) & 0xff); k < e; ++k) {
+      const dev_op& g = run[k];
+      if ((tid & g.cthr) == g.cthr && (base & g.cout) == g.cout) cmul_acc(lr[b], li[b], g.m[2], g.m[3]);
+    }
+  }
+  for (; k < count; ++k) {
+    const dev_op& g = run[k];
+    if ((tid & g.cthr) != g.cthr || (base & g.cout) != g.cout) continue;
+    const uint32_t mr = g.creg;
+    const double dr = g.m[2], di = g.m[3];
 #pragma unroll
-      for (int i = 0; i < NR; ++i) {
-        if ((uint32_t(i) & mr) != mr) continue;
-        const double xr = double(a[i].x), xi = double(a[i].y);
-        a[i].x = static_cast<Real>(xr * dr - xi * di);
-        a[i].y = static_cast<Real>(xr * di + xi * dr);
-      }
+    for (int i = 0; i < NR; ++i) {
+      if ((uint32_t(i) & mr) != mr) continue;
+      double xr = double(a[i].x), xi = double(a[i].y);
+      cmul_acc(xr, xi, dr, di);
+      a[i].x = static_cast<Real>(xr);
+      a[i].y = static_cast<Real>(xi);
     }
   }
 #pragma unroll
   for (int i = 0; i < NR; ++i) {
     double pr = fr, pi = fi;
 #pragma unroll
-    for (int b = 0; b < R; ++b) {
-      if ((i >> b) & 1) {
-        const double t = pr * lr[b] - pi * li[b];
-        pi = pr * li[b] + pi * lr[b];
-        pr = t;
-      }
-    }
+    for (int b = 0; b < R; ++b)
+      if ((i >> b) & 1) cmul_acc(pr, pi, lr[b], li[b]);
     const double xr = double(a[i].x), xi = double(a[i].y);
     a[i].x = static_cast<Real>(xr * pr - xi * pi);
     a[i].y = static_cast<Real>(xr * pi + xi * pr);
@@ -295,7 +295,7 @@ __device__ __forceinline__ int apply_op(typename ctype<Real>::c* a, const dev_op
       break;
     }
     case op_code(OPK_PHASES, 0, true, 0):
-      apply_phase_run<Real, R>(a, &op + 1, static_cast<int>(op.run), tid, base);
+      apply_phase_run<Real, R>(a, &op + 1, static_cast<int>(op.run), op.dout, tid, base);
       return static_cast<int>(op.run);
 #define RBK_LAYER_CASE(FORM, FULL) \
     case op_code(OPK_LAYER, FORM, FULL, 0): \

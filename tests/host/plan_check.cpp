@@ -135,15 +135,28 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
                                    : op.kind == OPK_LAYER ? op_code(OPK_LAYER, op.real, op.dreg == (1u << R) - 1, 0)
                                    : op_code(op.kind, 0, true, 0);
           if (op.code != want_code || op.code >= kNumOpCodes || op.treg >= R) { std::fprintf(stderr, "bad dispatch code\n"); std::exit(8); }
-          if (op.kind == OPK_PHASES) {  // a run header: the run's gates follow in this phase, each a pure phase
+          if (op.kind == OPK_PHASES) {  // a run header: the run's gates follow, each a factor on the amplitudes whose bits are all one
             if (op.run < 2 || o + static_cast<int>(op.run) >= D.op_end) { std::fprintf(stderr, "bad phase run\n"); std::exit(14); }
+            // class sizes (no register bit, register bit 0 .. R-1; the rest: two or more register bits)
+            int bound[9], sum = 0;
+            for (int c = 0; c <= R; ++c) { sum += static_cast<int>((op.dout >> (8 * c)) & 0xff); bound[c] = sum; }
+            if (sum > static_cast<int>(op.run) || (op.dout >> (8 * (R + 1))) != 0) { std::fprintf(stderr, "bad phase run classes\n"); std::exit(18); }
             for (int k = 1; k <= static_cast<int>(op.run); ++k) {
               const dev_op& g = P.ops[o + k];
-              if (!(g.kind == OPK_NEG || (g.kind == OPK_DIAG && g.diag_one && g.m[0] == 1.0 && g.m[1] == 0.0))) {
-                std::fprintf(stderr, "phase run holds a gate that is not a phase\n");
+              int c = 0;
+              while (c <= R && k - 1 >= bound[c]) ++c;  // the class member k - 1 belongs to
+              const int nr = __builtin_popcount(g.creg);
+              const bool ok_class = c == 0 ? nr == 0 : c <= R ? g.creg == (1u << (c - 1)) : nr >= 2;
+              if (g.kind != OPK_DIAG || g.dreg || g.dthr || g.dout || g.creg >= (1u << R) || !ok_class) {
+                std::fprintf(stderr, "phase run holds a gate out of its form or class\n");
                 std::exit(15);
               }
+              if ((uint32_t(tid) & g.cthr) != g.cthr || (base & g.cout) != g.cout) continue;
+              const cplx d{g.m[2], g.m[3]};
+              for (int i = 0; i < NR; ++i)
+                if ((uint32_t(i) & g.creg) == g.creg) a[i] *= d;
             }
+            o += static_cast<int>(op.run);
             continue;
           }
           if (op.kind == OPK_LAYER) {  // a layer header: one uncontrolled 2x2 gate per bit of dreg follows, in bit order
