@@ -302,3 +302,78 @@ def test_observables_right_after_queued_swaps(pkg):
     ob = oracle.COracle(n)
     ob.apply(ops[:120])
     assert abs(a.inner_product(b) - o.inner_product(ob)) <= TOL64
+
+
+def layer_circuit(n, seed):
+    """Runs of uncontrolled single-qubit gates on subsets of a few neighbouring
+    qubits, in every matrix form the layer blocks take (H: real; U3: m00 real;
+    H then U3 on one qubit, which the planner merges: general), separated by
+    CNOTs inside the window, so that register phases hold layers over every
+    mask of register bits and mixed forms."""
+    rng = np.random.default_rng(seed)
+    ops = []
+    for _ in range(40):
+        lo = int(rng.integers(0, n - 6))
+        window = list(range(lo, lo + 6))
+        subset = [q for q in window if rng.random() < 0.6] or [window[0]]
+        for q in subset:
+            form = int(rng.integers(3))
+            angles = tuple(float(x) for x in rng.uniform(0.0, 2.0 * np.pi, size=3))
+            if form == 0:
+                ops.append(("H", (q,), ()))
+            elif form == 1:
+                ops.append(("U3", (q,), angles))
+            else:
+                ops += [("H", (q,), ()), ("U3", (q,), angles)]
+        for _ in range(int(rng.integers(0, 3))):
+            c, t = (int(x) for x in rng.permutation(window)[:2])
+            ops.append(("CNOT", (c, t), ()))
+    return ops
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("budget", [4, 8, 0])
+def test_layer_blocks_every_mask_and_form(pkg, precision, budget):
+    n = 15
+    tol = TOL64 if precision == 0 else TOL32
+    ops = layer_circuit(n, 100 + budget)
+    init = random_state(n, 11)
+    s, o = run_both(pkg, n, ops, init=init, precision=precision, budget=budget)
+    assert np.abs(s.amplitudes().astype(np.complex128) - o.amplitudes()).max() <= tol
+    s.close()
+
+
+def phase_run_circuit(n, seed):
+    """Long runs of phase gates (controlled phases U m j k, CZ, Z, U1) whose
+    bits fall on register bits, thread bits and bits outside the tile, in every
+    combination, between dense layers; every accumulator class of a phase run
+    is exercised."""
+    rng = np.random.default_rng(seed)
+    ops = [("H", (q,), ()) for q in range(n)]
+    for _ in range(6):
+        for _ in range(60):
+            a, b = (int(x) for x in rng.permutation(n)[:2])
+            kind = int(rng.integers(4))
+            if kind == 0:
+                k = int(rng.integers(1, n + 1))
+                ops.append(("U", (a, b), (k if rng.random() < 0.7 else -k,)))
+            elif kind == 1:
+                ops.append(("CZ", (a, b), ()))
+            elif kind == 2:
+                ops.append(("Z", (a,), ()))
+            else:
+                ops.append(("U1", (a,), (float(rng.uniform(0.0, 2.0 * np.pi)),)))
+        for q in rng.permutation(n)[:5]:
+            ops.append(("U3", (int(q),), tuple(float(x) for x in rng.uniform(0.0, 2.0 * np.pi, size=3))))
+    return ops
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("n", [13, 18])
+def test_phase_runs_every_accumulator_class(pkg, precision, n):
+    tol = TOL64 if precision == 0 else TOL32
+    ops = phase_run_circuit(n, 200 + n)
+    init = random_state(n, 12)
+    s, o = run_both(pkg, n, ops, init=init, precision=precision)
+    assert np.abs(s.amplitudes().astype(np.complex128) - o.amplitudes()).max() <= tol
+    s.close()
