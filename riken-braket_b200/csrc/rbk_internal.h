@@ -161,7 +161,8 @@ struct dev_pass {
   uint8_t run_dst[16];
   uint8_t num_phases;
   uint8_t direct_load;   // phase 0's layout reads HBM coalesced: load straight into registers
-  uint8_t direct_store;  // the last phase's write layout is coalesced: store straight from registers
+                         // (1: 16-byte vectors; 2: 8-byte complex<float> amplitudes, lanes on HBM bits 0-4)
+  uint8_t direct_store;  // the last phase's write layout is coalesced: store straight from registers (modes as above)
   uint8_t pad[4];
   dev_hbm_layout load, store;
   dev_phase phases[kMaxPhases];

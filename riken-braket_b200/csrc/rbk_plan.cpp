@@ -234,10 +234,11 @@ std::vector<phase_build> phases_by_dag(const std::vector<pop>& ops, const int* t
 // A gate folds when no later kept op of the phase touches its target or acts
 // non-diagonally on its control, and no later folded gate is controlled by its
 // target (so every folded gate reads its control before any fold moved it and
-// their contributions add up).  direct_store: the phase stores straight to HBM
-// and the contributions are physical offsets (store layout); for complex<float>
-// the 16-byte pair (register bit 0) must then stay out of the folds.
-void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_end, bool direct_store)
+// their contributions add up).  direct_store (the store's mode, 0 when the
+// phase writes to shared memory): the phase stores straight to HBM and the
+// contributions are physical offsets (store layout); for complex<float> in
+// 16-byte vectors (mode 1) the pair (register bit 0) must then stay out of the folds.
+void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_end, int direct_store)
 {
   const int begin = dp.op_begin, count = op_end - begin;
   std::vector<char> folded(static_cast<size_t>(count), 0);
@@ -252,7 +253,7 @@ void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op
       // a lane-bit control would split a warp's direct HBM store; shared-memory writes take it
       ok = nctl <= 1 && (d.cthr == 0 || !direct_store || __builtin_ctz(d.cthr) >= 5) &&
            !((later_target | later_diag | later_fold_ctl) & t) && !(later_target & d.creg);
-      if (ok && direct_store && p.vbits) ok = d.treg != 0 && !(d.creg & 1u);
+      if (ok && direct_store == 1 && p.vbits) ok = d.treg != 0 && !(d.creg & 1u);
       if (ok && d.cout) ok = conditional < kMaxFolds;
     }
     if (ok) {
@@ -477,16 +478,41 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
   for (size_t ph = 0; ph < phases.size(); ++ph) {
     auto& pb = phases[ph];
     const bool first = ph == 0, last = ph + 1 == phases.size();
-    // Bits the fill should keep out of (or bring into) the registers so that
-    // the first phase can load and the last phase can store straight from HBM.
+    // Direct HBM access modes of the first phase's load and the last phase's
+    // store.  Mode 1: 16-byte vectors, lanes on HBM bits lane0 .. lane0+4 (a
+    // warp touches one 512-byte run) and, for c64, the amplitude pair bit
+    // (HBM bit 0) on register bit 0.  Mode 2 (c64 only): 8-byte amplitudes,
+    // lanes on HBM bits 0..4 (256-byte runs), for phases whose gates act on the
+    // pair bit or leave no register for it.  map[x]: tile bit at HBM bit x
+    // (identity for the load; for the store, after the pass's relabelling).
+    int identity[16];
+    for (int b = 0; b < 16; ++b) identity[b] = b;
+    auto lanes_of = [&](int mode, const int* map) {
+      std::vector<int> l;
+      const int first_lane = mode == 2 ? 0 : lane0;
+      for (int x = 0; x < 5; ++x) l.push_back(map[first_lane + x]);
+      return l;
+    };
+    auto mode_for = [&](const int* map) {
+      auto off = [&](const std::vector<int>& bits) {
+        for (int b : bits) if (contains(pb.reg, b)) return false;
+        return true;
+      };
+      if (off(lanes_of(1, map)) && (!p.vbits || contains(pb.reg, map[0]) || static_cast<int>(pb.reg.size()) < R)) return 1;
+      if (p.vbits && off(lanes_of(2, map))) return 2;
+      return 0;
+    };
+    const int lmode = first ? mode_for(identity) : 0;
+    const int smode = last ? mode_for(relabel_from) : 0;
+    // Bits the fill should keep out of (or bring into) the registers for those modes.
     std::vector<int> keep_out, bring_in;
-    if (first) {
-      for (int l = 0; l < 5; ++l) keep_out.push_back(lane0 + l);
-      if (p.vbits) bring_in.push_back(0);
+    if (lmode) {
+      for (int b : lanes_of(lmode, identity)) keep_out.push_back(b);
+      if (p.vbits && lmode == 1) bring_in.push_back(0);
     }
-    if (last) {
-      for (int l = 0; l < 5; ++l) keep_out.push_back(relabel_from[lane0 + l]);
-      if (p.vbits) bring_in.push_back(relabel_from[0]);
+    if (smode) {
+      for (int b : lanes_of(smode, relabel_from)) keep_out.push_back(b);
+      if (p.vbits && smode == 1) bring_in.push_back(relabel_from[0]);
     }
     for (int b : bring_in)
       if (!contains(pb.reg, b) && !contains(keep_out, b) && static_cast<int>(pb.reg.size()) < R) pb.reg.push_back(b);
@@ -495,18 +521,16 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     for (int b = K - 1; b >= 0 && static_cast<int>(pb.reg.size()) < R; --b)
       if (!contains(pb.reg, b)) pb.reg.push_back(b);
 
-    bool dl = false, ds = false;
-    if (first) {
-      dl = !p.vbits || contains(pb.reg, 0);
-      for (int l = 0; l < 5; ++l) dl = dl && !contains(pb.reg, lane0 + l);
-    }
-    if (last) {
-      ds = !p.vbits || contains(pb.reg, relabel_from[0]);
-      for (int l = 0; l < 5; ++l) ds = ds && !contains(pb.reg, relabel_from[lane0 + l]);
-      if (dl && ds) {  // one layout must serve both: only when the lanes (and the c64 pair bit) keep their place
-        for (int l = 0; l < 5; ++l) ds = ds && relabel_from[lane0 + l] == lane0 + l;
-        if (p.vbits) ds = ds && relabel_from[0] == 0;
-      }
+    auto holds = [&](int mode, const int* map) {
+      if (!mode) return false;
+      for (int b : lanes_of(mode, map)) if (contains(pb.reg, b)) return false;
+      return !(p.vbits && mode == 1) || contains(pb.reg, map[0]);
+    };
+    bool dl = holds(lmode, identity), ds = holds(smode, relabel_from);
+    if (dl && ds) {  // one layout must serve both: the same mode, with its lanes (and the c64 pair bit) in place
+      ds = lmode == smode;
+      for (int x = 0; x < 5 && ds; ++x) ds = lanes_of(lmode, identity)[x] == lanes_of(smode, relabel_from)[x];
+      if (ds && p.vbits && lmode == 1) ds = relabel_from[0] == 0;
     }
     std::vector<int> thr;
     for (int b = 0; b < K; ++b) if (!contains(pb.reg, b)) thr.push_back(b);
@@ -529,18 +553,17 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
       for (int b : thr) if (!contains(lanes, b)) o.push_back(b);
       thr = o;
     };
-    if (dl) lanes_first({lane0, lane0 + 1, lane0 + 2, lane0 + 3, lane0 + 4});
-    else if (ds) lanes_first({relabel_from[lane0], relabel_from[lane0 + 1], relabel_from[lane0 + 2],
-                              relabel_from[lane0 + 3], relabel_from[lane0 + 4]});
+    if (dl) lanes_first(lanes_of(lmode, identity));
+    else if (ds) lanes_first(lanes_of(smode, relabel_from));
     else order_thread_bits(thr, p.vbits, last ? relabel_to : nullptr);
-    // c64 vectors: register index bit 0 must be the amplitude pair bit.
-    if (p.vbits && (dl || ds)) {
-      const int want = dl ? 0 : relabel_from[0];
+    // c64 16-byte vectors: register index bit 0 must be the amplitude pair bit.
+    if (p.vbits && ((dl && lmode == 1) || (ds && smode == 1))) {
+      const int want = (dl && lmode == 1) ? 0 : relabel_from[0];
       auto it = std::find(pb.reg.begin(), pb.reg.end(), want);
       std::iter_swap(pb.reg.begin(), it);
     }
-    if (first) out.direct_load = dl ? 1 : 0;
-    if (last) out.direct_store = ds ? 1 : 0;
+    if (first) out.direct_load = static_cast<uint8_t>(dl ? lmode : 0);
+    if (last) out.direct_store = static_cast<uint8_t>(ds ? smode : 0);
 
     dev_phase& dp = out.phases[ph];
     int reg_index[64], thr_index[64];
@@ -624,7 +647,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
              : (d.kind == OPK_X || d.kind == OPK_Y) ? op_code(d.kind, 0, true, d.treg)
              : op_code(d.kind, 0, true, 0);
     }
-    if (p.fold_x) fold_trailing_x(p, out, dp, op_index, last && ds);
+    if (p.fold_x) fold_trailing_x(p, out, dp, op_index, last && ds ? smode : 0);
     if (p.phase_runs) group_phase_runs(p, out, dp, op_index, headers_left);
     if (p.layers) group_layers(p, out, dp, op_index, headers_left);
     dp.op_end = static_cast<uint16_t>(op_index);

@@ -399,13 +399,16 @@ __device__ __forceinline__ void apply_folds(const dev_phase& ph, uint64_t base, 
 }
 
 // One tile through the pass's phases, ending with the tile stored to HBM.
-// from_hbm: phase 0 loads its registers straight from HBM (the pass's direct
-// load); otherwise the tile is already in `tile` and visible to every thread.
+// load_mode: phase 0 loads its registers straight from HBM (the pass's direct
+// load: 1 in 16-byte vectors, 2 in 8-byte complex<float> amplitudes); 0: the
+// tile is already in `tile` and visible to every thread.  The pass's
+// direct_store gives the last phase's store the same way.
 // The caller synchronises before `tile` is reused.
 template <typename Real, int K, int R>
 __device__ __forceinline__ void tile_phases(typename ctype<Real>::c* __restrict__ state, const dev_pass& P,
-                                            typename ctype<Real>::c* tile, uint64_t base, uint32_t tid, bool from_hbm)
+                                            typename ctype<Real>::c* tile, uint64_t base, uint32_t tid, int load_mode)
 {
+  const bool from_hbm = load_mode != 0;
   using C = typename ctype<Real>::c;
   using V = typename ctype<Real>::v16;
   using PT = precision_traits<Real>;
@@ -422,12 +425,23 @@ __device__ __forceinline__ void tile_phases(typename ctype<Real>::c* __restrict_
       uint64_t rphys[R];
 #pragma unroll
       for (int b = 0; b < R; ++b) rphys[b] = P.load.rphys[b];
+      if (sizeof(Real) == 4 && load_mode == 2) {
+        const C* src = state;
 #pragma unroll
-      for (int i = 0; i < NR; i += VEC) {
-        uint64_t phys = tphys;
+        for (int i = 0; i < NR; ++i) {
+          uint64_t phys = tphys;
 #pragma unroll
-        for (int b = VB; b < R; ++b) if (i & (1 << b)) phys |= rphys[b];
-        vec_io<Real>::unpack(__ldcs(gsrc + (phys >> VB)), &a[i]);
+          for (int b = 0; b < R; ++b) if (i & (1 << b)) phys |= rphys[b];
+          a[i] = __ldcs(src + phys);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < NR; i += VEC) {
+          uint64_t phys = tphys;
+#pragma unroll
+          for (int b = VB; b < R; ++b) if (i & (1 << b)) phys |= rphys[b];
+          vec_io<Real>::unpack(__ldcs(gsrc + (phys >> VB)), &a[i]);
+        }
       }
     } else {
       const uint32_t ts = ph.tslot_lo[tid & 15] ^ ph.tslot_hi[tid >> 4];
@@ -457,12 +471,23 @@ __device__ __forceinline__ void tile_phases(typename ctype<Real>::c* __restrict_
 #pragma unroll
       for (int b = 0; b < R; ++b) rphys[b] = P.store.rphys[b];
       apply_folds<R>(ph, base, tid, tphys, rphys);
+      if (sizeof(Real) == 4 && P.direct_store == 2) {
+        C* dst = state;
 #pragma unroll
-      for (int i = 0; i < NR; i += VEC) {
-        uint64_t phys = tphys;
+        for (int i = 0; i < NR; ++i) {
+          uint64_t phys = tphys;
 #pragma unroll
-        for (int b = VB; b < R; ++b) if (i & (1 << b)) phys ^= rphys[b];
-        __stcs(gdst + (phys >> VB), vec_io<Real>::pack(&a[i]));
+          for (int b = 0; b < R; ++b) if (i & (1 << b)) phys ^= rphys[b];
+          __stcs(dst + phys, a[i]);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < NR; i += VEC) {
+          uint64_t phys = tphys;
+#pragma unroll
+          for (int b = VB; b < R; ++b) if (i & (1 << b)) phys ^= rphys[b];
+          __stcs(gdst + (phys >> VB), vec_io<Real>::pack(&a[i]));
+        }
       }
     } else {
       // Every thread has read this phase's layout from `tile` (a phase that
@@ -513,7 +538,7 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
       tile_copy<Real, K, T, 0>(state, P, tile, base, tid);
       __syncthreads();
     }
-    tile_phases<Real, K, R>(state, P, tile, base, tid, P.direct_load != 0);
+    tile_phases<Real, K, R>(state, P, tile, base, tid, P.direct_load);
   } else {
     uint64_t t = blockIdx.x;
     if (t < num_tiles) tile_copy<Real, K, T, 2>(state, P, tile, tile_base(P, t), tid);
@@ -525,7 +550,7 @@ tile_pass_kernel(typename ctype<Real>::c* __restrict__ state, const __grid_const
       cp_async_commit();
       cp_async_wait<1>();  // this thread's copies of tile t have landed
       __syncthreads();     // ... and every other thread's
-      tile_phases<Real, K, R>(state, P, tile + (cur << K), tile_base(P, t), tid, false);
+      tile_phases<Real, K, R>(state, P, tile + (cur << K), tile_base(P, t), tid, 0);
       __syncthreads();
       cur ^= 1u;
     }

@@ -71,22 +71,34 @@ static void apply_folds(const dev_phase& D, uint64_t base, int tid, int R, uint6
 // phase completes all threads' reads before any write, which is what the
 // kernel's barriers guarantee (including the one before the direct store of a
 // one-phase pass that also loaded straight from HBM).
-// The kernel moves complex<float> amplitudes as 16-byte pairs: a direct HBM
-// layout must put the pair bit (physical bit 0) on register bit 0 and nowhere else.
-static void check_pair_layout(const plan_params& p, const dev_hbm_layout& L)
+// Direct HBM layouts.  Mode 1 moves 16-byte vectors: complex<float> must have
+// the pair bit (physical bit 0) on register bit 0 and nowhere else, and the five
+// lanes on the next physical bits (one 512-byte run per warp).  Mode 2
+// (complex<float> only) moves 8-byte amplitudes with the lanes on physical bits
+// 0-4.  Lane l is thread bit l: its contribution is tphys_lo[1 << l] ^
+// tphys_lo[0] (l < 4), tphys_hi[1] ^ tphys_hi[0] (l = 4).
+static void check_direct_layout(const plan_params& p, const dev_hbm_layout& L, int mode)
 {
-  if (!p.vbits) return;
-  bool ok = L.rphys[0] == 1;
-  for (int b = 1; b < p.R; ++b) ok = ok && !(L.rphys[b] & 1);
-  for (int x = 0; x < 16; ++x) ok = ok && !(L.tphys_lo[x] & 1);
-  for (int x = 0; x < 32; ++x) ok = ok && !(L.tphys_hi[x] & 1);
-  if (!ok) { std::fprintf(stderr, "direct layout splits a 16-byte pair\n"); std::exit(10); }
+  if (mode != 1 && !(mode == 2 && p.vbits)) { std::fprintf(stderr, "bad direct mode\n"); std::exit(19); }
+  bool ok = true;
+  if (p.vbits && mode == 1) {
+    ok = L.rphys[0] == 1;
+    for (int b = 1; b < p.R; ++b) ok = ok && !(L.rphys[b] & 1);
+    for (int x = 0; x < 16; ++x) ok = ok && !((L.tphys_lo[x] ^ L.tphys_lo[0]) & 1);
+    for (int x = 0; x < 32; ++x) ok = ok && !((L.tphys_hi[x] ^ L.tphys_hi[0]) & 1);
+    if (!ok) { std::fprintf(stderr, "direct layout splits a 16-byte pair\n"); std::exit(10); }
+  }
+  const int lane0 = mode == 1 ? p.vbits : 0;
+  uint64_t lanes = 0;
+  for (int l = 0; l < 4; ++l) lanes |= L.tphys_lo[1 << l] ^ L.tphys_lo[0];
+  lanes |= L.tphys_hi[1] ^ L.tphys_hi[0];
+  if (lanes != (31ull << lane0)) { std::fprintf(stderr, "direct layout lanes are not one contiguous run\n"); std::exit(20); }
 }
 
 static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass& P)
 {
-  if (P.direct_load) check_pair_layout(p, P.load);
-  if (P.direct_store) check_pair_layout(p, P.store);
+  if (P.direct_load) check_direct_layout(p, P.load, P.direct_load);
+  if (P.direct_store) check_direct_layout(p, P.store, P.direct_store);
   const int K = p.K, R = p.R, T = K - R, NR = 1 << R, NT = 1 << T;
   const uint64_t blocks = 1ull << (p.n - K);
   std::vector<cplx> smem(1u << K);
