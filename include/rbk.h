@@ -250,6 +250,19 @@ int rbk_measure(rbk_state* s, uint64_t* outcome);
 /* M q: ket::gate::projective_measurement (ket/include/ket/gate/projective_measurement.hpp):
  * outcome 0/1 with probabilities p0/p1, the kept half scaled by p^(-1/2). */
 int rbk_projective_measurement(rbk_state* s, uint32_t qubit, int* outcome);
+/* The same three with the caller's random numbers.  ket's sampling functions take
+ * the caller's engine and draw from it with ket::utility::positive_random_value_upto,
+ * a uniform_real_distribution on [0, upper) (ket/include/ket/utility/
+ * positive_random_value_upto.hpp): draw(context, upper) must return such a value.
+ * It is called on the calling thread, once per event in order (generate_events.hpp:
+ * 18-48), once for measure (measure.hpp:16-46) and once for the projective
+ * measurement with upper = p0 + p1 (projective_measurement.hpp:154-186), so an
+ * engine shared with ket's CPU code advances exactly as it would there.  The state's
+ * own generator is not used. */
+typedef double (*rbk_uniform_fn)(void* context, double upper);
+int rbk_generate_events_with(rbk_state* s, int num_events, rbk_uniform_fn draw, void* context, uint64_t* events);
+int rbk_measure_with(rbk_state* s, rbk_uniform_fn draw, void* context, uint64_t* outcome);
+int rbk_projective_measurement_with(rbk_state* s, uint32_t qubit, rbk_uniform_fn draw, void* context, int* outcome);
 
 /* ---- adjoint gradient (no counterpart in the reference) --------------------
  * One gate of a parametrised circuit, in bra's terms.  qubits[0] is the target

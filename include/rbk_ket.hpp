@@ -21,9 +21,11 @@
  * types of ket are needed (<ket/qubit.hpp>, <ket/control.hpp>); include the
  * ket gate headers as well when the same translation unit also calls ket's
  * CPU implementation.  Errors throw rbk::error (ket itself only asserts;
- * bra's states throw).  Sampling and projective measurement keep bra's
- * semantics, with the state's own generator: call rbk_generate_events,
- * rbk_measure and rbk_projective_measurement on state.handle().
+ * bra's states throw).  Sampling (ket::ranges::generate_events, measure) and
+ * ket::gate::ranges::projective_measurement draw from the caller's engine as
+ * ket does, one std::uniform_real_distribution<double> value per draw, so an
+ * engine shared with ket's CPU code advances identically; unlike ket's
+ * generate_events, the state is left intact.
  *
  * C++14 or later.
  */
@@ -32,10 +34,12 @@
 
 #include <array>
 #include <cmath>
+#include <cstddef>
 #include <complex>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <random>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -54,6 +58,14 @@ struct b200 { };
 inline constexpr auto make_b200() noexcept -> b200 { return b200{}; }
 }  // namespace policy
 }  // namespace utility
+}  // namespace ket
+
+namespace ket {
+namespace gate {
+// ket/include/ket/gate/projective_measurement.hpp:29 defines it; the
+// declaration here lets this header name it without that header.
+enum class outcome : int;
+}  // namespace gate
 }  // namespace ket
 
 namespace rbk {
@@ -241,6 +253,15 @@ inline auto pauli(rbk_state* const state, char const letter, qubit_lists const& 
   std::string const paulis(lists.targets.size(), letter);
   check(rbk_pauli_string(state, paulis.c_str(), data(lists.targets), count(lists.targets), data(lists.controls),
                          count(lists.controls)));
+}
+
+// rbk_uniform_fn over a C++ engine: what ket::utility::positive_random_value_upto
+// draws (a uniform_real_distribution on [0, upper)).
+template <typename RandomNumberGenerator>
+inline double draw_upto(void* const engine, double const upper)
+{
+  std::uniform_real_distribution<double> distribution{0.0, upper};
+  return distribution(*static_cast<RandomNumberGenerator*>(engine));
 }
 
 inline auto exponential_pauli(rbk_state* const state, char const letter, double const phase, qubit_lists const& lists)
@@ -714,6 +735,19 @@ inline auto set(RBK_KET_POLICY, RBK_KET_STATE& state, ::ket::qubit<StateInteger,
   return state;
 }
 
+// ---- projective_measurement.hpp:154-186: outcome 0 when a draw on [0, p0 + p1)
+// from the caller's engine falls below p0; the kept half is scaled by p^(-1/2). ----
+template <typename Complex, typename RandomNumberGenerator, typename StateInteger, typename BitInteger>
+inline auto projective_measurement(RBK_KET_POLICY, RBK_KET_STATE& state, RandomNumberGenerator& random_number_generator,
+                                   ::ket::qubit<StateInteger, BitInteger> const qubit) -> ::ket::gate::outcome
+{
+  int one = 0;
+  ::rbk::check(rbk_projective_measurement_with(state.handle(), ::rbk::detail::bit(qubit),
+                                               &::rbk::detail::draw_upto<RandomNumberGenerator>,
+                                               static_cast<void*>(&random_number_generator), &one));
+  return static_cast< ::ket::gate::outcome>(one);
+}
+
 }  // namespace ranges
 }  // namespace gate
 
@@ -773,6 +807,29 @@ inline auto fidelity(RBK_KET_POLICY, RBK_KET_STATE const& state1, RBK_KET_STATE 
   double value = 0.0;
   ::rbk::check(rbk_fidelity(state1.handle(), state2.handle(), &value));
   return static_cast<typename Complex::value_type>(value);
+}
+
+// generate_events.hpp:18-48, 102-113: num_events basis-state indices drawn
+// from |a_i|^2 with the caller's engine, into result (cleared first).
+template <typename Complex, typename StateInteger, typename Allocator, typename RandomNumberGenerator>
+inline auto generate_events(RBK_KET_POLICY, std::vector<StateInteger, Allocator>& result, RBK_KET_STATE& state,
+                            int const num_events, RandomNumberGenerator& random_number_generator) -> void
+{
+  std::vector<std::uint64_t> events(static_cast<std::size_t>(num_events > 0 ? num_events : 0));
+  ::rbk::check(rbk_generate_events_with(state.handle(), num_events, &::rbk::detail::draw_upto<RandomNumberGenerator>,
+                                        static_cast<void*>(&random_number_generator), events.data()));
+  result.assign(events.begin(), events.end());
+}
+
+// measure.hpp:16-46, 56-66: one index drawn from |a_i|^2 with the caller's
+// engine; the state becomes that basis state.
+template <typename Complex, typename RandomNumberGenerator>
+inline auto measure(RBK_KET_POLICY, RBK_KET_STATE& state, RandomNumberGenerator& random_number_generator) -> std::ptrdiff_t
+{
+  std::uint64_t index = 0u;
+  ::rbk::check(rbk_measure_with(state.handle(), &::rbk::detail::draw_upto<RandomNumberGenerator>,
+                                static_cast<void*>(&random_number_generator), &index));
+  return static_cast<std::ptrdiff_t>(index);
 }
 
 }  // namespace ranges

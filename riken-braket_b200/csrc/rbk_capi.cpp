@@ -1554,13 +1554,15 @@ int prob_prefix(rbk_state* s, device_buffer& prefix, device_buffer& scratch, dou
   return RBK_OK;
 }
 
-int sample_indices(rbk_state* s, std::mt19937_64& g, int num, uint64_t* out)
+// draw(upper): one uniform value on [0, upper), taken in event order.
+template <typename Draw>
+int sample_indices(rbk_state* s, Draw&& draw, int num, uint64_t* out)
 {
   device_buffer prefix, scratch, rbuf;
   double total = 0;
   if (int rc = prob_prefix(s, prefix, scratch, &total)) return rc;
   std::vector<double> r(num);
-  for (auto& x : r) x = random_upto(g, total);
+  for (auto& x : r) x = draw(total);
   RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&rbuf.p), sizeof(double) * 2 * num));
   uint64_t* ev = reinterpret_cast<uint64_t*>(rbuf.p + num);
   RBK_CUDA(cudaMemcpyAsync(rbuf.p, r.data(), sizeof(double) * num, cudaMemcpyHostToDevice, s->stream));
@@ -1589,9 +1591,9 @@ extern "C" int rbk_generate_events(rbk_state* s, int num_events, int64_t seed, u
     if (int rc = check_state(s)) return rc;
     if (num_events < 0 || (num_events > 0 && !events)) return fail(RBK_ERR_INVALID, "bad event arguments");
     if (num_events == 0) return RBK_OK;
-    if (seed < 0) return sample_indices(s, s->rng, num_events, events);
+    if (seed < 0) return sample_indices(s, [&](double upper) { return random_upto(s->rng, upper); }, num_events, events);
     std::mt19937_64 fresh(static_cast<uint64_t>(seed));  // generate_events.hpp: a generator built from the seed
-    return sample_indices(s, fresh, num_events, events);
+    return sample_indices(s, [&](double upper) { return random_upto(fresh, upper); }, num_events, events);
   });
 }
 
@@ -1601,9 +1603,31 @@ extern "C" int rbk_measure(rbk_state* s, uint64_t* outcome)
     if (int rc = check_state(s)) return rc;
     if (!outcome) return fail(RBK_ERR_INVALID, "null output pointer");
     uint64_t idx = 0;
-    if (int rc = sample_indices(s, s->rng, 1, &idx)) return rc;
+    if (int rc = sample_indices(s, [&](double upper) { return random_upto(s->rng, upper); }, 1, &idx)) return rc;
     *outcome = idx;
     return rbk_state_reset(s, idx);  // measure.hpp: the state becomes |outcome>
+  });
+}
+
+extern "C" int rbk_generate_events_with(rbk_state* s, int num_events, rbk_uniform_fn draw, void* context, uint64_t* events)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (num_events < 0 || (num_events > 0 && !events) || !draw) return fail(RBK_ERR_INVALID, "bad event arguments");
+    if (num_events == 0) return RBK_OK;
+    return sample_indices(s, [&](double upper) { return draw(context, upper); }, num_events, events);
+  });
+}
+
+extern "C" int rbk_measure_with(rbk_state* s, rbk_uniform_fn draw, void* context, uint64_t* outcome)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!outcome || !draw) return fail(RBK_ERR_INVALID, "null output pointer or random source");
+    uint64_t idx = 0;
+    if (int rc = sample_indices(s, [&](double upper) { return draw(context, upper); }, 1, &idx)) return rc;
+    *outcome = idx;
+    return rbk_state_reset(s, idx);
   });
 }
 
@@ -1694,6 +1718,21 @@ int collapse(rbk_state* s, uint32_t q, int one, double p)
 }
 
 }  // namespace
+
+extern "C" int rbk_projective_measurement_with(rbk_state* s, uint32_t qubit, rbk_uniform_fn draw, void* context,
+                                               int* outcome)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    if (!outcome || !draw) return fail(RBK_ERR_INVALID, "null output pointer or random source");
+    if (qubit >= static_cast<uint32_t>(s->n)) return fail(RBK_ERR_INVALID, "qubit index out of range");
+    double p0 = 0, p1 = 0;
+    if (int rc = qubit_probabilities(s, qubit, &p0, &p1)) return rc;
+    const int one = draw(context, p0 + p1) < p0 ? 0 : 1;
+    *outcome = one;
+    return collapse(s, qubit, one, one ? p1 : p0);
+  });
+}
 
 extern "C" int rbk_x_rotation_half_pi(rbk_state* s, int adjoint, uint32_t target, const uint32_t* controls, int nc)
 {

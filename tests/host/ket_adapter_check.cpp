@@ -17,11 +17,13 @@
 #include <cstdlib>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <ket/all_spin_expectation_values.hpp>
 #include <ket/fidelity.hpp>
 #include <ket/gate/clear.hpp>
+#include <ket/gate/projective_measurement.hpp>
 #include <ket/gate/controlled_not.hpp>
 #include <ket/gate/controlled_phase_shift.hpp>
 #include <ket/gate/exponential_pauli_x.hpp>
@@ -42,7 +44,9 @@
 #include <ket/gate/toffoli.hpp>
 #include <ket/gate/x_rotation_half_pi.hpp>
 #include <ket/gate/y_rotation_half_pi.hpp>
+#include <ket/generate_events.hpp>
 #include <ket/inner_product.hpp>
+#include <ket/measure.hpp>
 #include <ket/spin_expectation_value.hpp>
 #include <ket/utility/loop_n.hpp>
 
@@ -152,6 +156,31 @@ bool run_case(unsigned const n, int const layers, int const mixed, double const 
   double const inner_err = std::abs(std::complex<double>(inner_got.real(), inner_got.imag()) - inner_want);
   double const fid_err = std::abs(double(ket::ranges::fidelity(policy_gpu, got, got2)) - fid_want);
 
+  // Sampling with the caller's engine (complex<double>: the same events as ket).
+  // ket's generate_events overwrites its input with prefix sums, so it gets a copy.
+  int sample_mismatches = -1;
+  double measured_err = 0.0;
+  if (std::is_same<Complex, std::complex<double>>::value) {
+    sample_mismatches = 0;
+    std::mt19937_64 engine_cpu(99u + n), engine_gpu(99u + n);
+    auto copy = want;
+    std::vector<std::uint64_t> events_cpu, events_gpu;
+    ket::ranges::generate_events(policy_cpu, events_cpu, copy, 64, engine_cpu);
+    ket::ranges::generate_events(policy_gpu, events_gpu, got, 64, engine_gpu);
+    sample_mismatches += events_cpu.size() == events_gpu.size() ? 0 : 1000;
+    for (std::size_t k = 0; k < std::min(events_cpu.size(), events_gpu.size()); ++k)
+      sample_mismatches += events_cpu[k] == events_gpu[k] ? 0 : 1;
+    auto const outcome_cpu = ket::gate::ranges::projective_measurement(policy_cpu, want, engine_cpu, qubit_t{1u});
+    auto const outcome_gpu = ket::gate::ranges::projective_measurement(policy_gpu, got, engine_gpu, qubit_t{1u});
+    sample_mismatches += outcome_cpu == outcome_gpu ? 0 : 1;
+    measured_err = max_error(got.amplitudes(), want);
+    auto measured2 = want2;
+    auto const index_cpu = ket::ranges::measure(policy_cpu, measured2, engine_cpu);
+    auto const index_gpu = ket::ranges::measure(policy_gpu, got2, engine_gpu);
+    sample_mismatches += index_cpu == index_gpu ? 0 : 1;
+    measured_err = std::max(measured_err, max_error(got2.amplitudes(), measured2));
+  }
+
   // clear / set, and a state built from host amplitudes
   ket::gate::ranges::clear(policy_cpu, want, qubit_t{0u});
   ket::gate::ranges::set(policy_cpu, want, qubit_t{n - 1u});
@@ -163,12 +192,12 @@ bool run_case(unsigned const n, int const layers, int const mixed, double const 
   rbk::device_state<Complex> loaded(host);
   double const load_err = max_error(loaded.amplitudes(), want2);
 
-  double const worst = std::max({amp_err, spin_err, inner_err, fid_err, project_err, load_err});
-  bool const ok = worst <= tol;
+  double const worst = std::max({amp_err, spin_err, inner_err, fid_err, project_err, load_err, measured_err});
+  bool const ok = worst <= tol && sample_mismatches <= 0;
   std::printf("{\"case\": \"%s\", \"qubits\": %u, \"layers\": %d, \"mixed_gates\": %d, \"max_amp_err\": %.3e, "
               "\"max_spin_err\": %.3e, \"inner_product_err\": %.3e, \"fidelity_err\": %.3e, \"clear_set_err\": %.3e, "
-              "\"upload_err\": %.3e, \"tol\": %.1e, \"ok\": %s}\n",
-              name, n, layers, mixed, amp_err, spin_err, inner_err, fid_err, project_err, load_err, tol,
+              "\"upload_err\": %.3e, \"measured_amp_err\": %.3e, \"sample_mismatches\": %d, \"tol\": %.1e, \"ok\": %s}\n",
+              name, n, layers, mixed, amp_err, spin_err, inner_err, fid_err, project_err, load_err, measured_err, sample_mismatches, tol,
               ok ? "true" : "false");
   std::fflush(stdout);
   return ok;

@@ -3,7 +3,9 @@
 The same ket program (tests/host/ket_adapter_check.cpp) runs with ket's
 sequential policy on a std::vector -- ket's own code -- and with the b200
 policy on an rbk::device_state; amplitudes and observables must agree to
-1e-12 (complex<double>) / 2e-5 (complex<float>).  The program is built by
+1e-12 (complex<double>) / 2e-5 (complex<float>), and events, measurement
+outcomes and projective-measurement outcomes drawn from equally seeded engines
+must be the same (complex<double>).  The program is built by
 `build()` into oracle/_ref where ket's headers are available.
 """
 import json
@@ -19,6 +21,8 @@ KET_INCLUDE = "/root/reference/ket/include"
 
 _HEADER_ONLY_TU = r"""
 #include <complex>
+#include <random>
+#include <vector>
 #include <ket/qubit.hpp>
 #include <ket/control.hpp>
 #include "rbk_ket.hpp"
@@ -59,7 +63,12 @@ void every_gate(rbk::device_state<Complex>& s)
   auto const spin = ket::ranges::spin_expectation_value(p, s, a);
   auto const ip = ket::ranges::inner_product(p, s, s);
   auto const f = ket::ranges::fidelity(p, s, s);
-  (void)spins; (void)spin; (void)ip; (void)f;
+  std::mt19937_64 engine{1u};
+  std::vector<std::uint64_t> events;
+  ket::ranges::generate_events(p, events, s, 4, engine);
+  auto const o = g::projective_measurement(p, s, engine, a);
+  auto const m = ket::ranges::measure(p, s, engine);
+  (void)spins; (void)spin; (void)ip; (void)f; (void)o; (void)m;
 }
 template void every_gate(rbk::device_state<std::complex<double>>&);
 template void every_gate(rbk::device_state<std::complex<float>>&);
