@@ -560,14 +560,34 @@ overlaps_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename 
   block_sum_store<2>(vals, 2, partials + (size_t(blockIdx.y) * gridDim.x + blockIdx.x) * 2);
 }
 
-// out[2y], out[2y+1] = sum over the partials of overlap y, in block order.
+// Sum of the (re, im) partials p[0..blocks) by one warp: lane l takes blocks
+// l, l + 32, ... in order, then a fixed butterfly adds the lanes.  The order is
+// the same on every run; the loads of a lane are independent, so the sum costs
+// a few L2 round trips instead of one per block.
+__device__ __forceinline__ double2 warp_sum_partials(const double* __restrict__ p, int blocks)
+{
+  const int lane = threadIdx.x & 31;
+  double re = 0, im = 0;
+  for (int b = lane; b < blocks; b += 32) {
+    re += p[2 * b];
+    im += p[2 * b + 1];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, o);
+    im += __shfl_xor_sync(0xffffffffu, im, o);
+  }
+  return make_double2(re, im);
+}
+
+// out[2y], out[2y+1] = sum over the partials of overlap y (one warp per overlap).
 __global__ void finish_overlaps_kernel(const double* __restrict__ partials, int blocks, double* __restrict__ out)
 {
-  if (threadIdx.x >= 2) return;
-  const double* p = partials + size_t(blockIdx.x) * blocks * 2 + threadIdx.x;
-  double acc = 0;
-  for (int b = 0; b < blocks; ++b) acc += p[2 * b];
-  out[2 * blockIdx.x + threadIdx.x] = acc;
+  const double2 v = warp_sum_partials(partials + size_t(blockIdx.x) * blocks * 2, blocks);
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = v.x;
+    out[2 * blockIdx.x + 1] = v.y;
+  }
 }
 
 size_t overlaps_partials_doubles() { return size_t(reduction_blocks()) * 2 * kMaxOverlaps; }
@@ -647,11 +667,11 @@ tile_overlaps_kernel(const typename ctype<Real>::c* __restrict__ lam, const type
 __global__ void finish_tile_overlaps_kernel(const double* __restrict__ partials, int blocks,
                                             const __grid_constant__ tile_overlap_set T, double* __restrict__ out)
 {
-  if (threadIdx.x >= 2) return;
-  const double* p = partials + size_t(blockIdx.x) * blocks * 2 + threadIdx.x;
-  double acc = 0;
-  for (int b = 0; b < blocks; ++b) acc += p[2 * b];
-  out[2 * T.spec[blockIdx.x].out_slot + threadIdx.x] = acc;
+  const double2 v = warp_sum_partials(partials + size_t(blockIdx.x) * blocks * 2, blocks);
+  if (threadIdx.x == 0) {
+    out[2 * T.spec[blockIdx.x].out_slot] = v.x;
+    out[2 * T.spec[blockIdx.x].out_slot + 1] = v.y;
+  }
 }
 
 size_t tile_overlaps_partials_doubles(int n, int K) { return (size_t(1) << (n > K ? n - K : 0)) * 2 * kMaxOverlaps; }
