@@ -11,7 +11,10 @@ DO MEASUREMENT (all spins) and its read-back, all inside the timed region.
 
 --impl reference times the reference's own CPU code (ket + bra fused gates,
 release flags -Ofast -fopenmp, all host cores) on a bounded sample of the
-same circuit: the first fusion blocks of the 30-qubit run.
+same circuit: its 4-qubit fusion blocks (4 U3 + 2 CNOT each), one reference
+pass per block, the same blocks the GPU arm's cpu_baseline leg times.  Both
+arms also report a circuit time: the GPU's measured, the reference's
+extrapolated from its mean block time to the circuit's 156 passes.
 
 Multi-GPU: the path does not shard in this tier, so --gpus N runs N
 independent replicas (one process per GPU, launched by torchrun).
@@ -139,6 +142,21 @@ def reference_blocks(ops):
     return blocks
 
 
+def sample_blocks(ops):
+    """The blocks both CPU legs time: the 4-qubit fusion blocks of the even
+    brick layers (each 4 U3 and 2 CNOT on 4 consecutive qubits), in circuit
+    order.  They share one structure, so a few of them give the same mean as
+    many; the circuit's other blocks hold 2-5 qubits and 2-7 gates."""
+    out = []
+    for b in reference_blocks(ops):
+        gates = [op for op in b if op[0] not in ("BEGIN FUSION", "END FUSION")]
+        qubits = {q for op in gates for q in op[1]}
+        kinds = sorted(op[0] for op in gates)
+        if len(qubits) == 4 and kinds == ["CNOT", "CNOT", "U3", "U3", "U3", "U3"]:
+            out.append(b)
+    return out
+
+
 class CpuReference:
     """The reference's own ket/bra code, release build (oracle/_ref/libketref_fast.so)."""
 
@@ -157,18 +175,21 @@ class CpuReference:
 
 
 def cpu_sample(ops, threads, budget_s, n=N_QUBITS):
-    """Times reference passes of the workload on the host until budget_s of CPU
-    time is spent.  Returns (passes, seconds, description)."""
+    """Times reference passes of the workload on the host, the blocks of
+    sample_blocks() in order (the ones the reference arm's timed steps start
+    with), until budget_s of CPU time is spent.  Returns (passes, seconds,
+    description)."""
     need = (16 << n) * 1.1
     if host_mem_available() < need:
         return None, None, f"host has {host_mem_available() / 2**30:.0f} GiB free, a {n}-qubit state needs {need / 2**30:.0f} GiB"
     ref = CpuReference(n, threads)
-    blocks = reference_blocks(ops)
+    blocks = sample_blocks(ops)
     done, secs = 0, 0.0
     while done < len(blocks) and secs < budget_s:
         secs += ref.run_blocks([blocks[done]])
         done += 1
-    desc = f"first {done} of {len(blocks)} reference passes (fusion blocks) of the {n}-qubit circuit"
+    desc = (f"first {done} of the {len(blocks)} 4-qubit fusion blocks (4 U3 + 2 CNOT) of the {n}-qubit circuit's "
+            f"even layers, one reference pass each")
     return done, secs, desc
 
 
@@ -266,17 +287,21 @@ def run_gpu(args):
         done, secs, desc = cpu_sample(ops, threads, budget_s=args.cpu_budget, n=N_QUBITS)
         if done:
             cpu = {"value": done * bytes_pass / secs / 1e9, "unit": "GB/s", "cores": threads, "kind": "reference",
-                   "sample": desc + f", {secs:.1f} s, reference release build (-Ofast -fopenmp)"}
+                   "sample": desc + f", {secs:.1f} s, reference release build (-Ofast -fopenmp)",
+                   "circuit_ms_extrapolated": secs / done * ref_passes * 1e3,
+                   "circuit_ms_basis": f"mean time of the sampled blocks x {ref_passes} reference passes (extrapolated)"}
         else:
             cpu = {"value": None, "unit": "GB/s", "cores": threads, "kind": "reference", "sample": desc}
 
     traffic = load_traffic()
+    desc_bytes = pkg.rbk.pass_descriptor_bytes()
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "depth": DEPTH, "fusion_k": FUSE_K, "seed": SEED,
                    "passes_per_step": passes_per_step, "reference_passes_per_step": ref_passes,
+                   "circuit_ms": ms_max / args.steps,
                    "bytes_per_pass": bytes_pass, "l2": "inputs larger than L2 (16 GiB state)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -284,8 +309,11 @@ def run_gpu(args):
                      "traffic": traffic.get("bytes_per_launch") if traffic else None,
                      "kernel": "rbk::tile_pass_kernel<double>"},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": int(e2e_passes * 12544),
-                "d2h_bytes_per_step": 8 * 3 * N_QUBITS,
+        "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": int(e2e_passes * desc_bytes),
+                "d2h_bytes_per_step": 8 * 3 * N_QUBITS, "circuit_ms": e2e_max / args.steps * 1e3,
+                "h2d_basis": f"{e2e_passes:g} fused passes x {desc_bytes} B pass descriptor (rbk_pass_descriptor_bytes), "
+                             "the kernel parameter block each pass launch carries; other launches' parameters "
+                             "(under 100 B each) are not counted",
                 "step": "reset |0..0>, gate calls through the C ABI, DO MEASUREMENT (all spins), read-back"},
         "gpu_launches": st["kernel_launches"],
         "clocks": clk,
@@ -314,9 +342,12 @@ def run_reference(args):
                                                              f"the 30-qubit state needs {need / 2**30:.0f} GiB"}))
         return
     ref = CpuReference(N_QUBITS, threads)
-    blocks = reference_blocks(ops)
+    blocks = sample_blocks(ops)
     per_step = max(1, args.ref_blocks_per_step)
-    pos = 0
+    # Warm-up steps take the blocks just before the sample's start (cyclically),
+    # so that the timed steps begin with its first block, as the GPU arm's
+    # cpu_baseline leg does.
+    pos = -args.warmup * per_step
 
     def step():
         nonlocal pos
@@ -328,13 +359,18 @@ def run_reference(args):
         step()
     secs = sum(step() for _ in range(args.steps))
     value = args.steps * per_step * bytes_pass / secs / 1e9
-    sample = (f"{per_step} reference pass(es) (fusion blocks, in circuit order) of the 30-qubit circuit per step; "
+    ref_passes = C.reference_passes(ops)
+    sample = (f"{per_step} reference pass(es) per step from the {len(blocks)} 4-qubit fusion blocks (4 U3 + 2 CNOT) "
+              f"of the 30-qubit circuit's even layers, in circuit order from the first; "
               f"reference release build (-Ofast -fopenmp), {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "depth": DEPTH, "fusion_k": FUSE_K, "seed": SEED},
+        "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "depth": DEPTH, "fusion_k": FUSE_K, "seed": SEED,
+                   "reference_passes_per_step": ref_passes,
+                   "circuit_ms_extrapolated": secs / (args.steps * per_step) * ref_passes * 1e3,
+                   "circuit_ms_basis": f"mean time of the timed blocks x {ref_passes} reference passes (extrapolated)"},
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -551,7 +587,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rbk", choices=["rbk", "reference"])
-    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU reference work for cpu_baseline")
+    ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of CPU reference work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-blocks-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=N_QUBITS, help="smaller cases for profiling only")

@@ -63,6 +63,12 @@ typedef struct rbk_stats {
 
 const char* rbk_last_error(void);
 int rbk_version(void);
+/* Bytes of the parameter block that one fused-pass launch carries from the
+ * host: the pass descriptor, passed by value as the kernel's constant
+ * parameter.  No reference counterpart (the reference has no device); it
+ * lets a caller account for the host->device bytes of a circuit, which are
+ * passes x this figure plus the smaller parameters of other launches. */
+int rbk_pass_descriptor_bytes(uint64_t* out);
 
 /* ---- state lifecycle ------------------------------------------------------
  * Replaces std::vector<complex> state creation in bra::nompi_state
@@ -341,18 +347,29 @@ int rbk_adjoint_destroy(rbk_adjoint_ctx* ctx);
 
 /* Pauli-string expectation value of a caller-owned device state, with no
  * device memory allocated.  No counterpart in the reference: it exists for
- * callers that cannot allocate when they need the value -- code in a CUDA
- * host callback, a process whose HBM another allocator has already reserved,
- * or a loop that must not take the device synchronisation of cudaMalloc /
- * cudaFree.  Same meaning and arguments as rbk_expectation_pauli, except:
- * device_amps points to 2^num_qubits amplitudes of the given precision in
- * logical order (e.g. rbk_state_canonicalize + rbk_state_device_pointer);
- * stream is a cudaStream_t (NULL: the default stream); out is a host pointer
- * to (re, im).  Its scratch is one fixed device array of about 10 KB, held by
- * every GPU that loads the library until exit and shared by all calls: calls
- * that overlap on the GPU race.  At most 64 groups of strings with distinct
- * X/Y positions (RBK_ERR_INVALID beyond).  The first call on a device looks up
- * the array's device address; make that first call before any stream capture. */
+ * callers that cannot allocate when they need the value -- a process whose
+ * HBM another allocator (a framework's caching allocator, a 128 GiB state)
+ * has already reserved in full, or a loop that must not take the device
+ * synchronisation of cudaMalloc / cudaFree.  It makes CUDA runtime calls
+ * (launches, a copy, stream queries), so it must not be called from a CUDA
+ * stream callback or host function.  Same meaning and arguments as
+ * rbk_expectation_pauli, except: device_amps points to 2^num_qubits
+ * amplitudes of the given precision in logical order (e.g.
+ * rbk_state_canonicalize + rbk_state_device_pointer); stream is a
+ * cudaStream_t (NULL: the legacy default stream); out is a host pointer to
+ * (re, im).  The call reads the amplitudes on `stream` only: the caller
+ * orders it after every write to them (for a library state,
+ * rbk_state_synchronize first, since the state's own stream does not order
+ * against other streams).  Its scratch is one fixed device array of about
+ * 10 KB, shared by all calls: calls that overlap on the GPU race.  The array
+ * takes device memory when the library's device code is loaded on a device
+ * (with CUDA's lazy loading, at the first launch or symbol lookup there), so
+ * on a device whose HBM will be reserved in full, make one call before that
+ * happens.  At most 64 groups of strings with distinct X/Y positions
+ * (RBK_ERR_INVALID beyond).  The first call on a device looks up the array's
+ * device address and keeps it for the process; make that first call before
+ * any stream capture, and do not use the function on a device after
+ * cudaDeviceReset of that device. */
 int rbk_expectation_pauli_noalloc(const void* device_amps, int num_qubits, int precision, int num_terms,
                                   const char* strings, const double* coeffs, double* out, void* stream);
 

@@ -415,6 +415,13 @@ extern "C" {
 const char* rbk_last_error(void) { return g_error.c_str(); }
 int rbk_version(void) { return 1; }
 
+int rbk_pass_descriptor_bytes(uint64_t* out)
+{
+  if (!out) return rbk::set_last_error(RBK_ERR_INVALID, "null pointer");
+  *out = sizeof(rbk::dev_pass);
+  return RBK_OK;
+}
+
 int rbk_state_create(int num_qubits, int precision, uint64_t initial_index, int device, rbk_state** out)
 {
   return guarded([&]() -> int {

@@ -2,13 +2,13 @@
 // expectation value of a caller-owned device state, allocating no memory.
 //
 // Some callers cannot allocate device memory at the time they need an
-// observable: code running in a CUDA host callback (no CUDA API call may
-// allocate there), a process whose HBM is already reserved in full by another
+// observable: a process whose HBM is already reserved in full by another
 // allocator (a 33-qubit complex<double> state alone is 128 GiB), or a loop
 // that must not hit the implicit device synchronisation of cudaMalloc /
 // cudaFree.  This entry point takes the amplitudes and the output from the
 // caller and keeps its scratch -- the per-block partial sums of the reduction
-// -- in a fixed file-scope device array, so it never allocates.
+// -- in a fixed file-scope device array, so it never allocates.  It does make
+// CUDA runtime calls, so a stream callback or host function cannot use it.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -27,14 +27,17 @@ namespace {
 
 // Scratch for one call: kNoAllocPartials doubles of per-block partial sums
 // (rbk::reduction_blocks() blocks x 2) and kNoAllocGroups (re, im) results,
-// one per group of Pauli strings that share their X/Y positions.  About 10 KB,
-// held by every device that loads the library until the process exits.
+// one per group of Pauli strings that share their X/Y positions.  About 10 KB
+// on every device where this library's device code has been loaded (at the
+// first launch or symbol lookup on that device under lazy loading), until the
+// process exits.
 constexpr int kNoAllocPartials = 2 * 148 * 4;
 constexpr int kNoAllocGroups = 64;
 __device__ __align__(256) double g_noalloc_scratch[kNoAllocPartials + 2 * kNoAllocGroups];
 
 // Device address of g_noalloc_scratch for each device, looked up once per
-// device by the first call made with that device current.
+// device by the first call made with that device current.  A cudaDeviceReset
+// unloads the module, so the address is not valid after one.
 double* g_scratch_ptr[64] = {};
 
 int noalloc_fail(int code, const std::string& msg) { return rbk::set_last_error(code, msg.c_str()); }

@@ -43,6 +43,7 @@ _U64 = ctypes.c_uint64
 _SIGNATURES = {
     "rbk_last_error": ([], ctypes.c_char_p),
     "rbk_version": ([], _I),
+    "rbk_pass_descriptor_bytes": ([ctypes.POINTER(_U64)], _I),
     "rbk_state_create": ([_I, _I, _U64, _I, ctypes.POINTER(_P)], _I),
     "rbk_state_destroy": ([_P], _I),
     "rbk_state_num_qubits": ([_P, ctypes.POINTER(_I)], _I),
@@ -119,6 +120,13 @@ def lib():
             f.restype = res
         _lib = L
     return _lib
+
+
+def pass_descriptor_bytes():
+    """Bytes of the parameter block one fused-pass launch carries from the host."""
+    v = _U64()
+    _check(lib().rbk_pass_descriptor_bytes(ctypes.byref(v)))
+    return v.value
 
 
 def _check(rc):

@@ -9,7 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from __graft_entry__ import load_package  # noqa: E402
+from __graft_entry__ import REFERENCE, load_package  # noqa: E402,F401  (REFERENCE: reference tree root)
 
 
 def pytest_configure(config):

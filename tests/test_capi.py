@@ -34,6 +34,13 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_pass_descriptor_bytes(pkg):
+    """The fused pass's by-value parameter block fits CUDA's 32 KB kernel
+    parameter limit (bench.py counts it as the host->device bytes of a pass)."""
+    b = pkg.rbk.pass_descriptor_bytes()
+    assert 16384 <= b <= 32764
+
+
 def test_no_gpu_is_a_clean_error(pkg):
     try:
         import torch

@@ -17,7 +17,9 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BINARY = os.path.join(ROOT, "oracle", "_ref", "ket_adapter_check")
-KET_INCLUDE = "/root/reference/ket/include"
+from conftest import REFERENCE  # noqa: E402
+
+KET_INCLUDE = os.path.join(REFERENCE, "ket", "include")
 
 _HEADER_ONLY_TU = r"""
 #include <complex>

@@ -10,12 +10,12 @@ import pytest
 
 import bra_ref
 import oracle
-from conftest import ROOT
+from conftest import REFERENCE, ROOT
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 PROGRAMS = sorted(glob.glob(os.path.join(GOLDEN, "qcx", "*.qcx")))
 REF_BUILT = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libketref.so"))
-REF_SAMPLES = "/root/reference/bra/qcx"
+REF_SAMPLES = os.path.join(REFERENCE, "bra", "qcx")
 FIELDS = ("op", "kind", "line", "circuit", "targets", "controls", "params", "text")
 
 
