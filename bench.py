@@ -143,9 +143,8 @@ def reference_blocks(ops):
 
 
 def sample_blocks(ops):
-    """The blocks both CPU legs time: the 4-qubit fusion blocks of the even
-    brick layers (each 4 U3 and 2 CNOT on 4 consecutive qubits), in circuit
-    order.  They share one structure, so a few of them give the same mean as
+    """The blocks both CPU legs time: the 4-qubit fusion blocks of the brick
+    layers (each 4 U3 and 2 CNOT on 4 consecutive qubits), in circuit order.  They share one structure, so a few of them give the same mean as
     many; the circuit's other blocks hold 2-5 qubits and 2-7 gates."""
     out = []
     for b in reference_blocks(ops):
@@ -188,8 +187,8 @@ def cpu_sample(ops, threads, budget_s, n=N_QUBITS):
     while done < len(blocks) and secs < budget_s:
         secs += ref.run_blocks([blocks[done]])
         done += 1
-    desc = (f"first {done} of the {len(blocks)} 4-qubit fusion blocks (4 U3 + 2 CNOT) of the {n}-qubit circuit's "
-            f"even layers, one reference pass each")
+    desc = (f"first {done} of the {len(blocks)} 4-qubit fusion blocks (4 U3 + 2 CNOT) of the {n}-qubit circuit, "
+            f"one reference pass each")
     return done, secs, desc
 
 
@@ -361,7 +360,7 @@ def run_reference(args):
     value = args.steps * per_step * bytes_pass / secs / 1e9
     ref_passes = C.reference_passes(ops)
     sample = (f"{per_step} reference pass(es) per step from the {len(blocks)} 4-qubit fusion blocks (4 U3 + 2 CNOT) "
-              f"of the 30-qubit circuit's even layers, in circuit order from the first; "
+              f"of the 30-qubit circuit, in circuit order from the first; "
               f"reference release build (-Ofast -fopenmp), {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,

@@ -116,6 +116,21 @@ int rbk_state_device_ms(rbk_state* s, double* out);
  * done several qubits per pass). */
 int rbk_state_get_permutation(rbk_state* s, uint32_t* perm);
 int rbk_state_canonicalize(rbk_state* s);
+/* Declares the layout map without moving data: from now on logical qubit q
+ * is the one held by physical bit perm[q] of the amplitudes as they lie in
+ * device memory (queued gates run first, under the old map).  The logical
+ * state changes unless perm equals rbk_state_get_permutation's map.  This is
+ * what ket::mpi::permutate does to a qubit_permutation
+ * (ket/include/ket/mpi/qubit_permutation.hpp:242-252): the labels change,
+ * the local data stays.  perm must be a permutation of 0..n-1. */
+int rbk_state_set_permutation(rbk_state* s, const uint32_t* perm);
+/* Moves the data so that the layout map becomes perm (logical qubit q on
+ * physical bit perm[q]), in relabel-only passes; the logical state is
+ * unchanged.  rbk_state_canonicalize is set_layout to the identity.  With
+ * perm = a ket::mpi::qubit_permutation's map, the device memory holds
+ * ket::mpi's local data order: amplitude i of the state at physical index
+ * permutate_bits(permutation, i) (qubit_permutation.hpp:470-491). */
+int rbk_state_set_layout(rbk_state* s, const uint32_t* perm);
 /* Device pointer to the amplitudes in physical order (after a flush). */
 int rbk_state_device_pointer(rbk_state* s, void** out);
 

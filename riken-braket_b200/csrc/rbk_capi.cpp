@@ -185,32 +185,33 @@ int flush(rbk_state* s)
   return RBK_OK;
 }
 
-int canonicalize(rbk_state* s)
+// Moves the data so that the layout map becomes `target` (logical qubit q on
+// physical bit target[q]).
+int move_layout(rbk_state* s, const std::vector<int>& target)
 {
   int rc = flush(s);
   if (rc) return rc;
-  bool identity = true;
-  for (int q = 0; q < s->n; ++q) identity = identity && s->perm[q] == q;
-  if (identity) return RBK_OK;
+  if (s->perm == target) return RBK_OK;
   device_guard g(s->device);
   if (s->n < tile_bits(s)) {
-    // Small states: swap qubits home one transposition at a time.
+    // Small states: move qubits to their targets one transposition at a time.
     for (int q = 0; q < s->n; ++q) {
-      while (s->perm[q] != q) {
-        const int other = s->inv[q];  // logical qubit sitting on physical bit q
+      while (s->perm[q] != target[q]) {
+        const int home = target[q];
+        const int other = s->inv[home];  // logical qubit sitting on q's target bit
         const int pq = s->perm[q];
-        // Swap physical bits pq and q with three controlled-X permutations.
+        // Swap physical bits pq and home with three controlled-X permutations.
         for (int step = 0; step < 3; ++step) {
           rbk::gate_rec r{};
           r.kind = rbk::OPK_X;
-          r.target = static_cast<uint8_t>(step == 1 ? pq : q);
-          r.cmask = 1ull << (step == 1 ? q : pq);
+          r.target = static_cast<uint8_t>(step == 1 ? pq : home);
+          r.cmask = 1ull << (step == 1 ? home : pq);
           const cudaError_t e = s->precision == RBK_C128 ? rbk::launch_gate<double>(s->amps, s->n, r, s->stream)
                                                         : rbk::launch_gate<float>(s->amps, s->n, r, s->stream);
           if (e != cudaSuccess) return cuda_fail(e, "swap launch");
           ++s->stats.kernel_launches;
         }
-        s->perm[q] = q; s->inv[q] = q;
+        s->perm[q] = home; s->inv[home] = q;
         s->perm[other] = pq; s->inv[pq] = other;
       }
     }
@@ -218,7 +219,7 @@ int canonicalize(rbk_state* s)
   }
   std::vector<rbk::dev_pass> passes;
   try {
-    rbk::plan_canonicalize(params_of(s), s->perm, s->inv, passes);
+    rbk::plan_layout(params_of(s), s->perm, s->inv, target, passes);
   } catch (std::exception const& ex) {
     return fail(RBK_ERR_STATE, std::string("planner: ") + ex.what());
   }
@@ -228,6 +229,28 @@ int canonicalize(rbk_state* s)
   if (rc) return rc;
   s->stats.relabel_passes += passes.size();
   RBK_CUDA(cudaEventRecord(s->ev_last, s->stream));
+  return RBK_OK;
+}
+
+int canonicalize(rbk_state* s)
+{
+  std::vector<int> identity(static_cast<size_t>(s->n));
+  for (int q = 0; q < s->n; ++q) identity[static_cast<size_t>(q)] = q;
+  return move_layout(s, identity);
+}
+
+// A layout map from the caller: a permutation of 0..n-1.
+int read_layout(const rbk_state* s, const uint32_t* perm, std::vector<int>& out)
+{
+  if (!perm) return fail(RBK_ERR_INVALID, "null permutation");
+  out.assign(static_cast<size_t>(s->n), -1);
+  std::vector<char> seen(static_cast<size_t>(s->n), 0);
+  for (int q = 0; q < s->n; ++q) {
+    if (perm[q] >= static_cast<uint32_t>(s->n) || seen[perm[q]])
+      return fail(RBK_ERR_INVALID, "not a permutation of the state's qubits");
+    seen[perm[q]] = 1;
+    out[static_cast<size_t>(q)] = static_cast<int>(perm[q]);
+  }
   return RBK_OK;
 }
 
@@ -645,6 +668,29 @@ int rbk_state_canonicalize(rbk_state* s)
   return guarded([&]() -> int {
     if (int rc = check_state(s)) return rc;
     return canonicalize(s);
+  });
+}
+
+int rbk_state_set_permutation(rbk_state* s, const uint32_t* perm)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    std::vector<int> map;
+    if (int rc = read_layout(s, perm, map)) return rc;
+    if (int rc = flush(s)) return rc;  // queued gates name logical qubits of the old map
+    s->perm = map;
+    for (int q = 0; q < s->n; ++q) s->inv[static_cast<size_t>(map[static_cast<size_t>(q)])] = q;
+    return RBK_OK;
+  });
+}
+
+int rbk_state_set_layout(rbk_state* s, const uint32_t* perm)
+{
+  return guarded([&]() -> int {
+    if (int rc = check_state(s)) return rc;
+    std::vector<int> map;
+    if (int rc = read_layout(s, perm, map)) return rc;
+    return move_layout(s, map);
   });
 }
 

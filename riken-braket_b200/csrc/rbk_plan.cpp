@@ -891,19 +891,21 @@ void plan_passes(const plan_params& p, const std::vector<hgate>& gates, std::vec
   }
 }
 
-void plan_canonicalize(const plan_params& p, std::vector<int>& perm, std::vector<int>& inv,
-                       std::vector<dev_pass>& out)
+void plan_layout(const plan_params& p, std::vector<int>& perm, std::vector<int>& inv, const std::vector<int>& target,
+                 std::vector<dev_pass>& out)
 {
   const uint64_t low_mask = bit(p.LOW) - 1;
   for (int guard = 0; guard < 4 * p.n + 4; ++guard) {
-    bool identity = true;
-    for (int q = 0; q < p.n; ++q) if (perm[q] != q) { identity = false; break; }
-    if (identity) return;
+    bool done = true;
+    for (int q = 0; q < p.n; ++q) if (perm[q] != target[q]) { done = false; break; }
+    if (done) return;
 
+    // Tile bits: the physical bits of as many misplaced qubits and of their
+    // homes as fit, then any others up to K.
     uint64_t tile = low_mask;
     for (int q = 0; q < p.n; ++q) {
-      if (perm[q] == q) continue;
-      const uint64_t need = bit(perm[q]) | bit(q);
+      if (perm[q] == target[q]) continue;
+      const uint64_t need = bit(perm[q]) | bit(target[q]);
       if (popc(tile | need) <= p.K) tile |= need;
     }
     for (int q = 0; q < p.n && popc(tile) < p.K; ++q) tile |= bit(q);
@@ -914,7 +916,7 @@ void plan_canonicalize(const plan_params& p, std::vector<int>& perm, std::vector
     std::vector<char> used(64, 0);
     std::vector<int> assign(p.K, -1);
     for (int b = 0; b < p.K; ++b) {
-      const int home = inv[tile_phys[b]];
+      const int home = target[inv[tile_phys[b]]];  // where the qubit on this tile bit belongs
       if ((tile & bit(home)) && !used[home]) { assign[b] = home; used[home] = 1; }
     }
     for (int b = 0; b < p.K; ++b) {
@@ -928,7 +930,15 @@ void plan_canonicalize(const plan_params& p, std::vector<int>& perm, std::vector
     out.emplace_back();
     build_pass(p, tile, std::vector<pop>{}, relabel_to, tile_phys, out.back());
   }
-  throw std::logic_error("planner: canonicalize did not converge");
+  throw std::logic_error("planner: layout change did not converge");
+}
+
+void plan_canonicalize(const plan_params& p, std::vector<int>& perm, std::vector<int>& inv,
+                       std::vector<dev_pass>& out)
+{
+  std::vector<int> identity(static_cast<size_t>(p.n));
+  for (int q = 0; q < p.n; ++q) identity[static_cast<size_t>(q)] = q;
+  plan_layout(p, perm, inv, identity, out);
 }
 
 }  // namespace rbk

@@ -42,7 +42,13 @@ struct plan_params {
 void plan_passes(const plan_params& p, const std::vector<hgate>& gates, std::vector<int>& perm,
                  std::vector<int>& inv, std::vector<dev_pass>& out);
 
-// Passes that only move data so that perm becomes the identity.
+// Passes that only move data so that perm becomes `target` (a permutation of
+// 0..n-1: logical qubit q on physical bit target[q]); the multi-qubit form of
+// ket::mpi's swap_permutated_local_qubits
+// (ket/include/ket/mpi/utility/detail/swap_permutated_local_qubits.hpp:26-81).
+void plan_layout(const plan_params& p, std::vector<int>& perm, std::vector<int>& inv, const std::vector<int>& target,
+                 std::vector<dev_pass>& out);
+// plan_layout to the identity.
 void plan_canonicalize(const plan_params& p, std::vector<int>& perm, std::vector<int>& inv,
                        std::vector<dev_pass>& out);
 

@@ -61,6 +61,8 @@ _SIGNATURES = {
     "rbk_state_device_ms": ([_P, ctypes.POINTER(_D)], _I),
     "rbk_state_get_permutation": ([_P, _U32P], _I),
     "rbk_state_canonicalize": ([_P], _I),
+    "rbk_state_set_permutation": ([_P, ctypes.POINTER(ctypes.c_uint32)], _I),
+    "rbk_state_set_layout": ([_P, ctypes.POINTER(ctypes.c_uint32)], _I),
     "rbk_state_device_pointer": ([_P, ctypes.POINTER(_P)], _I),
     "rbk_begin_fusion": ([_P], _I),
     "rbk_end_fusion": ([_P], _I),
@@ -228,6 +230,16 @@ class State:
 
     def canonicalize(self):
         _check(lib().rbk_state_canonicalize(self.h))
+
+    def set_permutation(self, perm):
+        """Declares the layout map (logical q on physical bit perm[q]) without moving data."""
+        arr = (ctypes.c_uint32 * self.n)(*[int(x) for x in perm])
+        _check(lib().rbk_state_set_permutation(self.h, arr))
+
+    def set_layout(self, perm):
+        """Moves the data so that the layout map becomes perm; the logical state is unchanged."""
+        arr = (ctypes.c_uint32 * self.n)(*[int(x) for x in perm])
+        _check(lib().rbk_state_set_layout(self.h, arr))
 
     def device_pointer(self):
         p = ctypes.c_void_p()

@@ -7,6 +7,7 @@
 // predicates, scatter back with the write positions, store).  The result,
 // read back through the final layout map, must equal the gates applied one by
 // one in logical order.  Test code only; built and run by tests/test_planner.py.
+#include <algorithm>
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
@@ -313,6 +314,14 @@ int main(int argc, char** argv)
       plan_passes(p, gates, perm, inv, passes);
       std::vector<cplx> st = init;
       for (const auto& P : passes) run_pass(st, p, P);
+      // A detour through a random layout, then home: both are data moves only.
+      std::vector<int> target(p.n);
+      for (int i = 0; i < p.n; ++i) target[i] = i;
+      std::shuffle(target.begin(), target.end(), rng);
+      std::vector<dev_pass> detour;
+      plan_layout(p, perm, inv, target, detour);
+      for (const auto& P : detour) run_pass(st, p, P);
+      if (perm != target) { std::printf("layout not reached\n"); ++failures; }
       std::vector<dev_pass> canon;
       plan_canonicalize(p, perm, inv, canon);
       for (const auto& P : canon) run_pass(st, p, P);
@@ -321,8 +330,8 @@ int main(int argc, char** argv)
       double err = 0, scale = 1;
       for (uint64_t i = 0; i < N; ++i) scale = std::max(scale, std::abs(want[i]));
       for (uint64_t i = 0; i < N; ++i) err = std::max(err, std::abs(st[i] - want[i]) / scale);
-      std::printf("prec=%d shape=%d seed=%d n=%d gates=%d budget=%d passes=%zu canon=%zu err=%.3e\n", prec, shape, seed, p.n, count,
-                  p.dense_budget, passes.size(), canon.size(), err);
+      std::printf("prec=%d shape=%d seed=%d n=%d gates=%d budget=%d passes=%zu detour=%zu canon=%zu err=%.3e\n", prec, shape, seed,
+                  p.n, count, p.dense_budget, passes.size(), detour.size(), canon.size(), err);
       if (!(err < 1e-12)) ++failures;
     }
   }

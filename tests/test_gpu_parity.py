@@ -207,6 +207,51 @@ def test_layout_map_swaps_and_canonicalize(pkg):
     np.testing.assert_array_equal(s.amplitudes(), before[src])
 
 
+def _permute_bits(perm, idx):
+    """Index whose bit perm[q] is bit q of idx (ket::mpi::permutate_bits)."""
+    out = np.zeros_like(idx)
+    for q, p in enumerate(perm):
+        out |= ((idx >> q) & 1) << p
+    return out
+
+
+@pytest.mark.parametrize("n,precision", [(9, 0), (18, 0), (18, 1)])
+def test_set_layout_and_set_permutation(pkg, n, precision):
+    """rbk_state_set_layout moves the data (the logical state stays the
+    oracle's); rbk_state_set_permutation relabels without moving it, so the
+    logical state becomes the physical data read under the new map."""
+    tol = TOL64 if precision == 0 else 2e-5
+    ops = pkg.circuits.random_circuit(n, 120, seed=31 + n)
+    s = pkg.State(n, precision)
+    s.upload(random_state(n, 5).astype(s.dtype))
+    s.apply(ops)
+    o = oracle.COracle(n)
+    o.set_amplitudes(random_state(n, 5).astype(s.dtype).astype(np.complex128))
+    o.apply(ops)
+    want = o.amplitudes()
+    rng = np.random.default_rng(n)
+    target = [int(x) for x in rng.permutation(n)]
+    s.set_layout(target)
+    assert s.permutation() == target
+    idx = np.arange(1 << n, dtype=np.int64)
+    phys = np.empty_like(want)
+    phys[_permute_bits(target, idx)] = want                    # the device memory now
+    # Declare the identity map: the logical state becomes the memory as it lies.
+    # (Reads bring the memory into logical order, so nothing is read before.)
+    s.set_permutation(list(range(n)))
+    assert np.abs(s.amplitudes() - phys).max() <= tol
+    # The memory is in identity order now; declaring `target` gives back the circuit's state.
+    s.set_permutation(target)
+    assert np.abs(s.amplitudes() - want).max() <= tol
+    # set_layout keeps the logical state.
+    s.set_layout(target[::-1])
+    assert s.permutation() == target[::-1]
+    assert np.abs(s.amplitudes() - want).max() <= tol
+    with pytest.raises(pkg.RbkError):
+        s.set_permutation([0] * n)
+    s.close()
+
+
 @pytest.mark.parametrize("n", [10, 14, 19])
 def test_observables_vs_oracle(pkg, n):
     ops = pkg.circuits.random_circuit(n, 150, seed=n)
