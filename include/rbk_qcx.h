@@ -16,9 +16,18 @@
  * +X/-X/+Y/-Y, EX/EY/EZ.., ESWAP, TOFFOLI, with "+" adjoints and C../Cn control
  * prefixes), M, CLEAR, SET, SHORBOX, BEGIN/END FUSION, BEGIN MEASUREMENT, DO
  * MEASUREMENT [p], DO AMPLITUDES [i ...], GENERATE EVENTS n seed, EXPECTATION
- * :PAULIS:<s> q..., INNERPROD / FIDELITY (k | ALL) [:PAULIS:<s> q...], PRINT /
+ * <operator> q..., INNERPROD / FIDELITY (k | ALL) [<operator> q...], PRINT /
  * PRINTLN of literals and built-in symbols (:RESULT, :OUTCOME, :OUTCOMES:i,
  * ...), EXIT.
+ * Operators are Pauli-string-space values (bra/include/bra/pauli_string_space.hpp:25-153):
+ * a :PAULIS:<s> literal, or a PAULISS variable (NAME or NAME:index) declared
+ * with VAR name PAULISS [size] and built with LET (bra/src/state.cpp:400-490):
+ * LET H := <pauliss>, LET H += <pauliss>, LET H -= <pauliss> (the strings of
+ * the right side, all of H's length, added or subtracted term by term), LET H
+ * *= <complex>, LET H /= <complex> (every coefficient; <complex> is
+ * :COMPLEX:<literal>, :COMPLEX, :I, :MINUS_I or :RESULT).  Variables belong
+ * to the circuit that declares them; an INNERPROD / FIDELITY operator is the
+ * running circuit's (circuit 0's for ALL).
  * Several circuits run as bra's nompi build runs them (bra/src/bra.cpp:299-760):
  * one state each, circuit 0 seeded with the given seed and circuit k >= 1 with
  * the k-th draw of std::mt19937_64(seed); each circuit runs until it finishes or
@@ -27,9 +36,10 @@
  * goes to :RESULT: <Psi_k|Psi_c> (c the running circuit, k the partner; circuit
  * 0 for ALL), with <Psi_k| H |Psi_c> when an operator is given, and the squared
  * modulus for FIDELITY.
- * Not supported (RBK_ERR_UNSUPPORTED naming the line): classical variables and
- * control flow (VAR, LET, @label, JUMP, JUMPIF, SEND, RECEIVE, BROADCAST,
- * GATHER, SCATTER), DEPOLARIZING, PERMUTATION, RANDOM PERMUTATION.
+ * Not supported (RBK_ERR_UNSUPPORTED naming the line): the rest of the
+ * classical layer -- INT / REAL / COMPLEX variables and LET on them, @label,
+ * JUMP, JUMPIF, SEND, RECEIVE, BROADCAST, GATHER, SCATTER, PRINT of variables
+ * -- DEPOLARIZING, PERMUTATION, RANDOM PERMUTATION.
  */
 #ifndef RBK_QCX_H_INCLUDED
 #define RBK_QCX_H_INCLUDED
@@ -59,13 +69,21 @@ enum {
   RBK_QCX_GENERATE_EVENTS = 6,  /* ints[0] = events, ints[1] = seed */
   RBK_QCX_EXIT = 7,
   RBK_QCX_PROJECTIVE = 8,       /* M t */
-  RBK_QCX_EXPECTATION = 9,      /* text = Pauli string, targets = operated qubits */
+  RBK_QCX_EXPECTATION = 9,      /* text = Pauli string, or with ints[1] = 1 the name of a PAULISS
+                                   variable (NAME or NAME:index); targets = operated qubits */
   RBK_QCX_PRINT = 10,           /* text = arguments separated by one space; ints[0] = 1 for PRINTLN */
   RBK_QCX_NOOP = 11,            /* I, IC, C..I: MPI-only identities */
   RBK_QCX_INNERPROD = 12,       /* ints[0] = partner circuit, RBK_QCX_ALL or RBK_QCX_NONE; text = Pauli
-                                   string (empty: no operator), targets = operated qubits */
-  RBK_QCX_FIDELITY = 13         /* as RBK_QCX_INNERPROD */
+                                   string (empty: no operator) or, with ints[1] = 1, a PAULISS variable
+                                   as for EXPECTATION; targets = operated qubits */
+  RBK_QCX_FIDELITY = 13,        /* as RBK_QCX_INNERPROD */
+  RBK_QCX_VAR = 14,             /* VAR name PAULISS [size]: text = name, ints[0] = size */
+  RBK_QCX_LET = 15              /* LET lhs op rhs on a PAULISS variable: text = "LHS RHS", ints[0] =
+                                   RBK_QCX_ASSIGN ... RBK_QCX_DIVIDE */
 };
+
+/* LET operations (bra/include/bra/state.hpp assign_operation_type). */
+enum { RBK_QCX_ASSIGN = 0, RBK_QCX_PLUS = 1, RBK_QCX_MINUS = 2, RBK_QCX_TIMES = 3, RBK_QCX_DIVIDE = 4 };
 
 /* Partner of INNERPROD / FIDELITY: every circuit (ALL), or none -- bra does
  * nothing for the running circuit's own index or a column that is neither a

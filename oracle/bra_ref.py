@@ -26,7 +26,8 @@ KG = dict(H=1, NOT=2, X=3, Y=4, Z=5, SWAP=6, SX=7, SX_ADJ=8, SY=9, SY_ADJ=10, SZ
           EX_ADJ=26, EY=27, EY_ADJ=28, EZ=29, EZ_ADJ=30, ESWAP=31, ESWAP_ADJ=32, TOFFOLI=33, CLEAR=34, SET=35,
           SHORBOX=36)
 OP = dict(GATE=1, BEGIN_FUSION=2, END_FUSION=3, MEASUREMENT=4, AMPLITUDES=5, GENERATE_EVENTS=6, EXIT=7,
-          PROJECTIVE=8, EXPECTATION=9, PRINT=10, NOOP=11, INNERPROD=12, FIDELITY=13)
+          PROJECTIVE=8, EXPECTATION=9, PRINT=10, NOOP=11, INNERPROD=12, FIDELITY=13, VAR=14, LET=15)
+LET_OPS = {":=": 0, "+=": 1, "-=": 2, "*=": 3, "/=": 4}
 ALL, NONE = -1, -2  # INNERPROD / FIDELITY partner: every circuit, or nothing to do
 
 CONSTANTS = {":REAL": 0.0, ":IMAG": 0.0, ":PI": math.pi, ":HALF_PI": math.pi / 2, ":TWO_PI": 2 * math.pi,
@@ -56,6 +57,15 @@ def _count(body, letter):
     if len(body) > 1 and body[1:].isdigit():
         return int(body[1:])
     return 0
+
+
+def _operator(tok):
+    """An operator column: (Pauli string, 0) for a :PAULIS:<s> literal,
+    (NAME[:index], 1) for a PAULISS variable."""
+    u = tok.upper()
+    if u.startswith(":PAULIS:"):
+        return u[len(":PAULIS:"):], 0
+    return u, 1
 
 
 def parse(text):
@@ -206,8 +216,14 @@ def parse_program(text):
                 partner = NONE if int(who) == state["circuit"] else int(who)
             else:
                 partner = ALL if who.upper() == "ALL" else NONE
-            pauli = cols[2][len(":PAULIS:"):].upper() if len(cols) >= 4 else ""
-            ins(m, line_no, ints=[partner, 0], text=pauli, targets=[qubit(t) for t in cols[3:]])
+            text, is_var = _operator(cols[2]) if len(cols) >= 4 else ("", 0)
+            ins(m, line_no, ints=[partner, is_var], text=text, targets=[qubit(t) for t in cols[3:]])
+        elif m == "VAR":
+            if cols[2].upper() != "PAULISS":
+                raise QcxError(f"line {line_no}: only PAULISS variables")
+            ins("VAR", line_no, text=cols[1].upper(), ints=[int(cols[3]) if len(cols) == 4 else 1, 0])
+        elif m == "LET":
+            ins("LET", line_no, text=cols[1].upper() + " " + cols[3].upper(), ints=[LET_OPS[cols[2]], 0])
         elif m == "DO":
             if word(1) == "MEASUREMENT":
                 ins("MEASUREMENT", line_no, ints=[int(cols[2]) if len(cols) == 3 else 3, 0])
@@ -219,8 +235,8 @@ def parse_program(text):
             ins("GENERATE_EVENTS", line_no, ints=[int(cols[2]), int(cols[3])])
             done = True
         elif m == "EXPECTATION":
-            pauli = cols[1][len(":PAULIS:"):].upper()
-            ins("EXPECTATION", line_no, text=pauli, targets=[qubit(t) for t in cols[2:]])
+            text, is_var = _operator(cols[1])
+            ins("EXPECTATION", line_no, text=text, ints=[0, is_var], targets=[qubit(t) for t in cols[2:]])
         elif m in ("PRINT", "PRINTLN"):
             ins("PRINT", line_no, text=" ".join(cols[1:]), ints=[int(m == "PRINTLN"), 0])
         elif m in ("U", "U+"):
@@ -328,9 +344,73 @@ class _MT64:
         return y & self.MASK
 
 
-def _overlap(a, b, ins):
-    """ket::inner_product(a, b[, P]) = <b| [P] |a> (squared modulus for FIDELITY) on the reference."""
-    v = a.inner_product_on(b, ins["text"], ins["targets"]) if ins["text"] else a.inner_product(b)
+# ---- PAULISS values (bra/include/bra/pauli_string_space.hpp:25-153; LET and
+# variable lookup as bra/src/state.cpp:400-490, :977-998): (num_qubits, {string: coeff}).
+
+def _new_space():
+    return [0, {"": 0j}]
+
+
+def _variable(c, ref):
+    name, _, idx = ref.partition(":")
+    if name not in c["vars"]:
+        raise QcxError(f"{name} is not a PAULISS variable")
+    return c["vars"][name][int(idx) if idx else 0]
+
+
+def _space_value(c, rhs):
+    if rhs.startswith(":PAULIS:"):
+        s = rhs[len(":PAULIS:"):]
+        return [len(s), {s: 1 + 0j}]
+    v = _variable(c, rhs)
+    return [v[0], dict(v[1])]
+
+
+def _complex_value(c, rhs):
+    fixed = {":COMPLEX": 0j, ":I": 1j, ":MINUS_I": -1j}
+    if rhs in fixed:
+        return fixed[rhs]
+    if rhs == ":RESULT":
+        return c["result"]
+    if rhs.startswith(":COMPLEX:"):
+        return complex(float(rhs[len(":COMPLEX:"):]), 0.0)
+    raise QcxError(f"unsupported complex value {rhs}")
+
+
+def _let(c, ins):
+    lhs_ref, rhs = ins["text"].split(" ")
+    lhs = _variable(c, lhs_ref)
+    op = ins["ints"][0]
+    if op == 0:
+        lhs[:] = _space_value(c, rhs)
+    elif op in (1, 2):
+        for s, v in _space_value(c, rhs)[1].items():
+            if len(s) != lhs[0]:
+                raise QcxError(f"{s} has the wrong length")
+            lhs[1][s] = lhs[1].get(s, 0j) + (v if op == 1 else -v)
+    else:
+        z = _complex_value(c, rhs)
+        for s in lhs[1]:
+            lhs[1][s] = lhs[1][s] * z if op == 3 else lhs[1][s] / z
+
+
+def _terms(c, ins):
+    """The operator of an instruction as [(string over the listed qubits, coefficient)]."""
+    if not ins["ints"][1]:
+        return [(ins["text"], 1 + 0j)]
+    nq, terms = _variable(c, ins["text"])
+    if nq != len(ins["targets"]):
+        raise QcxError("operator length differs from the number of qubits")
+    return list(terms.items())
+
+
+def _overlap(a, b, ins, owner):
+    """ket::inner_product(a, b[, P]) = <b| [P] |a> (squared modulus for FIDELITY) on the reference; the
+    operator is circuit owner's."""
+    if ins["text"]:
+        v = sum(w * a.inner_product_on(b, s, ins["targets"]) for s, w in _terms(owner, ins))
+    else:
+        v = a.inner_product(b)
     return complex(abs(v) ** 2, 0.0) if ins["op"] == OP["FIDELITY"] else v
 
 
@@ -386,7 +466,13 @@ def _run_circuit(c, n, out):
             c["outcomes"][q] = r.projective_measurement(q)
             c["last"] = q
         elif op == OP["EXPECTATION"]:
-            c["result"] = r.expectation_on(ins["text"], ins["targets"])
+            c["result"] = sum(w * r.expectation_on(s, ins["targets"]) for s, w in _terms(c, ins))
+        elif op == OP["VAR"]:
+            if ins["text"] in c["vars"]:
+                raise QcxError(f"variable {ins['text']} declared twice")
+            c["vars"][ins["text"]] = [_new_space() for _ in range(ins["ints"][0])]
+        elif op == OP["LET"]:
+            _let(c, ins)
         elif op in (OP["INNERPROD"], OP["FIDELITY"]):
             if ins["ints"][0] != NONE:
                 c["wait"] = ins
@@ -426,7 +512,7 @@ def run(text, seed=1, threads=1):
         r = oracle.KetRef(n, initial_index=init, threads=threads)
         r.seed(seed if k == 0 else draws())
         ctx.append(dict(r=r, code=[i for i in code if i["circuit"] == k], pc=0, outcomes=[-1] * n, last=0,
-                        result=0j, wait=None))
+                        result=0j, wait=None, vars={}))
     out = []
     while True:
         for c in ctx:
@@ -450,14 +536,14 @@ def run(text, seed=1, threads=1):
             o = ctx[c["wait"]["ints"][0]]
             if o["wait"] is None or _kind(o["wait"]) != kind or o["wait"]["ints"][0] != k:
                 continue
-            v = _overlap(c["r"], o["r"], c["wait"])
+            v = _overlap(c["r"], o["r"], c["wait"], c)
             c["result"], o["result"] = v, v.conjugate()
             c["wait"] = o["wait"] = None
             progress = True
         if not progress and all_same and all_kind is not None:
             w = ctx[0]["wait"]
             for c in ctx:
-                c["result"] = _overlap(ctx[0]["r"], c["r"], w)
+                c["result"] = _overlap(ctx[0]["r"], c["r"], w, ctx[0])
             for c in ctx:
                 c["wait"] = None
             progress = True

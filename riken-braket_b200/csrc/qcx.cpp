@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <iomanip>
+#include <map>
 #include <random>
 #include <sstream>
 #include <stdexcept>
@@ -117,6 +118,19 @@ int64_t to_phase_exponent(const std::string& s)
   return to_int(s);
 }
 
+// A variable reference: a letter, then letters, digits or '_', optionally
+// followed by ':<index>' (bra's NAME:index element access).
+bool valid_name(const std::string& s)
+{
+  if (s.empty() || !std::isalpha(static_cast<unsigned char>(s.front()))) return false;
+  const size_t colon = s.find(':');
+  for (size_t i = 0; i < std::min(colon, s.size()); ++i)
+    if (!std::isalnum(static_cast<unsigned char>(s[i])) && s[i] != '_') return false;
+  if (colon == std::string::npos) return true;
+  const std::string idx = s.substr(colon + 1);
+  return !idx.empty() && std::all_of(idx.begin(), idx.end(), [](char ch) { return std::isdigit(static_cast<unsigned char>(ch)) != 0; });
+}
+
 rbk_qcx_instruction blank(int op, int line)
 {
   rbk_qcx_instruction in;
@@ -166,6 +180,33 @@ struct parser {
       in.params[k] = exponent ? static_cast<double>(to_phase_exponent(v)) : to_real(v);
     }
     prog.code.push_back(in);
+  }
+
+  void copy_text(rbk_qcx_instruction& in, const std::string& s)
+  {
+    if (s.size() >= sizeof(in.text)) bad("operand too long");
+    std::memcpy(in.text, s.c_str(), s.size() + 1);
+  }
+
+  // The operator column of EXPECTATION / INNERPROD / FIDELITY: a :PAULIS:<s>
+  // literal whose length must equal the number of operated qubits (returns
+  // false), or a PAULISS variable NAME / NAME:index whose length is checked
+  // when it runs (returns true).  Either goes to in.text.
+  bool operator_column(const std::string& col, size_t num_qubits, rbk_qcx_instruction& in)
+  {
+    const std::string u = upper(col);
+    if (u.rfind(":PAULIS:", 0) == 0 && u.size() > 8) {
+      const std::string str = u.substr(8);
+      if (str.size() != num_qubits) bad("the Pauli string length must equal the number of qubits");
+      if (str.size() > RBK_QCX_MAX_QUBITS) bad("Pauli string too long");
+      for (char ch : str)
+        if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z') bad("Pauli strings use I, X, Y, Z");
+      copy_text(in, str);
+      return false;
+    }
+    if (!valid_name(u)) unsupported("the operator must be a :PAULIS:<string> literal or a PAULISS variable");
+    copy_text(in, u);
+    return true;
   }
 
   void noop(const columns& c, int nqubits)
@@ -304,7 +345,7 @@ struct parser {
       return;
     }
     if (m == "MPIPROCESSES" || m == "MPISWAPBUFFER") return;
-    if (m == "DEPOLARIZING" || m == "PERMUTATION" || m == "RANDOM" || m == "VAR" || m == "LET" || m == "SEND" ||
+    if (m == "DEPOLARIZING" || m == "PERMUTATION" || m == "RANDOM" || m == "SEND" ||
         m == "RECEIVE" || m == "BROADCAST" || m == "GATHER" || m == "SCATTER" || m == "JUMP" || m == "JUMPIF" ||
         m.front() == '@')
       unsupported("'" + m + "' is not supported");
@@ -382,17 +423,35 @@ struct parser {
       done = true;
       return;
     }
-    if (m == "EXPECTATION") {  // EXPECTATION :PAULIS:<s> q1 q2 ... (interpreter.cpp:3218-3240)
+    if (m == "VAR") {  // VAR name PAULISS [size] (interpreter.cpp:1966-1994)
+      if (c.size() != 3 && c.size() != 4) bad("expected VAR <name> <type> [<size>]");
+      const std::string name = upper(c[1]), type = upper(c[2]);
+      if (type != "PAULISS") unsupported("VAR of type " + type + " (only PAULISS variables are supported)");
+      if (!valid_name(name) || name.find(':') != std::string::npos) bad("'" + c[1] + "' is not a variable name");
+      auto in = blank(RBK_QCX_VAR, line);
+      in.ints[0] = c.size() == 4 ? to_int(c[3]) : 1;
+      if (in.ints[0] <= 0) bad("the size of a variable must be positive");
+      copy_text(in, name);
+      prog.code.push_back(in);
+      return;
+    }
+    if (m == "LET") {  // LET lhs op rhs (interpreter.cpp:1996-2027)
+      expect(c, 4);
+      const std::string lhs = upper(c[1]), rhs = upper(c[3]);
+      auto in = blank(RBK_QCX_LET, line);
+      const std::string& op = c[2];
+      in.ints[0] = op == ":=" ? RBK_QCX_ASSIGN : op == "+=" ? RBK_QCX_PLUS : op == "-=" ? RBK_QCX_MINUS
+                 : op == "*=" ? RBK_QCX_TIMES : op == "/=" ? RBK_QCX_DIVIDE : -1;
+      if (in.ints[0] < 0) bad("unknown LET operation '" + op + "'");
+      if (!valid_name(lhs)) bad("'" + c[1] + "' is not a variable");
+      copy_text(in, lhs + " " + rhs);
+      prog.code.push_back(in);
+      return;
+    }
+    if (m == "EXPECTATION") {  // EXPECTATION <operator> q1 q2 ... (interpreter.cpp:3218-3240)
       if (c.size() < 3) bad("expected EXPECTATION <operator> <qubits>");
-      const std::string& op = c[1];
-      if (op.rfind(":PAULIS:", 0) != 0 || op.size() <= 8) unsupported("EXPECTATION takes a :PAULIS:<string> literal");
       auto in = blank(RBK_QCX_EXPECTATION, line);
-      const std::string str = upper(op.substr(8));
-      if (str.size() != c.size() - 2) bad("the Pauli string length must equal the number of qubits");
-      if (str.size() >= sizeof(in.text) || str.size() > RBK_QCX_MAX_QUBITS) bad("Pauli string too long");
-      for (char ch : str)
-        if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z') bad("Pauli strings use I, X, Y, Z");
-      std::memcpy(in.text, str.c_str(), str.size() + 1);
+      in.ints[1] = operator_column(c[1], c.size() - 2, in) ? 1 : 0;
       std::vector<uint32_t> seen;
       for (size_t i = 2; i < c.size(); ++i) {
         const uint32_t q = qubit(c[i]);
@@ -415,14 +474,7 @@ struct parser {
         in.ints[0] = upper(who) == "ALL" ? RBK_QCX_ALL : RBK_QCX_NONE;
       }
       if (c.size() >= 4) {
-        const std::string& op = c[2];
-        if (op.rfind(":PAULIS:", 0) != 0 || op.size() <= 8) unsupported(m + " takes a :PAULIS:<string> literal");
-        const std::string str = upper(op.substr(8));
-        if (str.size() != c.size() - 3) bad("the Pauli string length must equal the number of qubits");
-        if (str.size() >= sizeof(in.text) || str.size() > RBK_QCX_MAX_QUBITS) bad("Pauli string too long");
-        for (char ch : str)
-          if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z') bad("Pauli strings use I, X, Y, Z");
-        std::memcpy(in.text, str.c_str(), str.size() + 1);
+        in.ints[1] = operator_column(c[2], c.size() - 3, in) ? 1 : 0;
         std::vector<uint32_t> seen;
         for (size_t i = 3; i < c.size(); ++i) {
           const uint32_t q = qubit(c[i]);
@@ -554,6 +606,14 @@ void check(int rc)
   if (rc != RBK_OK) throw qcx_error(rc, rbk_last_error());
 }
 
+// bra::pauli_string_space (bra/include/bra/pauli_string_space.hpp:25-153): a
+// linear combination of Pauli strings of one length; a new variable is the
+// zero-qubit space {"" : 0}.
+struct pauliss {
+  size_t num_qubits = 0;
+  std::map<std::string, cplx> terms{{std::string(), cplx{0.0, 0.0}}};
+};
+
 // One circuit of the program: bra's nompi_state with its wait reason
 // (bra/include/bra/state.hpp wait_reason; bra/src/nompi_state.cpp:1204-1275).
 struct circuit_ctx {
@@ -566,6 +626,7 @@ struct circuit_ctx {
   cplx result{0.0, 0.0};
   bool in_fusion = false;
   const rbk_qcx_instruction* wait = nullptr;  // INNERPROD / FIDELITY this circuit waits on
+  std::map<std::string, std::vector<pauliss>> variables;  // VAR name PAULISS [size]
 };
 
 struct runner {
@@ -757,14 +818,114 @@ struct runner {
     mark("Measurement");
   }
 
-  // EXPECTATION :PAULIS:<s> q...: character k of the string acts on the k-th listed qubit.
+  // ---- PAULISS variables (bra/src/state.cpp:400-490, :977-998) ----
+  // NAME or NAME:index of circuit c.
+  pauliss& variable(circuit_ctx& c, const std::string& ref)
+  {
+    const size_t colon = ref.find(':');
+    const std::string name = ref.substr(0, colon);
+    const auto it = c.variables.find(name);
+    if (it == c.variables.end()) throw qcx_error(RBK_ERR_UNSUPPORTED, "'" + name + "' is not a PAULISS variable of this circuit");
+    const int64_t index = colon == std::string::npos ? 0 : to_int(ref.substr(colon + 1));
+    if (index < 0 || static_cast<size_t>(index) >= it->second.size())
+      throw qcx_error(RBK_ERR_INVALID, "index of '" + name + "' out of range");
+    return it->second[static_cast<size_t>(index)];
+  }
+
+  // bra::state::to_pauli_string_space: a :PAULIS:<s> literal (coefficient 1) or a variable.
+  pauliss pauli_value(circuit_ctx& c, const std::string& rhs)
+  {
+    if (rhs.rfind(":PAULIS:", 0) == 0 && rhs.size() > 8) {
+      pauliss v;
+      const std::string str = rhs.substr(8);
+      for (char ch : str)
+        if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z') throw qcx_error(RBK_ERR_INVALID, "Pauli strings use I, X, Y, Z");
+      v.num_qubits = str.size();
+      v.terms = {{str, cplx{1.0, 0.0}}};
+      return v;
+    }
+    if (rhs.front() == ':') throw qcx_error(RBK_ERR_UNSUPPORTED, "'" + rhs + "' is not a Pauli-string-space value");
+    return variable(c, rhs);
+  }
+
+  // bra::state::to_complex for the literal forms.
+  cplx complex_value(const circuit_ctx& c, const std::string& rhs) const
+  {
+    if (rhs == ":COMPLEX") return cplx{0.0, 0.0};
+    if (rhs == ":I") return cplx{0.0, 1.0};
+    if (rhs == ":MINUS_I") return cplx{0.0, -1.0};
+    if (rhs == ":RESULT") return c.result;
+    if (rhs.rfind(":COMPLEX:", 0) == 0 && rhs.size() > 9) {
+      const std::string v = rhs.substr(9);
+      const char f = v.front();
+      if (std::isdigit(static_cast<unsigned char>(f)) || f == '+' || f == '-' || f == '.') return cplx{to_real(v), 0.0};
+    }
+    throw qcx_error(RBK_ERR_UNSUPPORTED, "'" + rhs + "' is not a supported complex value (:COMPLEX:<literal>, :I, :MINUS_I, :RESULT)");
+  }
+
+  void declare(const rbk_qcx_instruction& in)
+  {
+    const std::string name(in.text);
+    if (cur->variables.count(name)) throw qcx_error(RBK_ERR_INVALID, "variable '" + name + "' is declared twice");
+    cur->variables[name] = std::vector<pauliss>(static_cast<size_t>(in.ints[0]));
+  }
+
+  // bra::state::invoke_assign_operation on a PAULISS left side.
+  void let(const rbk_qcx_instruction& in)
+  {
+    const std::string text(in.text);
+    const size_t space = text.find(' ');
+    const std::string lhs_ref = text.substr(0, space), rhs = text.substr(space + 1);
+    pauliss& lhs = variable(*cur, lhs_ref);
+    const int op = static_cast<int>(in.ints[0]);
+    if (op == RBK_QCX_ASSIGN) {
+      lhs = pauli_value(*cur, rhs);
+    } else if (op == RBK_QCX_PLUS || op == RBK_QCX_MINUS) {
+      for (const auto& term : pauli_value(*cur, rhs).terms) {
+        if (term.first.size() != lhs.num_qubits)
+          throw qcx_error(RBK_ERR_INVALID, term.first + " is not a valid Pauli string or has wrong length");
+        if (op == RBK_QCX_PLUS) lhs.terms[term.first] += term.second;
+        else lhs.terms[term.first] -= term.second;
+      }
+    } else {
+      const cplx v = complex_value(*cur, rhs);
+      for (auto& term : lhs.terms) term.second = op == RBK_QCX_TIMES ? term.second * v : term.second / v;
+    }
+  }
+
+  // The operator of EXPECTATION / INNERPROD / FIDELITY as terms over all
+  // qubits: character k of each string acts on the k-th listed qubit.
+  void operator_terms(circuit_ctx& c, const rbk_qcx_instruction& in, std::string& strings, std::vector<double>& coeffs)
+  {
+    pauliss op;
+    if (in.ints[1]) {
+      op = variable(c, in.text);
+      if (op.num_qubits != static_cast<size_t>(in.num_targets))
+        throw qcx_error(RBK_ERR_INVALID, "the operator has " + std::to_string(op.num_qubits) + " qubits, " +
+                                           std::to_string(in.num_targets) + " are listed");
+    } else {
+      op.num_qubits = static_cast<size_t>(in.num_targets);
+      op.terms = {{std::string(in.text), cplx{1.0, 0.0}}};
+    }
+    strings.clear();
+    coeffs.clear();
+    for (const auto& term : op.terms) {
+      std::string full(static_cast<size_t>(prog.num_qubits), 'I');
+      for (int k = 0; k < in.num_targets; ++k) full[in.targets[k]] = term.first[static_cast<size_t>(k)];
+      strings += full;
+      coeffs.push_back(term.second.real());
+      coeffs.push_back(term.second.imag());
+    }
+  }
+
+  // EXPECTATION <operator> q...: sum over the operator's terms of coefficient x <psi|P|psi>.
   void expectation(const rbk_qcx_instruction& in)
   {
-    std::string full(static_cast<size_t>(prog.num_qubits), 'I');
-    for (int k = 0; k < in.num_targets; ++k) full[in.targets[k]] = in.text[k];
-    const double coeff[2] = {1.0, 0.0};
+    std::string strings;
+    std::vector<double> coeffs;
+    operator_terms(*cur, in, strings, coeffs);
     double r[2];
-    check(rbk_expectation_pauli(s, 1, full.c_str(), coeff, r));
+    check(rbk_expectation_pauli(s, static_cast<int>(coeffs.size() / 2), strings.c_str(), coeffs.data(), r));
     cur->result = cplx{r[0], r[1]};
   }
 
@@ -798,24 +959,22 @@ struct runner {
     if (in.ints[0]) out << '\n';
   }
 
-  // The Pauli string of an INNERPROD / FIDELITY operator over all qubits.
-  std::string operator_string(const rbk_qcx_instruction& in) const
-  {
-    std::string full(static_cast<size_t>(prog.num_qubits), 'I');
-    for (int k = 0; k < in.num_targets; ++k) full[in.targets[k]] = in.text[k];
-    return full;
-  }
-
-  // ket::inner_product(a, b[, H]) = <b| [H] |a>, or its squared modulus.
-  cplx overlap(rbk_state* a, rbk_state* b, const rbk_qcx_instruction& in)
+  // ket::inner_product(a, b[, H]) = <b| [H] |a>, or its squared modulus; the
+  // operator is circuit owner's.
+  cplx overlap(rbk_state* a, rbk_state* b, circuit_ctx& owner, const rbk_qcx_instruction& in)
   {
     double r[2] = {0.0, 0.0};
-    if (in.text[0]) {
-      const std::string full = operator_string(in);
-      const double coeff[2] = {1.0, 0.0};
-      check(rbk_inner_product_pauli(a, b, 1, full.c_str(), coeff, r));
-    } else {
-      check(rbk_inner_product(a, b, r));
+    try {
+      if (in.text[0]) {
+        std::string strings;
+        std::vector<double> coeffs;
+        operator_terms(owner, in, strings, coeffs);
+        check(rbk_inner_product_pauli(a, b, static_cast<int>(coeffs.size() / 2), strings.c_str(), coeffs.data(), r));
+      } else {
+        check(rbk_inner_product(a, b, r));
+      }
+    } catch (qcx_error const& e) {
+      throw qcx_error(e.code, "line " + std::to_string(in.line) + ": " + e.what());
     }
     if (in.op == RBK_QCX_FIDELITY) return cplx{r[0] * r[0] + r[1] * r[1], 0.0};
     return cplx{r[0], r[1]};
@@ -849,6 +1008,8 @@ struct runner {
           }
           case RBK_QCX_EXPECTATION: expectation(in); break;
           case RBK_QCX_PRINT: print(in); break;
+          case RBK_QCX_VAR: declare(in); break;
+          case RBK_QCX_LET: let(in); break;
           case RBK_QCX_INNERPROD: case RBK_QCX_FIDELITY:
             // bra::state::inner_product / fidelity refuse a fused block (bra/src/state.cpp:2133-2170)
             if (c.in_fusion) throw qcx_error(RBK_ERR_UNSUPPORTED, "INNERPROD / FIDELITY inside BEGIN/END FUSION");
@@ -897,7 +1058,7 @@ struct runner {
         const int other = static_cast<int>(c.wait->ints[0]);
         circuit_ctx& o = circ[static_cast<size_t>(other)];
         if (!o.wait || kind_of(o.wait) != kind || o.wait->ints[0] != k) continue;
-        const cplx r = overlap(c.s, o.s, *c.wait);  // <Psi_other| [H] |Psi_k>
+        const cplx r = overlap(c.s, o.s, c, *c.wait);  // <Psi_other| [H] |Psi_k>
         c.result = r;
         o.result = std::conj(r);
         c.wait = o.wait = nullptr;
@@ -905,7 +1066,7 @@ struct runner {
       }
       if (!progress && all_same && all_kind >= 0) {
         const rbk_qcx_instruction& in = *circ.front().wait;  // the operator comes from circuit 0
-        for (auto& c : circ) c.result = overlap(circ.front().s, c.s, in);  // <Psi_c| [H] |Psi_0>
+        for (auto& c : circ) c.result = overlap(circ.front().s, c.s, circ.front(), in);  // <Psi_c| [H] |Psi_0>
         for (auto& c : circ) c.wait = nullptr;
         progress = true;
       }

@@ -235,6 +235,57 @@ def circuits_tiles(n=14, seed=9):
     return "\n".join(L) + "\n"
 
 
+def _ansatz_lines(n, layers, rng):
+    """Config-4 style ansatz: EY and EZ on every qubit, then a CZ ring, per layer."""
+    L = []
+    for _ in range(layers):
+        L += ["EY %d %s" % (q, a(rng)) for q in range(n)]
+        L += ["EZ %d %s" % (q, a(rng)) for q in range(n)]
+        L += ["CZ %d %d" % (q, (q + 1) % n) for q in range(n)]
+    return L
+
+
+def _string(n, letters):
+    s = ["I"] * n
+    for q, ch in letters:
+        s[q] = ch
+    return "".join(s)
+
+
+def pauliss_hamiltonian(n=10, layers=3, seed=10):
+    """PAULISS variables: H = sum Z_i Z_i+1 + 0.5 sum X_i (periodic) built with
+    VAR / LET (:=, +=, -=, *=, /=, arrays, :RESULT as a scalar) and read by
+    EXPECTATION."""
+    rng = np.random.default_rng(seed)
+    L = ["! Pauli-string-space variables", "QUBITS %d" % n] + _ansatz_lines(n, layers, rng)
+    L += ["VAR H PAULISS", "VAR XS PAULISS 2", "LET H := :PAULIS:%s" % _string(n, [(0, "Z"), (1, "Z")])]
+    L += ["LET H += :PAULIS:%s" % _string(n, [(i, "Z"), ((i + 1) % n, "Z")]) for i in range(1, n)]
+    L += ["LET XS:0 := :PAULIS:%s" % _string(n, [(0, "X")])]
+    L += ["LET XS:0 += :PAULIS:%s" % _string(n, [(i, "X")]) for i in range(1, n)]
+    L += ["LET XS:0 *= :COMPLEX:0.5", "let h += xs:0", "EXPECTATION H " + " ".join(str(q) for q in range(n)),
+          "PRINTLN :RESULT"]
+    L += ["LET XS:1 := H", "LET XS:1 -= :PAULIS:%s" % _string(n, [(0, "Z"), (1, "Z")]), "LET XS:1 /= :COMPLEX:4",
+          "LET XS:1 *= :I", "LET XS:1 += :PAULIS:%s" % _string(n, [(2, "Y"), (5, "X"), (7, "Z")]),
+          "EXPECTATION XS:1 " + " ".join(str(q) for q in range(n)), "PRINTLN :RESULT"]
+    L += ["VAR Q PAULISS", "LET Q := :PAULIS:XZY", "LET Q *= :RESULT", "LET Q -= :PAULIS:ZIX", "LET Q *= :MINUS_I",
+          "EXPECTATION Q 3 1 7", "PRINTLN :RESULT", "EXPECTATION :PAULIS:YY 4 6", "PRINTLN :RESULT"]
+    L += ["DO MEASUREMENT 6"]
+    return "\n".join(L) + "\n"
+
+
+def pauliss_circuits(n=8, seed=11):
+    """PAULISS operators of INNERPROD / FIDELITY over two circuits: a pair whose
+    circuits each use their own H, and the ALL form with circuit 0's."""
+    rng = np.random.default_rng(seed)
+    L = ["CIRCUITS 2", "QUBITS %d" % n] + _ansatz_lines(n, 2, rng)
+    L += ["VAR H PAULISS", "LET H := :PAULIS:ZZX", "LET H += :PAULIS:XIY", "LET H *= :COMPLEX:0.75",
+          "INNERPROD 1 H 0 3 6", "PRINTLN :RESULT", "FIDELITY ALL H 2 5 7", "PRINTLN :RESULT"]
+    L += ["BEGIN CIRCUIT 1"] + _ansatz_lines(n, 2, rng)
+    L += ["VAR H PAULISS", "LET H := :PAULIS:YYZ", "LET H -= :PAULIS:IZI", "INNERPROD 0 H 1 2 4", "PRINTLN :RESULT",
+          "VAR G PAULISS", "LET G := :PAULIS:XXX", "FIDELITY ALL G 2 5 7", "PRINTLN :RESULT", "END CIRCUIT"]
+    return "\n".join(L) + "\n"
+
+
 PROGRAMS = {
     "every_gate": every_gate,
     "fused_brick": fused_brick,
@@ -246,6 +297,8 @@ PROGRAMS = {
     "bigger_mixed": bigger_mixed,
     "circuits_overlaps": circuits_overlaps,
     "circuits_tiles": circuits_tiles,
+    "pauliss_hamiltonian": pauliss_hamiltonian,
+    "pauliss_circuits": pauliss_circuits,
     "hadamards8": lambda: "QUBITS 8\n" + "".join("H %d\n" % q for q in range(8)) + "DO MEASUREMENT\n",
 }
 

@@ -168,3 +168,45 @@ def test_inner_product_pauli_vs_reference(pkg, n, precision):
     assert abs(a.inner_product_pauli(b, terms) - total_ref) <= 4 * tol
     a.close()
     b.close()
+
+
+def test_pauliss_hamiltonian_energy_full_precision(pkg):
+    """Config 4's Hamiltonian written as a .qcx program with PAULISS variables
+    (tests/golden/qcx/pauliss_hamiltonian.qcx): the ansatz state the program
+    leaves behind has the energy that EXPECTATION H printed, and it equals
+    rbk_expectation_pauli on that state and the reference's own ket code
+    (bra's EXPECTATION term by term, ketref_expectation_on) to 1e-12."""
+    import oracle
+    import bra_ref
+
+    text = open(os.path.join(GOLDEN, "qcx", "pauliss_hamiltonian.qcx")).read()
+    out, state = pkg.qcx.parse(text).run(keep_state=True)
+    n = 10
+    energy_engine = state.expectation(pkg.circuits.ansatz_hamiltonian(n))
+    state.close()
+    # The reference: the program's gates on ket as bra dispatches them, H term by term.
+    _, _, code = bra_ref.parse(text)
+    r = oracle.KetRef(n)
+    for ins in code:
+        if ins["op"] == bra_ref.OP["GATE"]:
+            r.gate(ins["kind"], ins["targets"], ins["controls"], ins["params"])
+    energy_ref = sum(r.expectation_on("ZZ", [i, (i + 1) % n]) for i in range(n))
+    energy_ref += 0.5 * sum(r.expectation_on("X", [i]) for i in range(n))
+    printed = complex(*(float(x) for x in out.splitlines()[0].strip("()").split(",")))
+    assert abs(energy_engine - energy_ref) <= TOL64
+    assert abs(printed - energy_ref) <= 1e-5 * max(1.0, abs(energy_ref))
+
+
+@pytest.mark.parametrize("body,message", [
+    ("VAR H PAULISS\nLET H += :PAULIS:ZZ\n", "wrong length"),            # a new variable has zero qubits
+    ("VAR H PAULISS\nLET H := :PAULIS:ZZ\nEXPECTATION H 0 1 2\n", "qubits"),
+    ("LET G := :PAULIS:ZZ\n", "not a PAULISS variable"),
+    ("VAR H PAULISS\nVAR H PAULISS\n", "declared twice"),
+    ("VAR H PAULISS 2\nLET H:2 := :PAULIS:Z\n", "out of range"),
+    ("VAR H PAULISS\nLET H := :PAULIS:Z\nLET H *= 2.0\n", "complex value"),
+])
+def test_pauliss_errors_name_the_line(pkg, body, message):
+    text = "QUBITS 3\nH 0\n" + body
+    with pytest.raises(pkg.RbkError) as e:
+        pkg.qcx.parse(text).run()
+    assert message in str(e.value) and "line" in str(e.value)

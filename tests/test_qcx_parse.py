@@ -65,7 +65,11 @@ def test_every_gate_program_covers_the_gate_set(pkg):
     ("QUBITS 3\nEND CIRCUIT\n", 1, "line 2"),
     ("QUBITS 3\nINNERPROD 1\n", 1, "line 2"),
     ("CIRCUITS 2\nQUBITS 3\nFIDELITY 1 :PAULIS:ZZ 0\n", 1, "line 3"),
-    ("CIRCUITS 2\nQUBITS 3\nINNERPROD ALL H 0 1\n", 5, "line 3"),
+    ("CIRCUITS 2\nQUBITS 3\nINNERPROD ALL :REAL:1 0 1\n", 5, "line 3"),
+    ("QUBITS 3\nVAR H PAULISS\nLET H ** :PAULIS:Z\n", 1, "line 3"),
+    ("QUBITS 3\nVAR 1H PAULISS\n", 1, "line 2"),
+    ("QUBITS 3\nVAR H PAULISS 0\n", 1, "line 2"),
+    ("QUBITS 3\nEXPECTATION :PAULIS:ZQ 0 1\n", 1, "line 2"),
     ("QUBITS 3\nDEPOLARIZING CHANNEL P_X=0.1\n", 5, "line 2"),
     ("QUBITS 3\nEXPECTATION :PAULIS:ZZ 0\n", 1, "line 2"),
     ("", 1, "QUBITS"),
