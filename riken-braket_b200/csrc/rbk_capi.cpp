@@ -34,6 +34,9 @@ struct rbk_state {
   double* d_partials = nullptr;
   double* d_out = nullptr;
   double* h_out = nullptr;  // pinned
+  float* d_tc_w = nullptr;   // W_hi, W_lo of the tensor-core unitaries (largest k), kept between calls
+  int* d_tc_flag = nullptr;  // set by a tensor-core unitary whose bounded wait ran out (sticky)
+  int* h_tc_flag = nullptr;  // pinned copy, read at every bounded_sync
   std::vector<int> perm, inv;
   std::vector<hgate> queue;
   bool deferred = true;
@@ -89,21 +92,29 @@ double wait_timeout_seconds()
 }
 
 // Bounded wait for everything issued on the state's stream.
+// Waits for the state's stream, polling: the first 200 us without sleeping
+// (short device work returns at once), then with sleeps that grow to 200 us,
+// so a wait ends at most that long after the device does.  Bounded by the
+// RBK_TIMEOUT_S limit.  Also reports a tensor-core unitary that gave up.
 int bounded_sync(rbk_state* s)
 {
   RBK_CUDA(cudaEventRecord(s->ev_sync, s->stream));
   const auto t0 = std::chrono::steady_clock::now();
   const double limit = wait_timeout_seconds();
-  int sleep_us = 20;
+  int sleep_us = 5;
   while (true) {
     const cudaError_t e = cudaEventQuery(s->ev_sync);
-    if (e == cudaSuccess) return RBK_OK;
+    if (e == cudaSuccess) break;
     if (e != cudaErrorNotReady) return cuda_fail(e, "device execution");
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (el > limit) return fail(RBK_ERR_TIMEOUT, "timed out waiting for the device");
-    std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
-    if (sleep_us < 2000) sleep_us *= 2;
+    if (el > 2e-4) {
+      std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+      if (sleep_us < 200) sleep_us *= 2;
+    }
   }
+  if (s->h_tc_flag && *s->h_tc_flag) return fail(RBK_ERR_TIMEOUT, "tensor-core unitary: a wait for the MMAs ran out");
+  return RBK_OK;
 }
 
 inline size_t amp_bytes(int precision) { return precision == RBK_C128 ? 16 : 8; }
@@ -502,6 +513,9 @@ int rbk_state_destroy(rbk_state* s)
   if (s->d_partials) cudaFree(s->d_partials);
   if (s->d_out) cudaFree(s->d_out);
   if (s->h_out) cudaFreeHost(s->h_out);
+  if (s->d_tc_w) cudaFree(s->d_tc_w);
+  if (s->d_tc_flag) cudaFree(s->d_tc_flag);
+  if (s->h_tc_flag) cudaFreeHost(s->h_tc_flag);
   for (cudaEvent_t ev : {s->ev_first, s->ev_last, s->ev_sync}) if (ev) cudaEventDestroy(ev);
   if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -2123,25 +2137,27 @@ int apply_unitary(rbk_state* s, const std::vector<cplx>& U, const uint32_t* q, i
       b += len;
     }
     const std::vector<float> w = build_w_split(U, k);
-    device_buffer dw;
-    RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&dw.p), sizeof(float) * w.size()));
-    RBK_CUDA(cudaMemcpyAsync(dw.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice, s->stream));
-    int* flag = reinterpret_cast<int*>(s->d_out);
-    RBK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
+    if (!s->d_tc_w) {  // once per state: W of the largest k, and the sticky error flag
+      RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&s->d_tc_w), sizeof(float) * rbk::tc_w_split_floats(6)));
+      RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&s->d_tc_flag), sizeof(int)));
+      RBK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&s->h_tc_flag), sizeof(int)));
+      *s->h_tc_flag = 0;
+      RBK_CUDA(cudaMemsetAsync(s->d_tc_flag, 0, sizeof(int), s->stream));
+    }
+    // Stream order keeps this copy behind the previous unitary's reads of the buffer; the
+    // pageable source is staged by the copy call, so w may go when it returns.
+    RBK_CUDA(cudaMemcpyAsync(s->d_tc_w, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice, s->stream));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     const uint64_t tiles = (1ull << (s->n - k)) / 128;
     const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(sms)));
-    const cudaError_t e = rbk::launch_unitary_tf32x3(s->amps, s->n, k, reinterpret_cast<const float*>(dw.p), flag, grid,
-                                                    lay, s->stream);
+    const cudaError_t e = rbk::launch_unitary_tf32x3(s->amps, s->n, k, s->d_tc_w, s->d_tc_flag, grid, lay, s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "tensor-core unitary");
     ++s->stats.kernel_launches;
     ++s->stats.passes;
-    int h = 0;
-    RBK_CUDA(cudaMemcpyAsync(s->h_out, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-    if (int rc = bounded_sync(s)) return rc;
-    std::memcpy(&h, s->h_out, sizeof(int));
-    if (h) return fail(RBK_ERR_TIMEOUT, "tensor-core unitary: a wait for the MMAs ran out");
+    // No wait here: the flag reaches the pinned copy in stream order and the next
+    // bounded_sync (every read of the state) reports a wait that ran out.
+    RBK_CUDA(cudaMemcpyAsync(s->h_tc_flag, s->d_tc_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   } else {
     device_buffer du;
     const size_t count = 2 * U.size();

@@ -16,15 +16,16 @@
 // tensor cores.  This is the bra-fused 2^k x 2^k unitary of a fusion block
 // (bra/src/nompi_state.cpp:1285-1357 replays the gates instead).
 //
-// One CTA per SM (persistent), 128 threads.  W_hi and W_lo stay in shared
-// memory for the whole launch in the canonical K-major layout without swizzle
-// (8-row x 16-byte core matrices).  Each 128-row tile is staged in two K
-// halves: threads load, split and store A_hi / A_lo, one thread issues the 3 x
-// K/16 tcgen05.mma of the half, and tcgen05.commit signals an mbarrier.  The
-// epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes
-// 32w..32w+31 = rows) and writes the rows back in place.  Every mbarrier wait is
-// bounded: on expiry the kernel raises an error flag, waits (bounded) for its
-// own MMAs, frees its TMEM and returns.
+// One CTA per SM (persistent), 288 threads in three roles that meet at
+// mbarriers (see the kernel): producer warps stream K quarters of 128-row
+// tiles from HBM, kTcDepth quarters ahead in registers, and split them into
+// A_hi / A_lo operand slots; one thread issues the tcgen05.mma of each quarter;
+// epilogue warps read finished accumulators with tcgen05.ld and write the rows
+// back in place.  W_hi and W_lo stay in shared memory for the whole launch in
+// the canonical K-major layout without swizzle (8-row x 16-byte core
+// matrices).  Every mbarrier wait is bounded: on expiry the kernel raises an
+// error flag, every role stops, the MMA thread waits (bounded) for its own
+// MMAs, and the CTA frees its TMEM and returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -35,7 +36,8 @@
 namespace rbk {
 namespace {
 
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 288;  // 4 producer, 4 epilogue and 1 MMA warp
+constexpr int kTcDepth = 3;       // K quarters whose loads are in flight
 constexpr int kTcM = 128;
 constexpr uint32_t kWaitLimit = 1u << 22;
 
@@ -119,27 +121,58 @@ __device__ __forceinline__ uint32_t kmajor_offset(uint32_t row, uint32_t kk, uin
   return (row >> 3) * (kc / 4) * 128u + (kk >> 2) * 128u + (row & 7u) * 16u + (kk & 3u) * 4u;
 }
 
+// Warp-collective load of 32 consecutive TMEM columns of the warp's lane quarter (one per thread).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
+{
+  asm volatile(
+    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+    "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+    "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+      "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+      "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+    : "r"(taddr)
+    : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
 template <int KB>  // KB = k + 1: K = N = 2^KB floats per row
 __global__ void __launch_bounds__(kTcThreads, 1)
 unitary_tf32x3_kernel(float2* __restrict__ state, uint64_t rows, const float4* __restrict__ w_split, int* error_flag,
                       const __grid_constant__ tc_layout L)
 {
-  // Software pipeline over "stages" = K quarters of this CTA's tiles.  Stage s
-  // is split into A buffer s % 2 while the registers already fetch stage s + 1
-  // from HBM and the tensor cores still run stage s - 1; a tile's four stages
-  // accumulate into TMEM accumulator (tile % 2), so one tile's epilogue also
-  // overlaps the next tile's loads.
+  // Warp roles, all running at once and meeting at mbarriers:
+  //   warps 0-3 (producers): load a K quarter ("stage") of the CTA's next
+  //     128-row tile from HBM into registers, kTcDepth stages ahead, split it
+  //     into TF32 hi / lo and store both into A slot (stage % 2), then arrive
+  //     on full[slot];
+  //   warp 8 (MMA issuer, one thread): for each stage wait full[slot], issue
+  //     the 3 x K/32 tcgen05.mma into accumulator (tile % 2) and commit to
+  //     empty[slot]; after a tile's fourth stage also commit to acc_full[acc];
+  //   warps 4-7 (epilogue): wait acc_full[acc], read the accumulator rows
+  //     (warp 4 + q owns TMEM lanes 32q..32q+31), write them back to HBM and
+  //     arrive on acc_empty[acc] for the MMA issuer.
+  // The producers stream the next tile while the tensor cores multiply and
+  // the epilogue stores the previous one.
   constexpr uint32_t K = 1u << KB, N = K, KQ = K / 4;
   constexpr uint32_t B_BYTES = N * K * 4, AQ_BYTES = kTcM * KQ * 4;
   constexpr uint32_t SBO_A = (KQ / 4) * 128u, SBO_B = (K / 4) * 128u;
   constexpr uint32_t NCOLS = 2 * N;  // two FP32 accumulators of 128 lanes x N columns
   constexpr uint32_t CG = KQ / 16;   // groups of 4 float4 per row quarter
-  constexpr uint32_t PER_THREAD = (kTcM / 8) * CG / (kTcThreads / 32);  // float4 per thread per stage
+  constexpr uint32_t PROD_WARPS = 4, PROD_THREADS = PROD_WARPS * 32, EPI_THREADS = 128, MMA_WARP = 8;
+  constexpr uint32_t PER_THREAD = (kTcM / 8) * CG / PROD_WARPS;  // float4 per producer thread per stage
+  static_assert(PER_THREAD * PROD_WARPS == (kTcM / 8) * CG, "stage split over the producer warps");
+  static_assert(kTcThreads == 9 * 32, "4 producer warps, 4 epilogue warps, 1 MMA warp");
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* b_hi = smem;
   unsigned char* b_lo = smem + B_BYTES;
-  unsigned char* a_base = smem + 2 * B_BYTES;  // buffer b: hi at a_base + 2b AQ, lo at + (2b + 1) AQ
-  __shared__ __align__(8) uint64_t mbar[2];
+  unsigned char* a_base = smem + 2 * B_BYTES;  // slot b: hi at a_base + 2b AQ, lo at + (2b + 1) AQ
+  __shared__ __align__(8) uint64_t full[2], empty[2], acc_full[2], acc_empty[2], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   __shared__ uint64_t row_off[kTcM], elem_off[N / 2];  // physical offsets of row bits / target bits
@@ -160,8 +193,14 @@ unitary_tf32x3_kernel(float2* __restrict__ state, uint64_t rows, const float4* _
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
                  "r"(NCOLS));
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar[0])), "r"(1u));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar[1])), "r"(1u));
+    for (int i = 0; i < 2; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[i])), "r"(PROD_THREADS));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[i])), "r"(1u));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_full[i])), "r"(1u));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acc_empty[i])), "r"(EPI_THREADS));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&done)), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
   }
   {
@@ -178,130 +217,156 @@ unitary_tf32x3_kernel(float2* __restrict__ state, uint64_t rows, const float4* _
   const uint64_t tiles = rows / kTcM;
   const uint64_t my_tiles = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const uint64_t stages = my_tiles * 4;
-
-  // Where thread tid's float4 number i of a stage lives: row r, float column c (within the quarter).
-  auto slot = [&](uint32_t i, uint32_t& r, uint32_t& c) {
-    const uint32_t blk = warp + i * (kTcThreads / 32);
-    const uint32_t rg = blk / CG, cg = blk % CG;
-    r = rg * 8 + (lane & 7u);
-    c = (cg * 4 + (lane >> 3)) * 4;
-  };
-  // Tile t: its 2^(n-k-7) index deposited into the bits that are neither row nor target bits.
+  // Tile of stage st: its 2^(n-k-7) index deposited into the bits that are neither row nor target bits.
   auto tile_base = [&](uint64_t st) {
     const uint64_t t = blockIdx.x + (st >> 2) * gridDim.x;
     uint64_t v = 0;
     for (int r = 0; r < L.num_runs; ++r) v |= ((t >> L.run_src[r]) & ((1ull << L.run_len[r]) - 1)) << L.run_dst[r];
     return v;
   };
-  float4 regs[PER_THREAD];
-  auto fetch = [&](uint64_t st) {
-    const uint64_t base = tile_base(st);
-    const uint32_t e0 = (uint32_t(st & 3u) * KQ) >> 1;  // first complex element of the quarter
-#pragma unroll
-    for (uint32_t i = 0; i < PER_THREAD; ++i) {
-      uint32_t r, c;
-      slot(i, r, c);
-      const uint64_t rb = base | row_off[r];
-      if (pair) {  // elements 2m and 2m+1 are neighbours in memory: one 16-byte load
-        regs[i] = *reinterpret_cast<const float4*>(state + (rb | elem_off[e0 + (c >> 1)]));
-      } else {
-        const float2 x0 = state[rb | elem_off[e0 + (c >> 1)]], x1 = state[rb | elem_off[e0 + (c >> 1) + 1]];
-        regs[i] = make_float4(x0.x, x0.y, x1.x, x1.y);
-      }
-    }
-  };
-  auto bounded_wait = [&](uint64_t st) {  // the MMAs of stage st have completed
-    if (!mbar_wait_bounded(smem_addr(&mbar[st & 1u]), uint32_t(st >> 1) & 1u)) {
-      atomicExch(error_flag, 1);
-      abort_flag = 1;
-    }
+  volatile int* const aborted = &abort_flag;  // written by the role that gives up, read by all
+  auto wait = [&](uint64_t* bar, uint32_t parity) {
+    if (*aborted) return false;
+    if (mbar_wait_bounded(smem_addr(bar), parity)) return true;
+    atomicExch(error_flag, 1);
+    *aborted = 1;
+    return false;
   };
 
-  if (stages) fetch(0);
-  for (uint64_t st = 0; st < stages; ++st) {
-    const uint32_t buf = uint32_t(st & 1u);
-    unsigned char* a_hi = a_base + (2 * buf) * AQ_BYTES;
-    unsigned char* a_lo = a_hi + AQ_BYTES;
-    if (st >= 2) bounded_wait(st - 2);  // the tensor cores are done with this buffer
+  if (warp < PROD_WARPS) {
+    // Where producer thread tid's float4 number i of a stage lives: row r, float column c (within the quarter).
+    auto slot_of = [&](uint32_t i, uint32_t& r, uint32_t& c) {
+      const uint32_t blk = warp + i * PROD_WARPS;
+      const uint32_t rg = blk / CG, cg = blk % CG;
+      r = rg * 8 + (lane & 7u);
+      c = (cg * 4 + (lane >> 3)) * 4;
+    };
+    float4 regs[kTcDepth][PER_THREAD];  // a ring of stages in flight, indexed statically
+    auto fetch = [&](uint64_t st, float4 (&out)[PER_THREAD]) {
+      const uint64_t base = tile_base(st);
+      const uint32_t e0 = (uint32_t(st & 3u) * KQ) >> 1;  // first complex element of the quarter
 #pragma unroll
-    for (uint32_t i = 0; i < PER_THREAD; ++i) {
-      uint32_t r, c;
-      slot(i, r, c);
-      const float4 v = regs[i];
-      float4 hi, lo;
-      hi.x = tf32_rna(v.x); lo.x = tf32_rna(v.x - hi.x);
-      hi.y = tf32_rna(v.y); lo.y = tf32_rna(v.y - hi.y);
-      hi.z = tf32_rna(v.z); lo.z = tf32_rna(v.z - hi.z);
-      hi.w = tf32_rna(v.w); lo.w = tf32_rna(v.w - hi.w);
-      const uint32_t off = kmajor_offset(r, c, KQ);
-      *reinterpret_cast<float4*>(a_hi + off) = hi;
-      *reinterpret_cast<float4*>(a_lo + off) = lo;
-    }
-    if (st + 1 < stages) fetch(st + 1);  // in flight while the tensor cores work
-    async_proxy_fence();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (abort_flag) break;
-    const uint32_t q = uint32_t(st & 3u);
-    const uint32_t acc = tmem + uint32_t((st >> 2) & 1u) * N;
-    if (tid == 0) {
-      const uint32_t ah = smem_addr(a_hi), al = smem_addr(a_lo), bh = smem_addr(b_hi), bl = smem_addr(b_lo);
-#pragma unroll
-      for (uint32_t j = 0; j < KQ / 8; ++j) {
-        const uint32_t g = q * (KQ / 8) + j;
-        const uint64_t da_hi = kmajor_desc(ah + j * 256u, 128u, SBO_A), da_lo = kmajor_desc(al + j * 256u, 128u, SBO_A);
-        const uint64_t db_hi = kmajor_desc(bh + g * 256u, 128u, SBO_B), db_lo = kmajor_desc(bl + g * 256u, 128u, SBO_B);
-        umma_tf32(acc, da_hi, db_hi, idesc, (q | j) != 0 ? 1u : 0u);
-        umma_tf32(acc, da_hi, db_lo, idesc, 1u);
-        umma_tf32(acc, da_lo, db_hi, idesc, 1u);
+      for (uint32_t i = 0; i < PER_THREAD; ++i) {
+        uint32_t r, c;
+        slot_of(i, r, c);
+        const uint64_t rb = base | row_off[r];
+        if (pair) {  // elements 2m and 2m+1 are neighbours in memory: one 16-byte load
+          out[i] = *reinterpret_cast<const float4*>(state + (rb | elem_off[e0 + (c >> 1)]));
+        } else {
+          const float2 x0 = state[rb | elem_off[e0 + (c >> 1)]], x1 = state[rb | elem_off[e0 + (c >> 1) + 1]];
+          out[i] = make_float4(x0.x, x0.y, x1.x, x1.y);
+        }
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_addr(&mbar[buf]))
-                   : "memory");
+    };
+#pragma unroll
+    for (uint32_t d = 0; d < kTcDepth; ++d)
+      if (d < stages) fetch(d, regs[d]);
+    bool stop = false;
+    for (uint64_t s0 = 0; s0 < stages && !stop; s0 += kTcDepth) {
+#pragma unroll
+      for (uint32_t d = 0; d < kTcDepth; ++d) {
+        const uint64_t st = s0 + d;
+        if (st >= stages) break;
+        const uint32_t buf = uint32_t(st & 1u);
+        if (st >= 2 && !wait(&empty[buf], uint32_t((st - 2) >> 1) & 1u)) { stop = true; break; }
+        unsigned char* a_hi = a_base + (2 * buf) * AQ_BYTES;
+        unsigned char* a_lo = a_hi + AQ_BYTES;
+#pragma unroll
+        for (uint32_t i = 0; i < PER_THREAD; ++i) {
+          uint32_t r, c;
+          slot_of(i, r, c);
+          const float4 v = regs[d][i];
+          float4 hi, lo;
+          hi.x = tf32_rna(v.x); lo.x = tf32_rna(v.x - hi.x);
+          hi.y = tf32_rna(v.y); lo.y = tf32_rna(v.y - hi.y);
+          hi.z = tf32_rna(v.z); lo.z = tf32_rna(v.z - hi.z);
+          hi.w = tf32_rna(v.w); lo.w = tf32_rna(v.w - hi.w);
+          const uint32_t off = kmajor_offset(r, c, KQ);
+          *reinterpret_cast<float4*>(a_hi + off) = hi;
+          *reinterpret_cast<float4*>(a_lo + off) = lo;
+        }
+        async_proxy_fence();  // these generic-proxy stores become visible to the tensor cores
+        mbar_arrive(smem_addr(&full[buf]));
+        if (st + kTcDepth < stages) fetch(st + kTcDepth, regs[d]);  // in flight while the tensor cores work
+      }
     }
-    if (q == 3) {
-      // Tile complete once this stage's MMAs are: read the accumulator, write the rows back.
-      bounded_wait(st);
+  } else if (warp == MMA_WARP) {
+    if (lane == 0) {
+      for (uint64_t st = 0; st < stages; ++st) {
+        const uint32_t buf = uint32_t(st & 1u), q = uint32_t(st & 3u);
+        const uint64_t tl = st >> 2;  // tile number within this CTA
+        const uint32_t accn = uint32_t(tl & 1u);
+        if (q == 0 && tl >= 2 && !wait(&acc_empty[accn], uint32_t((tl - 2) >> 1) & 1u)) break;
+        if (!wait(&full[buf], uint32_t(st >> 1) & 1u)) break;
+        tc_fence_after();
+        const uint32_t acc = tmem + accn * N;
+        unsigned char* a_hi = a_base + (2 * buf) * AQ_BYTES;
+        unsigned char* a_lo = a_hi + AQ_BYTES;
+        const uint32_t ah = smem_addr(a_hi), al = smem_addr(a_lo), bh = smem_addr(b_hi), bl = smem_addr(b_lo);
+#pragma unroll
+        for (uint32_t j = 0; j < KQ / 8; ++j) {
+          const uint32_t g = q * (KQ / 8) + j;
+          const uint64_t da_hi = kmajor_desc(ah + j * 256u, 128u, SBO_A), da_lo = kmajor_desc(al + j * 256u, 128u, SBO_A);
+          const uint64_t db_hi = kmajor_desc(bh + g * 256u, 128u, SBO_B), db_lo = kmajor_desc(bl + g * 256u, 128u, SBO_B);
+          umma_tf32(acc, da_hi, db_hi, idesc, (q | j) != 0 ? 1u : 0u);
+          umma_tf32(acc, da_hi, db_lo, idesc, 1u);
+          umma_tf32(acc, da_lo, db_hi, idesc, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&empty[buf]))
+                     : "memory");
+        if (q == 3)
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&acc_full[accn]))
+                       : "memory");
+      }
+      // Every MMA issued above has completed once this commit arrives (bounded).
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(&done))
+                   : "memory");
+      if (!mbar_wait_bounded(smem_addr(&done), 0u)) atomicExch(error_flag, 1);
+    }
+  } else {
+    // Epilogue: warp 4 + q reads TMEM lanes 32q .. 32q + 31 (its rows), 32 columns at a time, and
+    // turns them around in its 4 KB of shared memory so that 8 lanes write one row's 128 bytes
+    // (lane = row would put the 32 lanes of a store 512 bytes apart).  The float4 slots of a
+    // staged row are XOR-swizzled by the row, which keeps both sides free of bank conflicts.
+    const uint32_t quad = warp & 3u;
+    float4* stage = reinterpret_cast<float4*>(a_base + 4 * AQ_BYTES) + quad * (32 * 8);  // 32 rows x 8 float4
+    for (uint64_t tl = 0; tl < my_tiles; ++tl) {
+      const uint32_t accn = uint32_t(tl & 1u);
+      if (!wait(&acc_full[accn], uint32_t(tl >> 1) & 1u)) break;
       tc_fence_after();
-      __syncthreads();
-      if (abort_flag) break;
-      const uint64_t out_row = tile_base(st) | row_off[warp * 32 + lane];
+      const uint32_t acc = tmem + accn * N;
+      const uint64_t base = tile_base(tl << 2);
 #pragma unroll 1
       for (uint32_t c = 0; c < N / 32; ++c) {
         uint32_t v[32];
-        const uint32_t taddr = acc + ((warp * 32u) << 16) + c * 32u;
-        asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-          "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-          "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-          : "r"(taddr));
+        tmem_ld32(acc + ((quad * 32u) << 16) + c * 32u, v);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (pair) {
 #pragma unroll
-          for (int e = 0; e < 8; ++e)
-            *reinterpret_cast<float4*>(state + (out_row | elem_off[c * 16 + 2 * e])) =
-              make_float4(__uint_as_float(v[4 * e]), __uint_as_float(v[4 * e + 1]), __uint_as_float(v[4 * e + 2]),
-                          __uint_as_float(v[4 * e + 3]));
-        } else {
+        for (uint32_t j = 0; j < 8; ++j)
+          stage[lane * 8 + (j ^ (lane & 7u))] = make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                                            __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
+        __syncwarp();
+        const uint32_t j = lane & 7u;  // float4 j of the chunk: complex elements c * 16 + 2j, + 1
 #pragma unroll
-          for (int e = 0; e < 16; ++e)
-            state[out_row | elem_off[c * 16 + e]] = make_float2(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]));
+        for (uint32_t i = 0; i < 8; ++i) {
+          const uint32_t r = (lane >> 3) + 4 * i;
+          const float4 x = stage[r * 8 + (j ^ (r & 7u))];
+          const uint64_t row = base | row_off[quad * 32 + r];
+          const uint32_t e = c * 16 + 2 * j;
+          if (pair) {
+            *reinterpret_cast<float4*>(state + (row | elem_off[e])) = x;
+          } else {
+            state[row | elem_off[e]] = make_float2(x.x, x.y);
+            state[row | elem_off[e + 1]] = make_float2(x.z, x.w);
+          }
         }
+        __syncwarp();
       }
-      tc_fence_before();  // this accumulator is written again two tiles later
+      tc_fence_before();  // the accumulator is written again two tiles later
+      mbar_arrive(smem_addr(&acc_empty[accn]));
     }
-  }
-  // Let every MMA this CTA issued finish (bounded) before the accumulators are freed.
-  if (stages) {
-    const uint64_t last = stages - 1;
-    if (!mbar_wait_bounded(smem_addr(&mbar[last & 1u]), uint32_t(last >> 1) & 1u)) atomicExch(error_flag, 1);
-    if (last >= 1 && !mbar_wait_bounded(smem_addr(&mbar[(last - 1) & 1u]), uint32_t((last - 1) >> 1) & 1u))
-      atomicExch(error_flag, 1);
   }
   tc_fence_before();
   __syncthreads();
@@ -344,7 +409,8 @@ size_t tc_w_split_floats(int k) { return size_t(2) << (2 * (k + 1)); }
 size_t tc_shared_bytes(int k)
 {
   const size_t K = size_t(1) << (k + 1);
-  return 2 * K * K * 4 + 4 * size_t(kTcM) * (K / 4) * 4;  // W hi/lo + two A stages (hi/lo) of K/4 columns
+  // W hi/lo + two A stages (hi/lo) of K/4 columns + the epilogue's 4 x 4 KB turn-around
+  return 2 * K * K * 4 + 4 * size_t(kTcM) * (K / 4) * 4 + 4 * 32 * 32 * 4;
 }
 
 cudaError_t launch_unitary_tf32x3(void* state, int n, int k, const float* w_split, int* error_flag, int grid,
