@@ -64,6 +64,28 @@ enum op_kind : uint8_t {
                    // (mask dreg) in ascending bit order; applied as one straight-line block
 };
 
+// LAYER form 3, the factored layer: each gate M = [[a, b], [c, d]] of the layer is
+// written as
+//   M = diag(p0, p1) * [[1, t0], [t1, 1]] * diag(1, q),  |q| = 1, t0 and t1 real,
+// which exists when a and d are non-zero and b c / (a d) is real (every unitary
+// with a != 0).  Register slot i of a thread takes
+//   pre(i)  = product over the layer's bits b set in i of q_b        (skipped when every q is 1),
+//   post(i) = product over the layer's bits b of (bit b of i ? p1_b : p0_b),
+// around the middle factors, which cost four real multiply-adds per amplitude
+// pair (fourteen for the general 2x2 form).  Both diagonals are products over
+// bits, so each is stored as two factors: lo over register bits 0-1 (4 entries)
+// and hi over bits 2..R-1 (2^(R-2) entries), pre(i) = pre_lo[i & 3] pre_hi[i >> 2]
+// and the same for post (post_hi[0] = 1: the hi part's constant is moved into
+// post_lo).  A full 2^R-entry table took one constant load per amplitude and
+// kept the constant-load pipe 70 % busy; a shared-memory copy of it exposed the
+// load latency instead.  One table slot per layer holds, in the state's
+// precision, pre_lo[4], pre_hi[2^(R-2)], post_lo[4], post_hi[2^(R-2)].  The
+// member records hold t0, t1 in m[0], m[1]; the header holds its slot in dthr
+// and in diag_one whether the pre factors apply.
+constexpr int kLayerFactored = 3;
+constexpr int kMaxLayerTabs = 8;
+constexpr int kTabDoubles = 32;  // 256 bytes per slot
+
 // Dispatch key of a pass op: MAT ops are keyed by matrix form (0 general,
 // 1 real, 2 real m00), by whether register-bit controls exist and by the target
 // register bit; X and Y by the target bit; NEG, DIAG and PHASES by kind alone;
@@ -75,7 +97,7 @@ enum op_kind : uint8_t {
 #define RBK_HOST_DEVICE
 #endif
 // Dense codes 0 .. kNumOpCodes-1 (register bits 0..4), so that the kernel's
-// switch over them can be a jump table.
+// switch over them can be a jump table (LAYER forms 0..3: codes 43..50).
 RBK_HOST_DEVICE constexpr uint32_t op_code(int kind, int form, bool controlled, int treg)
 {
   return kind == OPK_MAT ? uint32_t((form * 2 + (controlled ? 1 : 0)) * 5 + treg)
@@ -84,7 +106,7 @@ RBK_HOST_DEVICE constexpr uint32_t op_code(int kind, int form, bool controlled, 
        : kind == OPK_NEG ? 40u : kind == OPK_DIAG ? 41u : kind == OPK_PHASES ? 42u
        : 43u + uint32_t(form * 2 + (controlled ? 1 : 0));
 }
-constexpr uint32_t kNumOpCodes = 49;
+constexpr uint32_t kNumOpCodes = 51;
 
 // One gate inside a pass, in the coordinates of the phase it belongs to.
 struct alignas(8) dev_op {
@@ -167,6 +189,7 @@ struct dev_pass {
   dev_hbm_layout load, store;
   dev_phase phases[kMaxPhases];
   dev_op ops[kMaxPassOps];
+  alignas(16) double tabs[kMaxLayerTabs * kTabDoubles];  // factored layers' diagonal factors (complex<double> or complex<float>)
 };
 
 // Per-gate (unfused) program record, used for states smaller than one tile

@@ -28,6 +28,8 @@
 #include "rbk_plan.h"
 
 #include <algorithm>
+#include <cmath>
+#include <complex>
 #include <cstring>
 #include <limits>
 #include <stdexcept>
@@ -390,7 +392,97 @@ int layer_form(int a, int b)
   return -1;
 }
 
-void group_layers(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_end, int& headers_left)
+// M = diag(p0, p1) * [[1, t0], [t1, 1]] * diag(1, q) for the factored layer
+// (kLayerFactored in rbk_internal.h): q = e^{i (arg b - arg a)} makes
+// t0 = |b| / |a| real, and t1 = c q / d is real when b c / (a d) is, as for every
+// unitary.  false: a or d is zero, t1 is not real to 4e-15, or |t0| or |t1|
+// exceeds 2^10 (a gate close to an X: the middle factor would grow the
+// amplitudes by up to that much per gate; complex<float> has the smaller range).
+struct gate_factors {
+  double t0, t1;
+  std::complex<double> p0, p1, q;
+};
+
+bool factor_gate(const double* m, gate_factors& f)
+{
+  using cd = std::complex<double>;
+  const cd a{m[0], m[1]}, b{m[2], m[3]}, c{m[4], m[5]}, d{m[6], m[7]};
+  const double na = std::abs(a), nb = std::abs(b), nd = std::abs(d);
+  if (na == 0.0 || nd == 0.0) return false;
+  f.q = nb > 0.0 ? (b / a) / std::abs(b / a) : cd{1.0, 0.0};
+  f.p0 = a;
+  f.p1 = d / f.q;
+  f.t0 = nb / na;
+  const cd w1 = c * f.q / d;
+  if (!(std::abs(w1.imag()) <= 4e-15 * std::max(1.0, std::abs(w1)))) return false;
+  f.t1 = w1.real();
+  constexpr double kMaxT = 1024.0;
+  return std::abs(f.t0) <= kMaxT && std::abs(f.t1) <= kMaxT;
+}
+
+// Rewrites the LAYER whose header is ops[0] (its members follow) into the
+// factored form when every member factors and a table slot is free.  The slot
+// is written in the state's precision (complex<float> entries for vbits 1).
+bool factor_layer(const plan_params& p, dev_pass& out, dev_op* ops, int& tabs_used)
+{
+  dev_op& h = ops[0];
+  const int run = static_cast<int>(h.run);
+  if (run < p.factored_min || tabs_used + 1 > kMaxLayerTabs) return false;
+  const int H = 1 << (p.R - 2);
+  if ((8 + 2 * H) * (p.vbits == 0 ? 16 : 8) > kTabDoubles * 8) throw std::logic_error("planner: layer table too small");
+  std::vector<gate_factors> f(static_cast<size_t>(run));
+  for (int k = 0; k < run; ++k)
+    if (!factor_gate(ops[1 + k].m, f[static_cast<size_t>(k)])) return false;
+  // Per register bit: q, p0, p1 (1 for bits outside the layer).
+  using cd = std::complex<double>;
+  std::vector<cd> q(static_cast<size_t>(p.R), 1.0), p0(static_cast<size_t>(p.R), 1.0), p1(static_cast<size_t>(p.R), 1.0);
+  bool any_q = false;
+  for (int k = 0; k < run; ++k) {
+    const gate_factors& g = f[static_cast<size_t>(k)];
+    const size_t b = ops[1 + k].treg;
+    q[b] = g.q;
+    p0[b] = g.p0;
+    p1[b] = g.p1;
+    any_q = any_q || g.q != cd{1.0, 0.0};
+  }
+  // Products over bits [lo, lo + count) of the entry's index bits.
+  auto pre_part = [&](int lo, int count, int x) {
+    cd v = 1.0;
+    for (int b = 0; b < count; ++b) if ((x >> b) & 1) v *= q[static_cast<size_t>(lo + b)];
+    return v;
+  };
+  auto post_part = [&](int lo, int count, int x) {
+    cd v = 1.0;
+    for (int b = 0; b < count; ++b) v *= ((x >> b) & 1) ? p1[static_cast<size_t>(lo + b)] : p0[static_cast<size_t>(lo + b)];
+    return v;
+  };
+  std::vector<cd> slot;  // pre_lo[4], pre_hi[H], post_lo[4], post_hi[H]
+  for (int l = 0; l < 4; ++l) slot.push_back(pre_part(0, 2, l));
+  for (int h = 0; h < H; ++h) slot.push_back(pre_part(2, p.R - 2, h));
+  const cd hi0 = post_part(2, p.R - 2, 0);
+  for (int l = 0; l < 4; ++l) slot.push_back(post_part(0, 2, l) * hi0);
+  for (int h = 0; h < H; ++h) slot.push_back(post_part(2, p.R - 2, h) / hi0);
+  double* tab = out.tabs + tabs_used * kTabDoubles;
+  float* t32 = reinterpret_cast<float*>(tab);
+  for (size_t i = 0; i < slot.size(); ++i) {
+    if (p.vbits == 0) { tab[2 * i] = slot[i].real(); tab[2 * i + 1] = slot[i].imag(); }
+    else { t32[2 * i] = static_cast<float>(slot[i].real()); t32[2 * i + 1] = static_cast<float>(slot[i].imag()); }
+  }
+  for (int k = 0; k < run; ++k) {
+    dev_op& g = ops[1 + k];
+    std::memset(g.m, 0, sizeof(g.m));
+    g.m[0] = f[static_cast<size_t>(k)].t0;
+    g.m[1] = f[static_cast<size_t>(k)].t1;
+  }
+  h.real = kLayerFactored;
+  h.dthr = static_cast<uint32_t>(tabs_used);
+  h.diag_one = any_q ? 1 : 0;
+  h.code = op_code(OPK_LAYER, kLayerFactored, h.dreg == (1u << p.R) - 1, 0);
+  tabs_used += 1;
+  return true;
+}
+
+void group_layers(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_end, int& headers_left, int& tabs_used)
 {
   const int begin = dp.op_begin;
   std::vector<dev_op> list(out.ops + begin, out.ops + op_end);
@@ -419,6 +511,7 @@ void group_layers(const plan_params& p, dev_pass& out, dev_phase& dp, int& op_en
       std::vector<dev_op> run(list.begin() + static_cast<long>(i), list.begin() + static_cast<long>(j));
       std::sort(run.begin(), run.end(), [](const dev_op& x, const dev_op& y) { return x.treg < y.treg; });
       grouped.insert(grouped.end(), run.begin(), run.end());
+      if (p.factored_min > 0) factor_layer(p, out, &grouped[grouped.size() - run.size() - 1], tabs_used);
     } else {
       if (j == i) ++j;
       for (size_t k = i; k < j; ++k) grouped.push_back(list[k]);
@@ -475,6 +568,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
 
   int op_index = 0;
   int headers_left = kMaxPassOps - kMaxPassGates;
+  int tabs_used = 0;
   for (size_t ph = 0; ph < phases.size(); ++ph) {
     auto& pb = phases[ph];
     const bool first = ph == 0, last = ph + 1 == phases.size();
@@ -649,7 +743,7 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
     }
     if (p.fold_x) fold_trailing_x(p, out, dp, op_index, last && ds ? smode : 0);
     if (p.phase_runs) group_phase_runs(p, out, dp, op_index, headers_left);
-    if (p.layers) group_layers(p, out, dp, op_index, headers_left);
+    if (p.layers) group_layers(p, out, dp, op_index, headers_left, tabs_used);
     dp.op_end = static_cast<uint16_t>(op_index);
   }
   out.num_phases = static_cast<uint8_t>(phases.size());

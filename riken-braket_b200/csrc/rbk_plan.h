@@ -35,6 +35,7 @@ struct plan_params {
   bool defer_x = true;   // register phases take CNOT / X gates last (so that they fold)
   bool phase_runs = true;  // runs of phase gates behind one PHASES header
   bool layers = true;      // uncontrolled 2x2 gates on distinct register bits behind one LAYER header
+  int factored_min = 3;    // layers of at least this many gates take the factored form (0: never)
 };
 
 // Plans `gates` (in order) into passes, updating the layout map

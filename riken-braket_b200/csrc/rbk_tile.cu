@@ -237,11 +237,71 @@ __device__ __forceinline__ void apply_layer(typename ctype<Real>::c* a, const de
   }
 }
 
+// The middle factor [[1, t0], [t1, 1]] of a factored layer's gate on register
+// bit B (kLayerFactored in rbk_internal.h): four real multiply-adds per pair.
+template <typename Real, int B, int NR>
+__device__ __forceinline__ void apply_factor(typename ctype<Real>::c* a, Real t0, Real t1)
+{
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    if (i & (1 << B)) continue;
+    auto& a0 = a[i];
+    auto& a1 = a[i | (1 << B)];
+    const Real x = madd(t0, a1.x, a0.x), y = madd(t0, a1.y, a0.y);
+    a1.x = madd(t1, a0.x, a1.x);
+    a1.y = madd(t1, a0.y, a1.y);
+    a0.x = x;
+    a0.y = y;
+  }
+}
+
+template <typename Real, int R, bool FULL, int B = 0>
+__device__ __forceinline__ void apply_factors(typename ctype<Real>::c* a, const dev_op* g, uint32_t mask)
+{
+  if constexpr (B < R) {
+    if (FULL || ((mask >> B) & 1u)) {
+      apply_factor<Real, B, 1 << R>(a, (Real)g->m[0], (Real)g->m[1]);
+      ++g;
+    }
+    apply_factors<Real, R, FULL, B + 1>(a, g, mask);
+  }
+}
+
+// A factored LAYER: the pre factors (when the header asks for them), the
+// middle factor of each member, the post factors.  The header's slot holds
+// pre_lo[4], pre_hi[2^(R-2)], post_lo[4], post_hi[2^(R-2)] in the state's
+// precision; slot i of the registers takes lo[i & 3] hi[i >> 2] (pre_lo[0],
+// pre_hi[0] and post_hi[0] are 1 and are not applied).
+template <typename Real, int R, bool FULL>
+__device__ __forceinline__ void apply_factored_layer(typename ctype<Real>::c* a, const dev_op& h, const double* tabs)
+{
+  using C = typename ctype<Real>::c;
+  constexpr int NR = 1 << R, H = 1 << (R - 2);
+  const C* pre_lo = reinterpret_cast<const C*>(tabs + h.dthr * kTabDoubles);
+  const C* pre_hi = pre_lo + 4;
+  const C* post_lo = pre_hi + H;
+  const C* post_hi = post_lo + 4;
+  if (h.diag_one) {
+#pragma unroll
+    for (int i = 1; i < NR; ++i) {
+      if (i & 3) a[i] = cmul(a[i], pre_lo[i & 3]);
+      if (i >> 2) a[i] = cmul(a[i], pre_hi[i >> 2]);
+    }
+  }
+  apply_factors<Real, R, FULL>(a, &h + 1, h.dreg);
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    a[i] = cmul(a[i], post_lo[i & 3]);
+    if (i >> 2) a[i] = cmul(a[i], post_hi[i >> 2]);
+  }
+}
+
 // One jump per op: the host encodes (kind, matrix form, controls, target bit)
 // into op.code (see op_code in rbk_internal.h).  Returns how many of the
 // following op records the op consumed (a phase run's gates).
 template <typename Real, int R>
-__device__ __forceinline__ int apply_op(typename ctype<Real>::c* a, const dev_op& op, uint32_t tid, uint64_t base)
+__device__ __forceinline__ int apply_op(typename ctype<Real>::c* a, const dev_op& op, uint32_t tid, uint64_t base,
+                                        const double* tabs)
 {
   using C = typename ctype<Real>::c;
   constexpr int NR = 1 << R;
@@ -305,6 +365,12 @@ __device__ __forceinline__ int apply_op(typename ctype<Real>::c* a, const dev_op
     RBK_LAYER_CASE(1, false) RBK_LAYER_CASE(1, true)
     RBK_LAYER_CASE(2, false) RBK_LAYER_CASE(2, true)
 #undef RBK_LAYER_CASE
+    case op_code(OPK_LAYER, kLayerFactored, false, 0):
+      apply_factored_layer<Real, R, false>(a, op, tabs);
+      return static_cast<int>(op.run);
+    case op_code(OPK_LAYER, kLayerFactored, true, 0):
+      apply_factored_layer<Real, R, true>(a, op, tabs);
+      return static_cast<int>(op.run);
     default: break;
   }
   return 0;
@@ -457,7 +523,7 @@ __device__ __forceinline__ void tile_phases(typename ctype<Real>::c* __restrict_
       }
     }
 
-    for (int o = ph.op_begin; o < ph.op_end; ++o) o += apply_op<Real, R>(a, P.ops[o], tid, base);
+    for (int o = ph.op_begin; o < ph.op_end; ++o) o += apply_op<Real, R>(a, P.ops[o], tid, base, P.tabs);
 
     if (p + 1 == nph && P.direct_store) {
       // A one-phase pass that also loaded straight from HBM: every warp of the
