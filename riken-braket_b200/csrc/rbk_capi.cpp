@@ -1257,9 +1257,12 @@ struct device_buffer {
 constexpr int kOverlapTileBits128 = 11, kOverlapTileBits64 = 12;
 
 // Overlaps of one group on the device, with as few reads of the states as
-// possible: one tiled launch covers every overlap whose flip bit is among the
-// launch's tile bits (the low coalescing bits plus up to K - LOW chosen ones);
-// Z-type overlaps (no flip) ride along in the first launch.
+// possible.  One-qubit Paulis (the rotation runs' EX, EY, EZ): every Z type in
+// one two-state Z-sum launch, X and Y types as pair sums, up to eight flip bits
+// per launch (rbk::launch_zsum2, rbk::launch_pair_overlaps).  Anything else:
+// one tiled launch covers every overlap whose flip bit is among the launch's
+// tile bits (the low coalescing bits plus up to K - LOW chosen ones), Z-type
+// overlaps (no flip) riding along in the first launch.
 int launch_group_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
                           const std::vector<rbk::overlap_spec>& specs, int first_slot, double* ov, double* mpart,
                           double* tpart);
@@ -1275,15 +1278,126 @@ struct rbk::adjoint_workspace {
   int ov_cap = 0;
   double* mpart = nullptr;
   double* tpart = nullptr;  // tiled overlaps (n >= tile bits)
+  double* ppart = nullptr;  // Z sums and pair sums (n >= 8 + kPairRegBits)
   ~adjoint_workspace()
   {
     if (ov) cudaFree(ov);
     if (mpart) cudaFree(mpart);
     if (tpart) cudaFree(tpart);
+    if (ppart) cudaFree(ppart);
     if (lam) rbk_state_destroy(lam);
     if (psi) rbk_state_destroy(psi);
   }
 };
+
+constexpr int kPairTileBits = 8 + rbk::kPairRegBits;
+constexpr int kPairLowBits = 3;  // tile bits always on the lowest physical bits: 128-byte runs
+
+size_t zsum2_partials_doubles() { return size_t(1 << 17) / 256 * 2 * (rbk::kMaxQubits + 1); }
+
+// The one-qubit-Pauli overlaps of `specs` (see launch_group_overlaps); marks
+// those it schedules in `done`.
+int launch_paired_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
+                           const std::vector<rbk::overlap_spec>& specs, int first_slot, double* ov,
+                           std::vector<char>& done)
+{
+  const bool c128 = w.precision == RBK_C128;
+  const int n = w.n;
+  cudaError_t e = cudaSuccess;
+  std::vector<size_t> zs, xs;  // Z type; X / Y type
+  for (size_t y = 0; y < specs.size(); ++y) {
+    const auto& sp = specs[y];
+    if (sp.flip == 0 && __builtin_popcountll(sp.sign) == 1) zs.push_back(y);
+    else if (__builtin_popcountll(sp.flip) == 1 && (sp.sign == 0 || sp.sign == sp.flip)) xs.push_back(y);
+  }
+  for (size_t c0 = 0; c0 < zs.size(); c0 += rbk::kMaxOverlaps) {
+    rbk::zsum2_set set{};
+    set.count = static_cast<int>(std::min<size_t>(rbk::kMaxOverlaps, zs.size() - c0));
+    for (int k = 0; k < set.count; ++k) {
+      const auto& sp = specs[zs[c0 + k]];
+      set.spec[k].bit = __builtin_ctzll(sp.sign);
+      set.spec[k].out_slot = first_slot + static_cast<int>(zs[c0 + k]);
+      set.spec[k].wr = sp.wr;
+      set.spec[k].wi = sp.wi;
+    }
+    e = c128 ? rbk::launch_zsum2<double>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream)
+             : rbk::launch_zsum2<float>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "Z-sum overlaps");
+    for (int k = 0; k < set.count; ++k) done[zs[c0 + k]] = 1;
+  }
+  // Pair groups: the low kPairLowBits bits plus up to 8 more tile bits; the
+  // flips of a group are up to kMaxPairFlips of the remaining X / Y types.
+  constexpr int RB = rbk::kPairRegBits, KT = kPairTileBits;
+  size_t next = 0;
+  while (next < xs.size()) {
+    std::vector<int> tile_bits;
+    for (int b = 0; b < kPairLowBits; ++b) tile_bits.push_back(b);
+    std::vector<size_t> mine;
+    uint64_t flips = 0;
+    while (next < xs.size() && static_cast<int>(mine.size()) < rbk::kMaxPairFlips) {
+      const int b = __builtin_ctzll(specs[xs[next]].flip);
+      const bool in = std::find(tile_bits.begin(), tile_bits.end(), b) != tile_bits.end();
+      if ((flips >> b) & 1) break;  // one register bit per flip in a group
+      if (!in && static_cast<int>(tile_bits.size()) >= KT) break;
+      flips |= 1ull << b;
+      if (!in) tile_bits.push_back(b);
+      mine.push_back(xs[next++]);
+    }
+    for (int b = 0; static_cast<int>(tile_bits.size()) < KT; ++b)  // fillers
+      if (std::find(tile_bits.begin(), tile_bits.end(), b) == tile_bits.end()) tile_bits.push_back(b);
+    std::sort(tile_bits.begin(), tile_bits.end());
+    rbk::pair_overlap_set set{};
+    rbk::spin_group& g = set.g;
+    g.K = KT;
+    uint64_t mask = 0;
+    for (int b = 0; b < KT; ++b) { g.tile_phys[b] = static_cast<uint8_t>(tile_bits[static_cast<size_t>(b)]); mask |= 1ull << tile_bits[static_cast<size_t>(b)]; }
+    std::vector<int> local;
+    for (size_t y : mine) {
+      const int b = __builtin_ctzll(specs[y].flip);
+      local.push_back(static_cast<int>(std::find(tile_bits.begin(), tile_bits.end(), b) - tile_bits.begin()));
+    }
+    g.nflips = static_cast<int>(mine.size());
+    g.nphases = (g.nflips + RB - 1) / RB;
+    for (int p = 0; p < g.nphases; ++p) {
+      std::vector<int> regs;
+      for (int k = 0; k < RB; ++k) {
+        const int f = p * RB + k;
+        if (f < g.nflips) regs.push_back(local[static_cast<size_t>(f)]);
+      }
+      for (int b = 0; static_cast<int>(regs.size()) < RB; ++b)  // fillers: other tile bits
+        if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
+      int nt = 0;
+      for (int b = 0; b < KT; ++b)
+        if (std::find(regs.begin(), regs.end(), b) == regs.end()) g.phase_thr[p][nt++] = static_cast<uint8_t>(b);
+      for (int k = 0; k < RB; ++k) g.phase_reg[p][k] = static_cast<uint8_t>(regs[static_cast<size_t>(k)]);
+    }
+    int runs = 0, src = 0;
+    for (int q = 0; q < n;) {
+      if ((mask >> q) & 1) { ++q; continue; }
+      int len = 0;
+      while (q + len < n && !((mask >> (q + len)) & 1)) ++len;
+      g.run_src[runs] = static_cast<uint8_t>(src);
+      g.run_len[runs] = static_cast<uint8_t>(len);
+      g.run_dst[runs] = static_cast<uint8_t>(q);
+      ++runs;
+      src += len;
+      q += len;
+    }
+    g.num_runs = runs;
+    for (size_t f = 0; f < mine.size(); ++f) {
+      const auto& sp = specs[mine[f]];
+      set.flip[f].out_slot = first_slot + static_cast<int>(mine[f]);
+      set.flip[f].minus = sp.sign != 0 ? 1 : 0;
+      set.flip[f].wr = sp.wr;
+      set.flip[f].wi = sp.wi;
+    }
+    e = c128 ? rbk::launch_pair_overlaps<double>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream)
+             : rbk::launch_pair_overlaps<float>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pair overlaps");
+    for (size_t y : mine) done[y] = 1;
+  }
+  return RBK_OK;
+}
 
 int launch_group_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
                           const std::vector<rbk::overlap_spec>& specs, int first_slot, double* ov, double* mpart,
@@ -1294,6 +1408,13 @@ int launch_group_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_s
   const int K = c128 ? kOverlapTileBits128 : kOverlapTileBits64;
   const int LOW = c128 ? rbk::precision_traits<double>::LOW : rbk::precision_traits<float>::LOW;
   cudaError_t e = cudaSuccess;
+  std::vector<char> done(specs.size(), 0);
+  if (n >= kPairTileBits && w.ppart) {
+    if (int rc = launch_paired_overlaps(w, lam, psi, specs, first_slot, ov, done)) return rc;
+    bool all = true;
+    for (char d : done) all = all && d;
+    if (all) return RBK_OK;
+  }
   if (n < K || !tpart) {
     for (size_t c0 = 0; c0 < specs.size(); c0 += rbk::kMaxOverlaps) {
       rbk::overlap_set set{};
@@ -1307,15 +1428,16 @@ int launch_group_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_s
     return RBK_OK;
   }
   std::vector<int> high;
-  for (const auto& sp : specs)
-    if (sp.flip) {
+  for (size_t y = 0; y < specs.size(); ++y) {
+    const auto& sp = specs[y];
+    if (sp.flip && !done[y]) {
       const int b = __builtin_ctzll(sp.flip);
       if (b >= LOW && std::find(high.begin(), high.end(), b) == high.end()) high.push_back(b);
     }
+  }
   std::sort(high.begin(), high.end());
   const int per = K - LOW;
   const int chunks = std::max<int>(1, static_cast<int>((high.size() + per - 1) / per));
-  std::vector<char> done(specs.size(), 0);
   for (int c = 0; c < chunks; ++c) {
     uint64_t tmask = (1ull << LOW) - 1;
     int tile_phys[16];
@@ -1398,6 +1520,9 @@ int rbk::adjoint_workspace_create(int num_qubits, int precision, int device, adj
     const int K = precision == RBK_C128 ? kOverlapTileBits128 : kOverlapTileBits64;
     if (num_qubits >= K)
       RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&w->tpart), sizeof(double) * rbk::tile_overlaps_partials_doubles(num_qubits, K)));
+    if (num_qubits >= kPairTileBits)
+      RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&w->ppart),
+                          sizeof(double) * std::max(rbk::pair_overlaps_partials_doubles(), zsum2_partials_doubles())));
     *out = w.release();
     return RBK_OK;
   });

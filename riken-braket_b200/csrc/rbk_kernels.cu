@@ -699,6 +699,259 @@ cudaError_t launch_tile_overlaps(const void* lam, const void* psi, int n, const 
   finish_tile_overlaps_kernel<<<set.count, 32, 0, stream>>>(partials, int(tiles), set, out);
   return cudaGetLastError();
 }
+// zsum2_set (rbk_kernels.h): exactly 2^kZsumLogThreads threads, thread gid
+// visiting indices (k << kZsumLogThreads) | gid as in zsum_kernel.  Per block
+// the partial sums of c_j = conj(lam_j) psi_j: the total, then for every bit q
+// the sum over j with bit q set.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads)
+zsum2_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename ctype<Real>::c* __restrict__ psi, int n,
+             double* partials)
+{
+  constexpr int HI = kMaxQubits - kZsumLogThreads;
+  const uint64_t size = 1ull << n;
+  const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+  double tr = 0, ti = 0, hr[HI], hi[HI];
+#pragma unroll
+  for (int k = 0; k < HI; ++k) hr[k] = hi[k] = 0;
+  for (uint64_t k = 0; (k << kZsumLogThreads) + gid < size; ++k) {
+    const uint64_t j = (k << kZsumLogThreads) | gid;
+    const auto l = __ldcs(lam + j), p = __ldcs(psi + j);
+    const double cr = double(l.x) * double(p.x) + double(l.y) * double(p.y);
+    const double ci = double(l.x) * double(p.y) - double(l.y) * double(p.x);
+    tr += cr;
+    ti += ci;
+#pragma unroll
+    for (int b = 0; b < HI; ++b)
+      if ((k >> b) & 1) { hr[b] += cr; hi[b] += ci; }
+  }
+  double vals[2 * (1 + kMaxQubits)];
+  vals[0] = tr;
+  vals[1] = ti;
+  for (int q = 0; q < n; ++q) {
+    double a = 0, c = 0;
+    if (q < kZsumLogThreads) {
+      if ((gid >> q) & 1) { a = tr; c = ti; }
+    } else {
+#pragma unroll
+      for (int b = 0; b < HI; ++b)
+        if (b == q - kZsumLogThreads) { a = hr[b]; c = hi[b]; }
+    }
+    vals[2 + 2 * q] = a;
+    vals[3 + 2 * q] = c;
+  }
+  block_sum_store<2 * (1 + kMaxQubits)>(vals, 2 * (n + 1), partials + size_t(blockIdx.x) * 2 * (n + 1));
+}
+
+// One warp per entry: S_q = total - 2 (sum over bit q set), out = w S_q.
+__global__ void finish_zsum2_kernel(const double* __restrict__ partials, int blocks, int n,
+                                    const __grid_constant__ zsum2_set set, double* __restrict__ out)
+{
+  const int lane = threadIdx.x & 31, width = 2 * (n + 1);
+  const int q = set.spec[blockIdx.x].bit;
+  double tr = 0, ti = 0, or_ = 0, oi = 0;
+  for (int b = lane; b < blocks; b += 32) {
+    const double* p = partials + size_t(b) * width;
+    tr += p[0];
+    ti += p[1];
+    or_ += p[2 + 2 * q];
+    oi += p[3 + 2 * q];
+  }
+  tr = warp_sum(tr);
+  ti = warp_sum(ti);
+  or_ = warp_sum(or_);
+  oi = warp_sum(oi);
+  if (lane == 0) {
+    const double sr = tr - 2.0 * or_, si = ti - 2.0 * oi;
+    const double wr = set.spec[blockIdx.x].wr, wi = set.spec[blockIdx.x].wi;
+    const int slot = set.spec[blockIdx.x].out_slot;
+    out[2 * slot] = sr * wr - si * wi;
+    out[2 * slot + 1] = sr * wi + si * wr;
+  }
+}
+
+template <typename Real>
+cudaError_t launch_zsum2(const void* lam, const void* psi, int n, const zsum2_set& set, double* partials, double* out,
+                         cudaStream_t stream)
+{
+  if (set.count < 1 || set.count > kMaxOverlaps || n < 1 || n > kMaxQubits) return cudaErrorInvalidValue;
+  for (int y = 0; y < set.count; ++y)
+    if (set.spec[y].bit < 0 || set.spec[y].bit >= n) return cudaErrorInvalidValue;
+  const int blocks = (1 << kZsumLogThreads) / kRedThreads;
+  zsum2_kernel<Real><<<blocks, kRedThreads, 0, stream>>>(static_cast<const typename ctype<Real>::c*>(lam),
+                                                          static_cast<const typename ctype<Real>::c*>(psi), n, partials);
+  finish_zsum2_kernel<<<set.count, 32, 0, stream>>>(partials, blocks, n, set, out);
+  return cudaGetLastError();
+}
+
+// pair_overlap_set (rbk_kernels.h): persistent CTAs, two per SM, each taking
+// tiles blockIdx.x, + gridDim.x, ...; both states' tiles of 2^11 amplitudes
+// sit in shared memory at the fused pass's swizzled slots.  In register phase
+// p a thread holds the 8 amplitudes of each state whose tile bits
+// phase_reg[p][0..2] vary; flip f = 3 p + k is register bit k of phase p.
+constexpr int kPairBlocksPerSm = 2;
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads, kPairBlocksPerSm)
+pair_overlaps_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename ctype<Real>::c* __restrict__ psi,
+                     const __grid_constant__ pair_overlap_set PS, uint64_t num_tiles, double* partials)
+{
+  const spin_group& S = PS.g;
+  using C = typename ctype<Real>::c;
+  constexpr int VB = precision_traits<Real>::VB;
+  constexpr int RB = kPairRegBits, NE = 1 << RB, KT = 8 + RB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tl = reinterpret_cast<C*>(smem_raw);
+  C* tp = tl + (1u << KT);
+  const uint32_t tid = threadIdx.x;
+  uint64_t tphys = 0;
+  for (int b = 0; b < 8; ++b) tphys |= uint64_t((tid >> b) & 1u) << S.tile_phys[b];
+  const uint32_t st = smem_slot<VB>(tid);
+  uint32_t sbase[kSpinPhases];
+#pragma unroll
+  for (int p = 0; p < kSpinPhases; ++p) {
+    uint32_t j = 0;
+    if (p < S.nphases)
+      for (int b = 0; b < 8; ++b) j |= ((tid >> b) & 1u) << S.phase_thr[p][b];
+    sbase[p] = smem_slot<VB>(j);
+  }
+  // A_f + s_f B_f per flip (s_f = -1 for Y type), which is all the result needs.
+  double xr[kMaxPairFlips], xi[kMaxPairFlips];
+#pragma unroll
+  for (int f = 0; f < kMaxPairFlips; ++f) xr[f] = xi[f] = 0.0;
+  for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+    uint64_t base = tphys;
+    for (int r = 0; r < S.num_runs; ++r) base |= ((t >> S.run_src[r]) & ((1ull << S.run_len[r]) - 1)) << S.run_dst[r];
+    C vl[NE], vp[NE];
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      uint64_t p = base;
+#pragma unroll
+      for (int b = 0; b < RB; ++b)
+        if ((it >> b) & 1) p |= 1ull << S.tile_phys[8 + b];
+      vl[it] = __ldcs(lam + p);
+      vp[it] = __ldcs(psi + p);
+    }
+    __syncthreads();  // the previous tile is no longer read
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      const uint32_t s = st ^ smem_slot<VB>(uint32_t(it) << 8);
+      tl[s] = vl[it];
+      tp[s] = vp[it];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kSpinPhases; ++p) {
+      if (p < S.nphases) {
+        uint32_t rs[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) rs[k] = smem_slot<VB>(1u << S.phase_reg[p][k]);
+        C el[NE], ep[NE];
+#pragma unroll
+        for (int i = 0; i < NE; ++i) {
+          uint32_t sidx = sbase[p];
+#pragma unroll
+          for (int k = 0; k < RB; ++k)
+            if ((i >> k) & 1) sidx ^= rs[k];
+          el[i] = tl[sidx];
+          ep[i] = tp[sidx];
+        }
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+          const int f = p * RB + k;
+          if (f < kMaxPairFlips && f < S.nflips) {
+            const double s = PS.flip[f].minus ? -1.0 : 1.0;
+#pragma unroll
+            for (int i = 0; i < NE; ++i) {
+              if ((i >> k) & 1) continue;
+              const C l0 = el[i], l1 = el[i | (1 << k)], p0 = ep[i], p1 = ep[i | (1 << k)];
+              const double ar = double(l0.x) * double(p1.x) + double(l0.y) * double(p1.y);
+              const double ai = double(l0.x) * double(p1.y) - double(l0.y) * double(p1.x);
+              const double br = double(l1.x) * double(p0.x) + double(l1.y) * double(p0.y);
+              const double bi = double(l1.x) * double(p0.y) - double(l1.y) * double(p0.x);
+              xr[f] += __fma_rn(s, br, ar);
+              xi[f] += __fma_rn(s, bi, ai);
+            }
+          }
+        }
+      }
+    }
+  }
+  // Block sums, in a fixed order: A_f + s_f B_f as 2 doubles per flip.
+  __shared__ double red[kRedThreads / 32][2 * kMaxPairFlips];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int f = 0; f < kMaxPairFlips; ++f) {
+    if (f < S.nflips) {
+      const double a0 = warp_sum(xr[f]), a1 = warp_sum(xi[f]);
+      if (lane == 0) { red[warp][2 * f] = a0; red[warp][2 * f + 1] = a1; }
+    }
+  }
+  __syncthreads();
+  const int width = 2 * S.nflips;
+  for (int k = threadIdx.x; k < width; k += blockDim.x) {
+    double acc = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) acc += red[w][k];
+    partials[size_t(blockIdx.x) * width + k] = acc;
+  }
+}
+
+// One warp per flip: A + s B over the blocks, then out = w (A + s B).
+__global__ void finish_pair_overlaps_kernel(const double* __restrict__ partials, int blocks, int nflips,
+                                            const __grid_constant__ pair_overlap_set set, double* __restrict__ out)
+{
+  const int lane = threadIdx.x & 31, f = blockIdx.x, width = 2 * nflips;
+  double xr = 0, xi = 0;
+  for (int b = lane; b < blocks; b += 32) {
+    xr += partials[size_t(b) * width + 2 * f];
+    xi += partials[size_t(b) * width + 2 * f + 1];
+  }
+  xr = warp_sum(xr);
+  xi = warp_sum(xi);
+  if (lane == 0) {
+    const double wr = set.flip[f].wr, wi = set.flip[f].wi;
+    const int slot = set.flip[f].out_slot;
+    out[2 * slot] = xr * wr - xi * wi;
+    out[2 * slot + 1] = xr * wi + xi * wr;
+  }
+}
+
+size_t pair_overlaps_partials_doubles() { return size_t(148) * kPairBlocksPerSm * 2 * kMaxPairFlips; }
+
+template <typename Real>
+cudaError_t launch_pair_overlaps(const void* lam, const void* psi, int n, const pair_overlap_set& set, double* partials,
+                                 double* out, cudaStream_t stream)
+{
+  const spin_group& g = set.g;
+  if (g.K != 8 + kPairRegBits || g.K > n || g.nflips < 1 || g.nflips > kMaxPairFlips || g.nphases < 1 ||
+      g.nphases > kSpinPhases || g.nphases * kPairRegBits < g.nflips)
+    return cudaErrorInvalidValue;
+  const size_t smem = 2 * sizeof(typename ctype<Real>::c) << g.K;
+  static std::atomic<bool> configured[64] = {};
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!configured[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(pair_overlaps_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured[dev].store(true, std::memory_order_release);
+  }
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t tiles = 1ull << (n - g.K);
+  // Capped at 148 SMs' worth: the partials buffer is sized for that.
+  const int blocks = static_cast<int>(std::min<uint64_t>(tiles, uint64_t(std::min(sms, 148)) * kPairBlocksPerSm));
+  pair_overlaps_kernel<Real><<<blocks, kRedThreads, smem, stream>>>(static_cast<const typename ctype<Real>::c*>(lam),
+                                                                   static_cast<const typename ctype<Real>::c*>(psi), set, tiles,
+                                                                   partials);
+  finish_pair_overlaps_kernel<<<g.nflips, 32, 0, stream>>>(partials, blocks, g.nflips, set, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_zsum2<double>(const void*, const void*, int, const zsum2_set&, double*, double*, cudaStream_t);
+template cudaError_t launch_zsum2<float>(const void*, const void*, int, const zsum2_set&, double*, double*, cudaStream_t);
+template cudaError_t launch_pair_overlaps<double>(const void*, const void*, int, const pair_overlap_set&, double*, double*, cudaStream_t);
+template cudaError_t launch_pair_overlaps<float>(const void*, const void*, int, const pair_overlap_set&, double*, double*, cudaStream_t);
+
 template cudaError_t launch_tile_overlaps<double>(const void*, const void*, int, const tile_overlap_set&, double*, double*, cudaStream_t);
 template cudaError_t launch_tile_overlaps<float>(const void*, const void*, int, const tile_overlap_set&, double*, double*, cudaStream_t);
 

@@ -83,6 +83,7 @@ struct tile_overlap_set {
   tile_overlap_spec spec[kMaxOverlaps];
 };
 size_t tile_overlaps_partials_doubles(int n, int K);
+
 template <typename Real> cudaError_t launch_tile_overlaps(const void* lam, const void* psi, int n, const tile_overlap_set& set,
                                                           double* partials, double* out, cudaStream_t stream);
 
@@ -108,6 +109,31 @@ struct spin_group {
 inline int spin_register_bits(int precision) { return precision == 0 ? 3 : 4; }
 template <typename Real> cudaError_t launch_spins(const void* state, int n, const spin_group& g, double* partials, double* out,
                                                   cudaStream_t stream);
+
+// Overlaps of one-qubit Paulis in one read of both states (the adjoint sweep's
+// rotation runs).  Z type: S_q = sum_j (-1)^{j_q} conj(lam_j) psi_j for
+// physical bit q; out[2 slot] = w * S_q for each entry.
+struct zsum2_set {
+  int count, pad;
+  struct { int32_t bit, out_slot; double wr, wi; } spec[kMaxOverlaps];
+};
+// X / Y type, for the flips of one tile layout (spin_group with K = 11: three
+// register bits and eight thread bits, both states' tiles in shared memory):
+//   A_f = sum over j with tile bit b_f clear of conj(lam_j) psi_{j | b_f},
+//   B_f = the same with lam and psi exchanged in position (conj(lam_{j | b_f}) psi_j),
+// out[2 slot_f] = w_f (A_f + B_f) (X, minus 0) or w_f (A_f - B_f) (Y: minus 1,
+// the sign bit is the flip).
+constexpr int kMaxPairFlips = 8;
+constexpr int kPairRegBits = 3;
+struct pair_overlap_set {
+  spin_group g;
+  struct { int32_t out_slot, minus; double wr, wi; } flip[kMaxPairFlips];
+};
+size_t pair_overlaps_partials_doubles();
+template <typename Real> cudaError_t launch_zsum2(const void* lam, const void* psi, int n, const zsum2_set& set,
+                                                  double* partials, double* out, cudaStream_t stream);
+template <typename Real> cudaError_t launch_pair_overlaps(const void* lam, const void* psi, int n, const pair_overlap_set& set,
+                                                          double* partials, double* out, cudaStream_t stream);
 
 // Sampling: prefix = inclusive scan of |a_i|^2 (scratch: scan_scratch_doubles(count)
 // doubles); events[k] = upper_bound(prefix, r[k]).

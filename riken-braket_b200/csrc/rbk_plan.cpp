@@ -320,9 +320,66 @@ void fold_trailing_x(const plan_params& p, dev_pass& out, dev_phase& dp, int& op
 // and the header's dout holds the class sizes, one byte each in that order
 // (the last class takes the rest of `run`).  The gates of a run commute, so
 // their order is free.
-bool is_phase_op(const dev_op& d)
+// A diagonal gate diag(d0, d1) with d0 != 1 (EZ: d0 = e^{i theta}) joins a run
+// as two members: d0 on its controls alone (an empty condition: every
+// amplitude) and d1 / d0 on its controls and target.  Members with the same
+// condition are then multiplied into one, and members whose factor is exactly
+// 1 dropped.  (A per-member sign parity for the factor -1, two multiply chains
+// and branch-free selects in the kernel's run loop were measured too: the
+// adjoint sweep gained nothing from them and the QFT workload lost 6-9 %.)
+bool is_phase_op(const dev_op& d, bool general)
 {
-  return d.kind == OPK_NEG || (d.kind == OPK_DIAG && d.diag_one && d.m[0] == 1.0 && d.m[1] == 0.0);
+  if (d.kind == OPK_NEG || (d.kind == OPK_DIAG && d.diag_one && d.m[0] == 1.0 && d.m[1] == 0.0)) return true;
+  return general && d.kind == OPK_DIAG && (d.m[0] != 0.0 || d.m[1] != 0.0);
+}
+
+// The members of a run of phase ops list[i..j) (see is_phase_op).
+std::vector<dev_op> phase_members(const std::vector<dev_op>& list, size_t i, size_t j)
+{
+  using cd = std::complex<double>;
+  std::vector<dev_op> members;
+  auto add = [&](dev_op g, cd f) {
+    for (dev_op& m : members)
+      if (m.creg == g.creg && m.cthr == g.cthr && m.cout == g.cout) {
+        const cd v = cd{m.m[2], m.m[3]} * f;
+        m.m[2] = v.real();
+        m.m[3] = v.imag();
+        return;
+      }
+    g.m[2] = f.real();
+    g.m[3] = f.imag();
+    members.push_back(g);
+  };
+  for (size_t k = i; k < j; ++k) {
+    dev_op g = list[k];
+    const dev_op orig = g;
+    g.kind = OPK_DIAG;
+    g.diag_one = 1;
+    g.m[0] = 1.0;
+    g.m[1] = 0.0;
+    g.m[4] = g.m[5] = g.m[6] = g.m[7] = 0.0;
+    if (orig.kind == OPK_NEG) {
+      add(g, cd{-1.0, 0.0});
+      continue;
+    }
+    const cd d0{orig.m[0], orig.m[1]}, d1{orig.m[2], orig.m[3]};
+    if (!orig.diag_one || d0 != cd{1.0, 0.0}) {  // d0 on the controls alone
+      dev_op c = g;
+      c.dreg = c.dthr = 0;
+      c.dout = 0;
+      add(c, d0);
+    }
+    g.creg |= g.dreg;
+    g.cthr |= g.dthr;
+    g.cout |= g.dout;
+    g.dreg = g.dthr = 0;
+    g.dout = 0;
+    add(g, (!orig.diag_one || d0 != cd{1.0, 0.0}) ? d1 / d0 : d1);
+  }
+  std::vector<dev_op> kept;
+  for (const dev_op& m : members)
+    if (!(m.m[2] == 1.0 && m.m[3] == 0.0)) kept.push_back(m);
+  return kept;
 }
 
 // headers_left: headers the pass may still add (kMaxPassOps - kMaxPassGates in
@@ -333,25 +390,20 @@ void group_phase_runs(const plan_params& p, dev_pass& out, dev_phase& dp, int& o
   std::vector<dev_op> list(out.ops + begin, out.ops + op_end);
   std::vector<dev_op> grouped;
   for (size_t i = 0; i < list.size();) {
+    // Runs take general diagonals when the extra member records fit in the
+    // records kept back for headers; otherwise only the phase form.
     size_t j = i;
-    while (j < list.size() && is_phase_op(list[j])) ++j;
+    while (j < list.size() && is_phase_op(list[j], true)) ++j;
+    std::vector<dev_op> members;
     if (j - i >= 2 && headers_left > 0) {
-      std::vector<dev_op> members;
-      for (size_t k = i; k < j; ++k) {
-        dev_op g = list[k];
-        const bool neg = g.kind == OPK_NEG;
-        g.creg |= g.dreg;
-        g.cthr |= g.dthr;
-        g.cout |= g.dout;
-        g.dreg = g.dthr = 0;
-        g.dout = 0;
-        g.kind = OPK_DIAG;
-        g.diag_one = 1;
-        g.m[0] = 1.0;
-        g.m[1] = 0.0;
-        if (neg) { g.m[2] = -1.0; g.m[3] = 0.0; }
-        members.push_back(g);
+      members = phase_members(list, i, j);
+      if (static_cast<int>(members.size()) - static_cast<int>(j - i) > headers_left - 1 || members.empty()) {
+        j = i;
+        while (j < list.size() && is_phase_op(list[j], false)) ++j;
+        members = j - i >= 2 ? phase_members(list, i, j) : std::vector<dev_op>{};
       }
+    }
+    if (j - i >= 2 && headers_left > 0 && !members.empty()) {
       auto cls = [&](const dev_op& g) {
         const int c = __builtin_popcount(g.creg);
         return c == 0 ? 0 : c == 1 ? 1 + __builtin_ctz(g.creg) : 1 + p.R;
@@ -359,14 +411,14 @@ void group_phase_runs(const plan_params& p, dev_pass& out, dev_phase& dp, int& o
       std::stable_sort(members.begin(), members.end(), [&](const dev_op& x, const dev_op& y) { return cls(x) < cls(y); });
       dev_op h{};
       h.kind = OPK_PHASES;
-      h.run = static_cast<uint32_t>(j - i);
+      h.run = static_cast<uint32_t>(members.size());
       h.code = op_code(OPK_PHASES, 0, true, 0);
       for (const dev_op& g : members) {
         const int c = cls(g);
         if (c <= p.R) h.dout += 1ull << (8 * c);
       }
       grouped.push_back(h);
-      --headers_left;
+      headers_left -= 1 + std::max(0, static_cast<int>(members.size()) - static_cast<int>(j - i));
       grouped.insert(grouped.end(), members.begin(), members.end());
     } else {
       if (j == i) ++j;  // a gate that is not a phase

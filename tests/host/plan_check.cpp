@@ -149,7 +149,7 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
                                    : op_code(op.kind, 0, true, 0);
           if (op.code != want_code || op.code >= kNumOpCodes || op.treg >= R) { std::fprintf(stderr, "bad dispatch code\n"); std::exit(8); }
           if (op.kind == OPK_PHASES) {  // a run header: the run's gates follow, each a factor on the amplitudes whose bits are all one
-            if (op.run < 2 || o + static_cast<int>(op.run) >= D.op_end) { std::fprintf(stderr, "bad phase run\n"); std::exit(14); }
+            if (op.run < 1 || o + static_cast<int>(op.run) >= D.op_end) { std::fprintf(stderr, "bad phase run\n"); std::exit(14); }
             // class sizes (no register bit, register bit 0 .. R-1; the rest: two or more register bits)
             int bound[9], sum = 0;
             for (int c = 0; c <= R; ++c) { sum += static_cast<int>((op.dout >> (8 * c)) & 0xff); bound[c] = sum; }

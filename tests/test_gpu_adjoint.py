@@ -67,11 +67,12 @@ def test_adjoint_config4_20_qubits(pkg):
         assert abs(g[k] - shift) <= 1e-9
 
 
-def test_adjoint_general_gates_and_c64(pkg):
+@pytest.mark.parametrize("n", [7, 13])
+def test_adjoint_general_gates_and_c64(pkg, n):
     """Fixed gates of every kind around the rotations (exact inverses in the
-    reverse sweep); complex<float> against the FP64 result."""
+    reverse sweep); complex<float> against the FP64 result.  At 13 qubits the
+    EX / EY / EZ overlaps come from the two-state Z-sum and pair-sum kernels."""
     C = pkg.circuits
-    n = 7
     rng = np.random.default_rng(3)
     spec, k = [], 0
     for _ in range(3):
