@@ -346,7 +346,7 @@ typedef struct rbk_batch_stats {
 } rbk_batch_stats;
 int rbk_batch_create(int precision, int device, int num_instances, const rbk_batch_instance* instances, rbk_batch** out);
 int rbk_batch_run(rbk_batch* batch, const double* theta, double* energies, double* grads);
-/* Host threads that drive the larger instances concurrently (default 4). */
+/* Host threads that drive the larger instances concurrently (default 8). */
 int rbk_batch_set_workers(rbk_batch* batch, int workers);
 int rbk_batch_get_stats(const rbk_batch* batch, rbk_batch_stats* out);
 int rbk_batch_destroy(rbk_batch* batch);

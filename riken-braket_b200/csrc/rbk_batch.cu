@@ -357,7 +357,7 @@ struct rbk_batch {
   std::vector<std::vector<double>> large_coeffs;
   rbk_batch_stats stats{};
   // Worker threads for the large instances, each with its own workspaces by size.
-  int workers = 4;
+  int workers = 8;
   std::vector<std::map<int, rbk::adjoint_workspace*>> pools;
 
   ~rbk_batch()

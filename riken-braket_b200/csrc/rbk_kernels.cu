@@ -702,7 +702,9 @@ cudaError_t launch_tile_overlaps(const void* lam, const void* psi, int n, const 
 // zsum2_set (rbk_kernels.h): exactly 2^kZsumLogThreads threads, thread gid
 // visiting indices (k << kZsumLogThreads) | gid as in zsum_kernel.  Per block
 // the partial sums of c_j = conj(lam_j) psi_j: the total, then for every bit q
-// the sum over j with bit q set.
+// the sum over j with bit q set.  k runs in groups of 8 where it can: the
+// group's three low bits of k are known at compile time, and its higher bits
+// add the group's sum once instead of once per amplitude.
 template <typename Real>
 __global__ void __launch_bounds__(kRedThreads)
 zsum2_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename ctype<Real>::c* __restrict__ psi, int n,
@@ -714,16 +716,43 @@ zsum2_kernel(const typename ctype<Real>::c* __restrict__ lam, const typename cty
   double tr = 0, ti = 0, hr[HI], hi[HI];
 #pragma unroll
   for (int k = 0; k < HI; ++k) hr[k] = hi[k] = 0;
-  for (uint64_t k = 0; (k << kZsumLogThreads) + gid < size; ++k) {
-    const uint64_t j = (k << kZsumLogThreads) | gid;
-    const auto l = __ldcs(lam + j), p = __ldcs(psi + j);
-    const double cr = double(l.x) * double(p.x) + double(l.y) * double(p.y);
-    const double ci = double(l.x) * double(p.y) - double(l.y) * double(p.x);
-    tr += cr;
-    ti += ci;
+  const uint64_t ks = size >> kZsumLogThreads;  // k values of every thread (n >= kZsumLogThreads)
+  if (ks >= 8) {
+    for (uint64_t m = 0; m < ks / 8; ++m) {
+      double gr = 0, gi = 0, r0 = 0, i0 = 0, r1 = 0, i1 = 0, r2 = 0, i2 = 0;
 #pragma unroll
-    for (int b = 0; b < HI; ++b)
-      if ((k >> b) & 1) { hr[b] += cr; hi[b] += ci; }
+      for (int r = 0; r < 8; ++r) {
+        const uint64_t j = ((m * 8 + r) << kZsumLogThreads) | gid;
+        const auto l = __ldcs(lam + j), p = __ldcs(psi + j);
+        const double cr = double(l.x) * double(p.x) + double(l.y) * double(p.y);
+        const double ci = double(l.x) * double(p.y) - double(l.y) * double(p.x);
+        gr += cr;
+        gi += ci;
+        if (r & 1) { r0 += cr; i0 += ci; }
+        if (r & 2) { r1 += cr; i1 += ci; }
+        if (r & 4) { r2 += cr; i2 += ci; }
+      }
+      tr += gr;
+      ti += gi;
+      hr[0] += r0; hi[0] += i0;
+      hr[1] += r1; hi[1] += i1;
+      hr[2] += r2; hi[2] += i2;
+#pragma unroll
+      for (int b = 3; b < HI; ++b)
+        if ((m >> (b - 3)) & 1) { hr[b] += gr; hi[b] += gi; }
+    }
+  } else {
+    for (uint64_t k = 0; (k << kZsumLogThreads) + gid < size; ++k) {
+      const uint64_t j = (k << kZsumLogThreads) | gid;
+      const auto l = __ldcs(lam + j), p = __ldcs(psi + j);
+      const double cr = double(l.x) * double(p.x) + double(l.y) * double(p.y);
+      const double ci = double(l.x) * double(p.y) - double(l.y) * double(p.x);
+      tr += cr;
+      ti += ci;
+#pragma unroll
+      for (int b = 0; b < HI; ++b)
+        if ((k >> b) & 1) { hr[b] += cr; hi[b] += ci; }
+    }
   }
   double vals[2 * (1 + kMaxQubits)];
   vals[0] = tr;

@@ -447,7 +447,8 @@ int layer_form(int a, int b)
 // M = diag(p0, p1) * [[1, t0], [t1, 1]] * diag(1, q) for the factored layer
 // (kLayerFactored in rbk_internal.h): q = e^{i (arg b - arg a)} makes
 // t0 = |b| / |a| real, and t1 = c q / d is real when b c / (a d) is, as for every
-// unitary.  false: a or d is zero, t1 is not real to 4e-15, or |t0| or |t1|
+// unitary.  When b / a is already real (real matrices: H, EY) q = 1 and t0 = b / a,
+// so that a layer of such gates needs no pre factors.  false: a or d is zero, t1 is not real to 4e-15, or |t0| or |t1|
 // exceeds 2^10 (a gate close to an X: the middle factor would grow the
 // amplitudes by up to that much per gate; complex<float> has the smaller range).
 struct gate_factors {
@@ -461,10 +462,16 @@ bool factor_gate(const double* m, gate_factors& f)
   const cd a{m[0], m[1]}, b{m[2], m[3]}, c{m[4], m[5]}, d{m[6], m[7]};
   const double na = std::abs(a), nb = std::abs(b), nd = std::abs(d);
   if (na == 0.0 || nd == 0.0) return false;
-  f.q = nb > 0.0 ? (b / a) / std::abs(b / a) : cd{1.0, 0.0};
+  const cd r = b / a;
+  if (nb == 0.0 || std::abs(r.imag()) <= 4e-15 * std::abs(r.real())) {
+    f.q = cd{1.0, 0.0};
+    f.t0 = r.real();
+  } else {
+    f.q = r / std::abs(r);
+    f.t0 = nb / na;
+  }
   f.p0 = a;
   f.p1 = d / f.q;
-  f.t0 = nb / na;
   const cd w1 = c * f.q / d;
   if (!(std::abs(w1.imag()) <= 4e-15 * std::max(1.0, std::abs(w1)))) return false;
   f.t1 = w1.real();
