@@ -520,7 +520,8 @@ bool factor_layer(const plan_params& p, dev_pass& out, dev_op* ops, int& tabs_us
   for (int h = 0; h < H; ++h) slot.push_back(pre_part(2, p.R - 2, h));
   const cd hi0 = post_part(2, p.R - 2, 0);
   for (int l = 0; l < 4; ++l) slot.push_back(post_part(0, 2, l) * hi0);
-  for (int h = 0; h < H; ++h) slot.push_back(post_part(2, p.R - 2, h) / hi0);
+  slot.push_back(1.0);  // post_hi[0] is exactly 1: the kernel skips it
+  for (int h = 1; h < H; ++h) slot.push_back(post_part(2, p.R - 2, h) / hi0);
   double* tab = out.tabs + tabs_used * kTabDoubles;
   float* t32 = reinterpret_cast<float*>(tab);
   for (size_t i = 0; i < slot.size(); ++i) {

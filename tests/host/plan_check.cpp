@@ -204,7 +204,8 @@ static void run_pass(std::vector<cplx>& st, const plan_params& p, const dev_pass
                 return cplx{f[2 * i], f[2 * i + 1]};
               };
               if (entry(0) != cplx{1.0, 0.0} || entry(4) != cplx{1.0, 0.0} || entry(8 + H) != cplx{1.0, 0.0}) {
-                std::fprintf(stderr, "a layer factor that the kernel skips is not 1\n");
+                std::fprintf(stderr, "a layer factor that the kernel skips is not 1 (%.17g %.17g / %.17g %.17g / %.17g %.17g)\n",
+                             entry(0).real(), entry(0).imag(), entry(4).real(), entry(4).imag(), entry(8 + H).real(), entry(8 + H).imag());
                 std::exit(19);
               }
               if (op.diag_one)
@@ -319,6 +320,42 @@ static std::vector<hgate> brick_gates(std::mt19937_64& rng, int n, int depth)
   return out;
 }
 
+// The adjoint ansatz: EY (real rotation) and EZ (diagonal) on every qubit, then a CZ ring.
+static std::vector<hgate> ansatz_gates(std::mt19937_64& rng, int n, int depth)
+{
+  std::uniform_real_distribution<double> ang(-3.0, 3.0);
+  std::vector<hgate> out;
+  for (int l = 0; l < depth; ++l) {
+    for (int q = 0; q < n; ++q) {
+      hgate g{};
+      g.kind = OPK_MAT;
+      g.target = static_cast<int8_t>(q);
+      g.target2 = -1;
+      const double t = ang(rng);
+      g.m[0] = std::cos(t); g.m[2] = std::sin(t); g.m[4] = -std::sin(t); g.m[6] = std::cos(t);
+      out.push_back(g);
+    }
+    for (int q = 0; q < n; ++q) {
+      hgate g{};
+      g.kind = OPK_DIAG;
+      g.target = static_cast<int8_t>(q);
+      g.target2 = -1;
+      const double t = ang(rng);
+      g.m[0] = std::cos(t); g.m[1] = std::sin(t); g.m[2] = std::cos(t); g.m[3] = -std::sin(t);
+      out.push_back(g);
+    }
+    for (int q = 0; q < n; ++q) {
+      hgate g{};
+      g.kind = OPK_NEG;
+      g.target = -1;
+      g.target2 = -1;
+      g.cmask = (1ull << q) | (1ull << ((q + 1) % n));
+      out.push_back(g);
+    }
+  }
+  return out;
+}
+
 // phase_heavy: mostly diagonal gates and sign flips between dense ones, so
 // that register phases hold many short runs of phase gates.
 static hgate random_gate(std::mt19937_64& rng, int n, bool phase_heavy = false)
@@ -371,7 +408,8 @@ int main(int argc, char** argv)
       std::vector<hgate> gates;
       const int count = 50 + static_cast<int>(rng() % 300);
       const bool phase_heavy = seed % 2 == 1;
-      if (seed % 3 == 2) gates = brick_gates(rng, p.n, 2 + static_cast<int>(rng() % 6));
+      if (seed % 6 == 5) gates = ansatz_gates(rng, p.n, 1 + static_cast<int>(rng() % 4));
+      else if (seed % 3 == 2) gates = brick_gates(rng, p.n, 2 + static_cast<int>(rng() % 6));
       else for (int i = 0; i < count; ++i) gates.push_back(random_gate(rng, p.n, phase_heavy));
 
       std::vector<cplx> want = init;
