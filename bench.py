@@ -318,11 +318,51 @@ def run_gpu(args):
         "clocks": clk,
     }
     s.close()
+    if rank == 0 and world == 1 and not args.no_secondary:
+        line["secondary"] = secondary_workloads(pkg)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier(device_ids=[local])
         dist.destroy_process_group()
+
+
+def secondary_workloads(pkg):
+    """Configs 4 and 5 measured after the headline's timed region, so that the
+    default run records them too: the 20-qubit adjoint gradient on a kept
+    context (rbk_adjoint_run; 3 warm-up, 10 timed) and the 4096-instance
+    complex<double> batch (rbk_batch_run; 1 warm-up, 1 timed).  Host wall clock
+    around calls that return results to the host (each call ends synchronised)."""
+    A, C = pkg.adjoint, pkg.circuits
+    out = {}
+    n, layers = 20, 16
+    terms = C.ansatz_hamiltonian(n)
+    _, theta = C.ansatz(n, layers, seed=SEED)
+    spec, _ = A.ansatz_spec(n, layers)
+    ctx = A.AdjointContext(n)
+    for _ in range(3):
+        ctx.gradient(spec, theta, terms)
+    t0 = time.perf_counter()
+    for _ in range(10):
+        ctx.gradient(spec, theta, terms)
+    out["adjoint_20q_640_params"] = {"ms_per_gradient": (time.perf_counter() - t0) / 10 * 1e3,
+                                     "workload": "energy + gradient, 20-qubit ansatz, 16 layers, 640 parameters"}
+    ctx.close()
+    inst, thetas = [], []
+    for nq, lay, th in C.batch_instances(4096):
+        sp, k = A.ansatz_spec(nq, lay)
+        inst.append((nq, sp, k, C.ansatz_hamiltonian(nq)))
+        thetas.append(th)
+    b = A.Batch(inst, precision=pkg.C128)
+    b.run(thetas)
+    t0 = time.perf_counter()
+    b.run(thetas)
+    secs = time.perf_counter() - t0
+    out["batch_4096_c128"] = {"seconds": secs, "instances_per_s": len(inst) / secs,
+                              "workload": "4096 ansatz instances, n log-uniform in [10, 24], depth U{4..16}, "
+                                          "energies + adjoint gradients"}
+    b.close()
+    return out
 
 
 def run_reference(args):
@@ -588,6 +628,7 @@ def main():
     ap.add_argument("--impl", default="rbk", choices=["rbk", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of CPU reference work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the config-4 / config-5 timings after the headline")
     ap.add_argument("--ref-blocks-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=N_QUBITS, help="smaller cases for profiling only")
     ap.add_argument("--depth", type=int, default=DEPTH)
