@@ -652,8 +652,9 @@ void build_pass(const plan_params& p, uint64_t tile_mask, const std::vector<pop>
         for (int b : bits) if (contains(pb.reg, b)) return false;
         return true;
       };
-      if (off(lanes_of(1, map)) && (!p.vbits || contains(pb.reg, map[0]) || static_cast<int>(pb.reg.size()) < R)) return 1;
-      if (p.vbits && off(lanes_of(2, map))) return 2;
+      // the lanes' HBM bits must be tile bits in every tile: the fixed low bits
+      if (lane0 + 5 <= p.LOW && off(lanes_of(1, map)) && (!p.vbits || contains(pb.reg, map[0]) || static_cast<int>(pb.reg.size()) < R)) return 1;
+      if (p.vbits && 5 <= p.LOW && off(lanes_of(2, map))) return 2;
       return 0;
     };
     const int lmode = first ? mode_for(identity) : 0;
