@@ -328,13 +328,37 @@ def run_gpu(args):
 
 
 def secondary_workloads(pkg):
-    """Configs 4 and 5 measured after the headline's timed region, so that the
-    default run records them too: the 20-qubit adjoint gradient on a kept
-    context (rbk_adjoint_run; 3 warm-up, 10 timed) and the 4096-instance
-    complex<double> batch (rbk_batch_run; 1 warm-up, 1 timed).  Host wall clock
-    around calls that return results to the host (each call ends synchronised)."""
+    """Configs 3, 4 and 5 measured after the headline's timed region, so that
+    the default run records them too:
+    * the QFT + brick circuit: 33 qubits complex<double> (128 GiB) and
+      32 qubits complex<float> in both fusion modes, one warm-up and one timed
+      circuit each, CUDA events on the state's stream (rbk_state_device_ms);
+    * the 20-qubit adjoint gradient on a kept context (rbk_adjoint_run;
+      3 warm-up, 10 timed) and the 4096-instance complex<double> batch
+      (rbk_batch_run; 1 warm-up, 1 timed): host wall clock around calls that
+      return their results to the host."""
     A, C = pkg.adjoint, pkg.circuits
     out = {}
+
+    def circuit_ms(n, prec, mode):
+        ops = C.qft_brick(n, 5, seed=SEED, fuse_k=6)
+        s = pkg.State(n, prec)
+        s.set_fusion_mode(mode)
+        s.apply(ops)
+        s.synchronize()
+        s.reset(0)
+        s.synchronize()
+        s.reset_stats()
+        s.apply(ops)
+        s.synchronize()
+        ms, passes = s.device_ms(), s.stats()["passes"]
+        s.close()
+        return {"ms": ms, "passes": passes}
+
+    out["qft_brick"] = {"workload": "H j + U m j (m-j+1) for all m > j, then 5 seeded brick layers, fusion blocks of 6",
+                        "c128_33q": circuit_ms(33, pkg.C128, 0),
+                        "c64_32q_gate_by_gate": circuit_ms(32, pkg.C64, 0),
+                        "c64_32q_tensor_core_blocks": circuit_ms(32, pkg.C64, 1)}
     n, layers = 20, 16
     terms = C.ansatz_hamiltonian(n)
     _, theta = C.ansatz(n, layers, seed=SEED)
