@@ -3,7 +3,7 @@
 // Runs the reference's own C++ code for the state-vector hot path:
 // the header-only ket gate / observable functions from ket/include and bra's
 // fused-gate classes from bra/src/fused_*.cpp, compiled unchanged against the
-// project-written Boost shim in oracle/shim.  bra itself (bra::state,
+// project-written Boost stand-ins in riken-braket_b200/bra/shim.  bra itself (bra::state,
 // bra::nompi_state, the interpreter) needs Boost.Variant, fmt and cxxopts, which
 // are absent, so this file restates only the dispatch that bra::nompi_state
 // performs for each instruction and calls exactly the ket function it calls:

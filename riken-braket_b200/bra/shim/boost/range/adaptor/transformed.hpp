@@ -1,6 +1,6 @@
 // Project-written stand-in for `range | boost::adaptors::transformed(f)` as used
 // by the reference's ket headers (e.g. ket/include/ket/gate/phase_shift.hpp:2034).
-// Random-access only, which is all the reference needs.  Test infrastructure only.
+// Random-access only, which is all the reference needs.  Used to build the reference's code in this image, which has no Boost.
 #ifndef RBK_SHIM_BOOST_RANGE_ADAPTOR_TRANSFORMED_HPP
 #define RBK_SHIM_BOOST_RANGE_ADAPTOR_TRANSFORMED_HPP
 

@@ -1,5 +1,5 @@
 // Project-written stand-in for boost::iterator_range / make_iterator_range as
-// used by the reference's ket headers.  Test infrastructure only.
+// used by the reference's ket headers.  Used to build the reference's code in this image, which has no Boost.
 #ifndef RBK_SHIM_BOOST_RANGE_ITERATOR_RANGE_HPP
 #define RBK_SHIM_BOOST_RANGE_ITERATOR_RANGE_HPP
 

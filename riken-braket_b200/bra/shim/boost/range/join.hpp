@@ -1,7 +1,7 @@
 // Project-written stand-in for boost::join over two random-access ranges with
 // the same value type, as used by the reference's ket headers (e.g.
 // ket/include/ket/gate/phase_shift.hpp:2032).  Elements are yielded by value.
-// Test infrastructure only.
+// Used to build the reference's code in this image, which has no Boost.
 #ifndef RBK_SHIM_BOOST_RANGE_JOIN_HPP
 #define RBK_SHIM_BOOST_RANGE_JOIN_HPP
 

@@ -1,5 +1,5 @@
 // Project-written stand-in for boost::is_nothrow_swappable (used by the
-// reference's ket::mpi headers before C++17).  Test infrastructure only.
+// reference's ket::mpi headers before C++17).  Used to build the reference's code in this image, which has no Boost.
 #ifndef RBK_SHIM_BOOST_IS_NOTHROW_SWAPPABLE_HPP
 #define RBK_SHIM_BOOST_IS_NOTHROW_SWAPPABLE_HPP
 #include <type_traits>

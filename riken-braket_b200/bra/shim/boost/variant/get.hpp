@@ -1,0 +1,2 @@
+// Project-written stand-in (see variant.hpp).
+#include <boost/variant/variant.hpp>

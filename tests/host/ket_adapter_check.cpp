@@ -7,7 +7,7 @@
 // against the complex<double> ket run).
 //
 // Build (test infrastructure; needs ket's headers and the Boost stand-ins of
-// oracle/shim):  make -C oracle _ref/ket_adapter_check
+// riken-braket_b200/bra/shim):  make -C oracle _ref/ket_adapter_check
 #include <algorithm>
 #include <array>
 #include <cmath>

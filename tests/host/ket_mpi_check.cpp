@@ -12,7 +12,7 @@
 // complex<float> (both against the complex<double> ket::mpi run).
 //
 // Build (test infrastructure; needs ket's headers and the stand-ins of
-// oracle/shim; links librbk.so and the CUDA runtime, which reads the device
+// oracle/shim and riken-braket_b200/bra/shim; links librbk.so and the CUDA runtime, which reads the device
 // memory back):  make -C oracle _ref/ket_mpi_check
 #include <algorithm>
 #include <array>

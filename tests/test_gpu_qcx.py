@@ -16,42 +16,18 @@ import numpy as np
 import pytest
 
 from conftest import ROOT
+from qcx_compare import same_output
 
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 PROGRAMS = sorted(glob.glob(os.path.join(GOLDEN, "qcx", "*.qcx")))
 TOL64 = 1e-12
-NUM = re.compile(r"^[-+]?(\d+\.?\d*|\.\d+)([eE][-+]?\d+)?$")
 
 
 @pytest.fixture(scope="module")
 def expected():
     return json.load(open(os.path.join(GOLDEN, "qcx_expected.json"))), dict(np.load(os.path.join(GOLDEN, "qcx_golden.npz")))
-
-
-def last_digit(tok):
-    """Unit in the last printed digit of a decimal token."""
-    mant, _, exp = tok.lower().partition("e")
-    decimals = len(mant.split(".")[1]) if "." in mant else 0
-    return 10.0 ** (-decimals + (int(exp) if exp else 0))
-
-
-def same_output(got, want):
-    gl, wl = got.splitlines(), want.splitlines()
-    assert len(gl) == len(wl), (got, want)
-    for g, w in zip(gl, wl):
-        gt = re.split(r"([\s(),]+)", g)
-        wt = re.split(r"([\s(),]+)", w)
-        assert len(gt) == len(wt), (g, w)
-        for a, b in zip(gt, wt):
-            if NUM.match(b) and NUM.match(a):
-                if re.match(r"^[-+]?\d+$", b):  # integers (indices, bit strings, outcomes, a zero): equal values
-                    assert (a == b) if len(b) > 1 and set(b) <= {"0", "1"} else float(a) == float(b), (g, w)
-                else:
-                    assert abs(float(a) - float(b)) <= max(1e-12, 1.01 * last_digit(b)), (g, w)
-            elif a.strip() != b.strip():
-                assert a == b, (g, w)
 
 
 @pytest.mark.parametrize("path", PROGRAMS, ids=os.path.basename)

@@ -96,7 +96,7 @@ def test_ket_program_selects_device_overloads(tmp_path):
     iterators), so success means every call on the device state resolved to
     the overloads of rbk_ket.hpp."""
     cmd = ["g++", "-std=c++17", "-fsyntax-only", "-w", "-I", os.path.join(ROOT, "include"),
-           "-I", os.path.join(ROOT, "oracle", "shim"), "-I", KET_INCLUDE,
+           "-I", os.path.join(ROOT, "riken-braket_b200", "bra", "shim"), "-I", KET_INCLUDE,
            os.path.join(ROOT, "tests", "host", "ket_adapter_check.cpp")]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]

@@ -21,7 +21,8 @@ from conftest import REFERENCE, ROOT
 
 BINARY = os.path.join(ROOT, "oracle", "_ref", "ket_mpi_check")
 KET_INCLUDE = os.path.join(REFERENCE, "ket", "include")
-SHIM = os.path.join(ROOT, "oracle", "shim")
+SHIM = os.path.join(ROOT, "oracle", "shim")  # yampi
+BSHIM = os.path.join(ROOT, "riken-braket_b200", "bra", "shim")  # Boost
 needs_ket = pytest.mark.skipif(not os.path.isdir(KET_INCLUDE) or shutil.which("g++") is None,
                                reason="needs ket's headers and g++ (build machine only)")
 
@@ -70,7 +71,7 @@ def test_ket_mpi_header_compiles_as_cpp14_without_warnings(tmp_path):
     src = tmp_path / "ket_mpi_tu.cpp"
     src.write_text(_HEADER_TU)
     cmd = ["g++", "-std=c++14", "-fsyntax-only", "-Wall", "-Wextra", "-Werror",
-           "-I", os.path.join(ROOT, "include"), "-isystem", SHIM, "-isystem", KET_INCLUDE, str(src)]
+           "-I", os.path.join(ROOT, "include"), "-isystem", SHIM, "-isystem", BSHIM, "-isystem", KET_INCLUDE, str(src)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]
 
@@ -81,7 +82,7 @@ def test_ket_mpi_program_compiles_against_the_stand_in(tmp_path):
     single-process yampi stand-in, and the device overloads (a call that fell
     through to ket::mpi's CPU templates would not compile: the device state
     has no iterators)."""
-    cmd = ["g++", "-std=c++17", "-fsyntax-only", "-w", "-I", os.path.join(ROOT, "include"), "-I", SHIM,
+    cmd = ["g++", "-std=c++17", "-fsyntax-only", "-w", "-I", os.path.join(ROOT, "include"), "-I", SHIM, "-I", BSHIM,
            "-I", KET_INCLUDE, "-I", "/usr/local/cuda/include",
            os.path.join(ROOT, "tests", "host", "ket_mpi_check.cpp")]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -146,7 +147,7 @@ int main() {
 }
 """)
     exe = tmp_path / "stand_in"
-    cmd = ["g++", "-std=c++17", "-O1", "-w", "-I", SHIM, "-I", KET_INCLUDE, str(src), "-o", str(exe)]
+    cmd = ["g++", "-std=c++17", "-O1", "-w", "-I", SHIM, "-I", BSHIM, "-I", KET_INCLUDE, str(src), "-o", str(exe)]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr

@@ -137,7 +137,7 @@ def test_sampling_restatement_equals_reference_on_fresh_states(pkg, n):
 
 @pytest.mark.parametrize("prog", ["runtime_gate_numerical", "fused_runtime_gate_numerical", "runtime_observable_numerical"])
 def test_reference_own_tests_pass_with_shim(prog):
-    """The reference's ket/test/*.cpp, compiled unchanged against oracle/shim."""
+    """The reference's ket/test/*.cpp, compiled unchanged against the Boost stand-ins (riken-braket_b200/bra/shim)."""
     import subprocess
     path = os.path.join(ROOT, "oracle", "_ref", prog)
     if not os.path.exists(path):
