@@ -7,6 +7,7 @@ text exactly.  Timing lines ("... finished: t (dt)") are dropped first."""
 import re
 
 NUM = re.compile(r"^[-+]?(\d+\.?\d*|\.\d+)([eE][-+]?\d+)?$")
+INT = re.compile(r"^[-+]?\d+$")
 TIMING = re.compile(r"finished: [-+0-9.eE]+ \([-+0-9.eE]+\)$")
 
 
@@ -30,9 +31,11 @@ def same_output(got, want):
         assert len(gt) == len(wt), (g, w)
         for a, b in zip(gt, wt):
             if NUM.match(b) and NUM.match(a):
-                if re.match(r"^[-+]?\d+$", b):  # integers (indices, bit strings, outcomes, a zero): equal values
+                a_int, b_int = INT.match(a), INT.match(b)
+                if a_int and b_int:  # integers (indices, bit strings, outcomes, a zero): equal values
                     assert (a == b) if len(b) > 1 and set(b) <= {"0", "1"} else float(a) == float(b), (g, w)
-                else:
-                    assert abs(float(a) - float(b)) <= max(1e-12, 1.01 * last_digit(b)), (g, w)
+                else:  # a value printed as an integer on one side (a zero) takes the other side's digits
+                    unit = last_digit(a) if b_int else last_digit(b)
+                    assert abs(float(a) - float(b)) <= max(1e-12, 1.01 * unit), (g, w)
             elif a.strip() != b.strip():
                 assert a == b, (g, w)

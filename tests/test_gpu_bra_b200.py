@@ -5,8 +5,10 @@ and whose do_* backend calls the engine's C ABI.  It must print what the
 reference's own bra prints for the same .qcx text: the golden programs
 against tests/golden/qcx_expected.json and, where the reference's CPU build
 (oracle/_ref/bra) is at hand, against its output run for run; a 20-qubit
-fused brick against the reference's CPU run; the instructions the reference
-rejects, rejected with the same message."""
+fused brick, a program of bra's classical layer (VAR/LET/@label/JUMPIF with
+variables as gate operands) and a depolarizing-channel run, each against the
+reference's CPU run; the instructions the reference rejects, rejected with
+the same message."""
 import json
 import os
 import subprocess
@@ -80,6 +82,61 @@ def test_bra_b200_20_qubit_fused_brick_matches_reference_bra(expected):
         pytest.skip("oracle/_ref/bra was not built")
     text = brick_program(20, 10, 7)
     got, ref = run(B200, text), run(REF, text, "--threads", str(os.cpu_count() or 1))
+    assert got.returncode == 0 and ref.returncode == 0, got.stderr[-2000:] + ref.stderr[-2000:]
+    same_output(without_timings(got.stdout), without_timings(ref.stdout))
+
+
+CLASSICAL = """QUBITS 6
+VAR K INT
+VAR TH REAL
+VAR ACC COMPLEX
+LET K := 0
+LET TH := 0.3
+H 0
+H 1
+@LOOP
+U3 0 TH 0.2 0.1
+CNOT 0 1
+EZ 2 TH
+CNOT 1 2
+LET TH *= 1.5
+LET K += 1
+JUMPIF LOOP K < 4
+M 1
+PRINTLN K TH :OUTCOME
+VAR OP PAULISS
+LET OP := :PAULIS:ZZX
+EXPECTATION OP 0 1 2
+LET ACC := :RESULT
+PRINTLN ACC
+DO MEASUREMENT
+"""
+
+DEPOLARIZING = """QUBITS 8
+DEPOLARIZING CHANNEL P_X=0.05,P_Y=0.04,P_Z=0.03,SEED=17
+H 0
+CNOT 0 1
+U3 2 0.7 0.1 0.2
+BEGIN FUSION
+U3 3 0.4 0.5 0.6
+CNOT 3 4
+CZ 4 5
+END FUSION
+T 6
+CNOT 6 7
+DO MEASUREMENT 6
+DO AMPLITUDES 0 3 17 255
+"""
+
+
+@pytest.mark.parametrize("name,text,args", [
+    ("classical", CLASSICAL, ()), ("classical_seed5", CLASSICAL, ("--seed", "5")),
+    ("depolarizing", DEPOLARIZING, ()), ("depolarizing_own_seed", DEPOLARIZING.replace("SEED=17", "SEED=-1"), ("--seed", "3")),
+])
+def test_bra_b200_classical_layer_and_noise_match_reference_bra(expected, name, text, args):
+    if not os.path.exists(REF):
+        pytest.skip("oracle/_ref/bra was not built")
+    got, ref = run(B200, text, *args), run(REF, text, *args)
     assert got.returncode == 0 and ref.returncode == 0, got.stderr[-2000:] + ref.stderr[-2000:]
     same_output(without_timings(got.stdout), without_timings(ref.stdout))
 
