@@ -533,6 +533,7 @@ def run_batch(args):
         times[name] = (time.perf_counter() - t0) / args.steps
         results[name] = (e, g)
         stats[name] = b.stats()
+        stats[name]["tuned_tile_shapes"] = {str(k): v for k, v in b.tuned_shapes([d[0] for d in draws]).items()}
         b.close()
     e64, g64 = results["c128"]
     e32, g32 = results["c64"]

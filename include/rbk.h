@@ -349,6 +349,10 @@ int rbk_batch_run(rbk_batch* batch, const double* theta, double* energies, doubl
 /* Host threads that drive the larger instances concurrently (default 8). */
 int rbk_batch_set_workers(rbk_batch* batch, int workers);
 int rbk_batch_get_stats(const rbk_batch* batch, rbk_batch_stats* out);
+/* Tile shape (rbk_state_set_tile_shape: the fusion width of the fused passes)
+ * that the batch's autotuner picked for its instances of num_qubits qubits,
+ * or -1 where the default is kept (fewer than 16 qubits, or no such instance). */
+int rbk_batch_tuned_shape(const rbk_batch* batch, int num_qubits, int* shape);
 int rbk_batch_destroy(rbk_batch* batch);
 
 /* The same sweep on a context that keeps its two state vectors and buffers

@@ -146,6 +146,17 @@ class Batch:
         rbk.lib().rbk_batch_get_stats(self.h, ctypes.byref(st))
         return {f: getattr(st, f) for f, _ in BatchStats._fields_}
 
+    def tuned_shapes(self, sizes):
+        """{num_qubits: tile shape} that the autotuner picked (rbk_batch_tuned_shape; sizes left at the default omitted)."""
+        L = rbk.lib()
+        L.rbk_batch_tuned_shape.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        out = {}
+        for n in sorted(set(sizes)):
+            sh = ctypes.c_int(-1)
+            if L.rbk_batch_tuned_shape(self.h, int(n), ctypes.byref(sh)) == 0 and sh.value >= 0:
+                out[int(n)] = sh.value
+        return out
+
     def close(self):
         if getattr(self, "h", None):
             rbk.lib().rbk_batch_destroy(self.h)

@@ -12,7 +12,8 @@
 // replayed for every later parameter vector.  The CTA size is picked by an
 // autotuner that times the candidates on the batch's own small instances.
 // Larger instances run through the engine's adjoint sweep
-// (rbk_adjoint_gradient) one after the other.
+// (rbk_adjoint_gradient) on worker threads, with the fused passes' tile shape
+// (their fusion width) picked per qubit count by a second autotuner.
 //
 // The reference has no differentiation or batching; the gate arithmetic is
 // ket's (exponential_pauli_y.hpp:40-85, exponential_pauli_z.hpp:40-78,
@@ -359,6 +360,9 @@ struct rbk_batch {
   // Worker threads for the large instances, each with its own workspaces by size.
   int workers = 8;
   std::vector<std::map<int, rbk::adjoint_workspace*>> pools;
+  // Tile shape of the fused passes per qubit count of the large instances (the
+  // fusion width: 2^11 or 2^12 amplitudes per tile), picked by timing.
+  std::map<int, int> shape_of;
 
   ~rbk_batch()
   {
@@ -421,7 +425,64 @@ int sync_bounded(cudaStream_t s)
   }
 }
 
+// Fusion width of the large instances: for every qubit count from
+// kTuneMinQubits up, one instance of that size is run through the sweep with
+// each tile shape (2^11 amplitudes per tile in 4 CTAs per SM, 2^12 in 2, and
+// 2^11 in 3 persistent CTAs that prefetch), and the fastest shape is kept for
+// all instances of that size.  Below that size the default shape is kept: the
+// sweeps there are bound by launches, not by the passes.
+constexpr int kTuneMinQubits = 16;
+int tune_shapes(rbk_batch* b)
+{
+  std::map<int, size_t> rep;  // qubit count -> index into b->large of the first instance of that size
+  for (size_t k = 0; k < b->large.size(); ++k) {
+    const int nt = static_cast<int>(b->large_coeffs[k].size() / 2);
+    const int nq = static_cast<int>(b->large_strings[k].size() / static_cast<size_t>(nt));
+    if (nq >= kTuneMinQubits && !rep.count(nq)) rep.emplace(nq, k);
+  }
+  for (const auto& kv : rep) {
+    const int nq = kv.first;
+    const size_t k = kv.second;
+    const int i = b->large[k];
+    const auto& gs = b->large_gates[k];
+    const int nt = static_cast<int>(b->large_coeffs[k].size() / 2);
+    std::vector<double> theta(static_cast<size_t>(std::max(1, b->num_params[i])), 0.1);
+    std::vector<double> grad(theta.size());
+    double energy = 0.0;
+    rbk::adjoint_workspace* w = nullptr;
+    if (int rc = rbk::adjoint_workspace_create(nq, b->precision, b->device, &w)) return rc;
+    double best = 1e300;
+    int best_shape = 2;
+    int rc = RBK_OK;
+    for (int shape : {2, 0, 3}) {
+      rc = rbk::adjoint_workspace_set_shape(w, shape);
+      double ms = 1e300;
+      for (int r = 0; rc == RBK_OK && r < 3; ++r) {  // the first run warms up
+        const auto t0 = std::chrono::steady_clock::now();
+        rc = rbk::adjoint_run(w, gs.data(), static_cast<int>(gs.size()), theta.data(), b->num_params[i], nt,
+                              b->large_strings[k].data(), b->large_coeffs[k].data(), &energy, grad.data());
+        const double t = 1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (r > 0) ms = std::min(ms, t);
+      }
+      if (rc != RBK_OK) break;
+      if (ms < best) { best = ms; best_shape = shape; }
+    }
+    rbk::adjoint_workspace_destroy(w);
+    if (rc != RBK_OK) return rc;
+    b->shape_of[nq] = best_shape;
+  }
+  return RBK_OK;
+}
+
 }  // namespace
+
+extern "C" int rbk_batch_tuned_shape(const rbk_batch* b, int num_qubits, int* shape)
+{
+  if (!b || !shape) return fail(RBK_ERR_INVALID, "null argument");
+  const auto it = b->shape_of.find(num_qubits);
+  *shape = it == b->shape_of.end() ? -1 : it->second;
+  return RBK_OK;
+}
 
 extern "C" int rbk_batch_create(int precision, int device, int num_instances, const rbk_batch_instance* instances,
                                 rbk_batch** out)
@@ -572,6 +633,7 @@ extern "C" int rbk_batch_create(int precision, int device, int num_instances, co
       if (ce != cudaSuccess || cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess)
         return fail(RBK_ERR_CUDA, "graph instantiate");
     }
+    if (int rc = tune_shapes(b.get())) return rc;
     *out = b.release();
     return RBK_OK;
   } catch (std::bad_alloc const&) {
@@ -615,7 +677,10 @@ extern "C" int rbk_batch_run(rbk_batch* b, const double* theta, double* energies
           if (it == pool.end()) {
             rbk::adjoint_workspace* w = nullptr;
             rc = rbk::adjoint_workspace_create(nq, b->precision, b->device, &w);
+            const auto sh = b->shape_of.find(nq);
+            if (rc == RBK_OK && sh != b->shape_of.end()) rc = rbk::adjoint_workspace_set_shape(w, sh->second);
             if (rc == RBK_OK) it = pool.emplace(nq, w).first;
+            else if (w) rbk::adjoint_workspace_destroy(w);
           }
           if (rc == RBK_OK)
             rc = rbk::adjoint_run(it->second, gs.data(), static_cast<int>(gs.size()), theta + pb, b->num_params[i], nt,

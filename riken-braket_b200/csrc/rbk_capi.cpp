@@ -1399,6 +1399,135 @@ int launch_paired_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_
   return RBK_OK;
 }
 
+// Z-type overlaps (flip 0, one sign bit) of specs[idx...] in two-state Z-sum launches.
+int launch_z_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
+                      const std::vector<rbk::overlap_spec>& specs, const std::vector<size_t>& idx, int first_slot,
+                      double* ov)
+{
+  const bool c128 = w.precision == RBK_C128;
+  for (size_t c0 = 0; c0 < idx.size(); c0 += rbk::kMaxOverlaps) {
+    rbk::zsum2_set set{};
+    set.count = static_cast<int>(std::min<size_t>(rbk::kMaxOverlaps, idx.size() - c0));
+    for (int k = 0; k < set.count; ++k) {
+      const auto& sp = specs[idx[c0 + k]];
+      set.spec[k].bit = __builtin_ctzll(sp.sign);
+      set.spec[k].out_slot = first_slot + static_cast<int>(idx[c0 + k]);
+      set.spec[k].wr = sp.wr;
+      set.spec[k].wi = sp.wi;
+    }
+    const cudaError_t e = c128 ? rbk::launch_zsum2<double>(lam->amps, psi->amps, w.n, set, w.ppart, ov, psi->stream)
+                               : rbk::launch_zsum2<float>(lam->amps, psi->amps, w.n, set, w.ppart, ov, psi->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "Z-sum overlaps");
+  }
+  return RBK_OK;
+}
+
+// One gate of a fused reverse run on its physical bit: the 2x2 matrix of U^dagger
+// and, for a rotation, its X / Y-type overlap (slot < 0: none).
+struct rotate_item {
+  int bit;
+  int slot;
+  rbk::overlap_spec spec;
+  double m[8];
+};
+
+// Pair-rotate launches over `items`: tiles of the low kPairLowBits bits plus up
+// to 8 others, up to kMaxRotFlips gates per launch, in register phases of
+// kPairRegBits gates (the layout of launch_paired_overlaps).
+int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi, const std::vector<rotate_item>& items,
+                     double* ov)
+{
+  const bool c128 = w.precision == RBK_C128;
+  const int n = w.n;
+  constexpr int RB = rbk::kPairRegBits, KT = kPairTileBits;
+  size_t next = 0;
+  while (next < items.size()) {
+    std::vector<int> tile_bits;
+    for (int b = 0; b < kPairLowBits; ++b) tile_bits.push_back(b);
+    std::vector<size_t> mine;
+    while (next < items.size() && static_cast<int>(mine.size()) < rbk::kMaxRotFlips) {
+      const int b = items[next].bit;
+      const bool in = std::find(tile_bits.begin(), tile_bits.end(), b) != tile_bits.end();
+      if (!in && static_cast<int>(tile_bits.size()) >= KT) break;
+      if (!in) tile_bits.push_back(b);
+      mine.push_back(next++);
+    }
+    for (int b = 0; static_cast<int>(tile_bits.size()) < KT; ++b)  // fillers
+      if (std::find(tile_bits.begin(), tile_bits.end(), b) == tile_bits.end()) tile_bits.push_back(b);
+    std::sort(tile_bits.begin(), tile_bits.end());
+    rbk::pair_rotate_set set{};
+    rbk::spin_group& g = set.g;
+    g.K = KT;
+    uint64_t mask = 0;
+    for (int b = 0; b < KT; ++b) { g.tile_phys[b] = static_cast<uint8_t>(tile_bits[static_cast<size_t>(b)]); mask |= 1ull << tile_bits[static_cast<size_t>(b)]; }
+    std::vector<int> local;
+    for (size_t y : mine)
+      local.push_back(static_cast<int>(std::find(tile_bits.begin(), tile_bits.end(), items[y].bit) - tile_bits.begin()));
+    g.nflips = static_cast<int>(mine.size());
+    g.nphases = (g.nflips + RB - 1) / RB;
+    for (int p = 0; p < g.nphases; ++p) {
+      std::vector<int> regs;
+      for (int k = 0; k < RB; ++k) {
+        const int f = p * RB + k;
+        if (f < g.nflips) regs.push_back(local[static_cast<size_t>(f)]);
+      }
+      for (int b = 0; static_cast<int>(regs.size()) < RB; ++b)  // fillers: other tile bits, left alone
+        if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
+      int nt = 0;
+      for (int b = 0; b < KT; ++b)
+        if (std::find(regs.begin(), regs.end(), b) == regs.end()) g.phase_thr[p][nt++] = static_cast<uint8_t>(b);
+      for (int k = 0; k < RB; ++k) g.phase_reg[p][k] = static_cast<uint8_t>(regs[static_cast<size_t>(k)]);
+    }
+    int runs = 0, src = 0;
+    for (int q = 0; q < n;) {
+      if ((mask >> q) & 1) { ++q; continue; }
+      int len = 0;
+      while (q + len < n && !((mask >> (q + len)) & 1)) ++len;
+      g.run_src[runs] = static_cast<uint8_t>(src);
+      g.run_len[runs] = static_cast<uint8_t>(len);
+      g.run_dst[runs] = static_cast<uint8_t>(q);
+      ++runs;
+      src += len;
+      q += len;
+    }
+    g.num_runs = runs;
+    for (size_t f = 0; f < mine.size(); ++f) {
+      const rotate_item& it = items[mine[f]];
+      auto& fl = set.flip[f];
+      fl.out_slot = it.slot;
+      fl.minus = it.spec.sign != 0 ? 1 : 0;
+      fl.wr = it.spec.wr;
+      fl.wi = it.spec.wi;
+      std::memcpy(fl.m, it.m, sizeof(fl.m));
+    }
+    const cudaError_t e = c128 ? rbk::launch_pair_rotate<double>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream)
+                               : rbk::launch_pair_rotate<float>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pair rotations");
+  }
+  return RBK_OK;
+}
+
+bool queue_is_diagonal(const rbk_state* s)
+{
+  for (const hgate& h : s->queue)
+    if (h.kind != rbk::OPK_DIAG && h.kind != rbk::OPK_NEG) return false;
+  return true;
+}
+
+// The engine's record of U_g^dagger for a one-qubit circuit gate: what
+// apply_circuit_gate(s, g, theta, true) queues, taken back off s's queue.
+int inverse_record(rbk_state* s, const rbk_circuit_gate& g, const double* theta, hgate* out)
+{
+  const size_t mark = s->queue.size();
+  const auto issued = s->stats.gates_issued;
+  if (int rc = apply_circuit_gate(s, g, theta, true)) return rc;
+  if (s->queue.size() != mark + 1) return fail(RBK_ERR_STATE, "adjoint sweep: a one-qubit gate queued other than one record");
+  *out = s->queue.back();
+  s->queue.pop_back();
+  s->stats.gates_issued = issued;
+  return RBK_OK;
+}
+
 int launch_group_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
                           const std::vector<rbk::overlap_spec>& specs, int first_slot, double* ov, double* mpart,
                           double* tpart)
@@ -1522,10 +1651,19 @@ int rbk::adjoint_workspace_create(int num_qubits, int precision, int device, adj
       RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&w->tpart), sizeof(double) * rbk::tile_overlaps_partials_doubles(num_qubits, K)));
     if (num_qubits >= kPairTileBits)
       RBK_CUDA(cudaMalloc(reinterpret_cast<void**>(&w->ppart),
-                          sizeof(double) * std::max(rbk::pair_overlaps_partials_doubles(), zsum2_partials_doubles())));
+                          sizeof(double) * std::max({rbk::pair_overlaps_partials_doubles(), rbk::pair_rotate_partials_doubles(),
+                                                     zsum2_partials_doubles()})));
     *out = w.release();
     return RBK_OK;
   });
+}
+
+int rbk::adjoint_workspace_set_shape(adjoint_workspace* w, int shape)
+{
+  if (!w) return fail(RBK_ERR_INVALID, "null workspace");
+  device_guard dg(w->device);
+  if (int rc = rbk_state_set_tile_shape(w->psi, shape)) return rc;
+  return rbk_state_set_tile_shape(w->lam, shape);
 }
 
 void rbk::adjoint_workspace_destroy(adjoint_workspace* w)
@@ -1626,6 +1764,10 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
              g.kind == RBK_GATE_U1 || g.kind == RBK_GATE_U2 || g.kind == RBK_GATE_U3 || g.kind == RBK_GATE_EX ||
              g.kind == RBK_GATE_EY || g.kind == RBK_GATE_EZ;
     };
+    // Runs of one-qubit gates take the pair-rotate path where its tile fits
+    // (RBK_ADJOINT_PAIR_ROTATE=0 selects the overlap-then-queue path instead).
+    const char* pr_env = std::getenv("RBK_ADJOINT_PAIR_ROTATE");
+    const bool fused_runs = num_qubits >= kPairTileBits && w->ppart && !(pr_env && pr_env[0] == '0');
     int i = num_gates - 1;
     while (i >= 0) {
       // A run of single-qubit gates on distinct qubits commutes gate by gate, so
@@ -1639,11 +1781,100 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
         used |= 1ull << gates[j].qubits[0];
         --j;
       }
+      const bool run1q = single_qubit(gates[i]);
       if (j == i) j = i - 1;  // a gate on two qubits: no rotation, un-applied below
       std::vector<rbk::overlap_spec> specs;
       int first = slot;
       for (int k = i; k > j; --k)
         if (gates[k].param >= 0) --first;
+      if (run1q && fused_runs) {
+        // The run in as few reads of both states as possible: Z-type overlaps from
+        // one two-state Z sum (no flush needed while only diagonal gates are queued:
+        // those commute with Z), the run's diagonal gates queued on both states,
+        // and every other gate of the run applied by pair-rotate launches that also
+        // take the X / Y-type overlaps.
+        std::vector<hgate> recs;
+        for (int k = i; k > j; --k) {
+          hgate h{};
+          if (int rc = inverse_record(psi.s, gates[k], theta, &h)) return rc;
+          recs.push_back(h);
+        }
+        auto is_diag = [](const hgate& h) { return h.kind == rbk::OPK_DIAG || h.kind == rbk::OPK_NEG; };
+        std::vector<size_t> zidx;
+        specs.assign(static_cast<size_t>(slot - first), rbk::overlap_spec{0, 0, 1.0, 0.0});
+        std::vector<int> slot_of(static_cast<size_t>(i - j), -1);
+        {
+          int y = slot - first;
+          for (int k = i; k > j; --k) {
+            const auto& g = gates[k];
+            if (g.param < 0) continue;
+            --y;
+            slot_param[first + y] = g.param;
+            slot_scale[first + y] = g.scale;
+            slot_of[static_cast<size_t>(i - k)] = first + y;
+            if (g.kind == RBK_GATE_EZ) zidx.push_back(static_cast<size_t>(y));
+            else if (is_diag(recs[static_cast<size_t>(i - k)])) return fail(RBK_ERR_STATE, "adjoint sweep: diagonal rotation of X / Y type");
+          }
+        }
+        if (!zidx.empty()) {
+          if (!queue_is_diagonal(psi.s) || !queue_is_diagonal(lam.s)) {
+            if (int rc = flush(psi.s)) return rc;
+            if (int rc = flush(lam.s)) return rc;
+          }
+          if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
+          for (int k = i; k > j; --k) {
+            const int sl = slot_of[static_cast<size_t>(i - k)];
+            if (sl >= 0 && gates[k].kind == RBK_GATE_EZ) specs[static_cast<size_t>(sl - first)].sign = 1ull << psi.s->perm[gates[k].qubits[0]];
+          }
+          if (int rc = launch_z_overlaps(*w, lam.s, psi.s, specs, zidx, first, ov.p)) return rc;
+        }
+        bool any_rotation = false;
+        for (int k = i; k > j; --k) {
+          const hgate& h = recs[static_cast<size_t>(i - k)];
+          if (is_diag(h)) {
+            if (int rc = enqueue(psi.s, h)) return rc;
+            if (int rc = enqueue(lam.s, h)) return rc;
+          } else {
+            any_rotation = true;
+          }
+        }
+        if (any_rotation) {
+          if (int rc = flush(psi.s)) return rc;
+          if (int rc = flush(lam.s)) return rc;
+          if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
+          std::vector<rotate_item> items;
+          for (int k = i; k > j; --k) {
+            const hgate& h = recs[static_cast<size_t>(i - k)];
+            if (is_diag(h)) continue;
+            if (h.cmask != 0) return fail(RBK_ERR_STATE, "adjoint sweep: controlled gate in a one-qubit run");
+            rotate_item it{};
+            it.bit = psi.s->perm[gates[k].qubits[0]];
+            it.slot = slot_of[static_cast<size_t>(i - k)];
+            it.spec = rbk::overlap_spec{0, 0, 1.0, 0.0};
+            if (it.slot >= 0) {
+              const uint64_t t = 1ull << it.bit;
+              it.spec.flip = t;
+              if (gates[k].kind == RBK_GATE_EY) { it.spec.sign = t; it.spec.wr = 0.0; it.spec.wi = -1.0; }
+            }
+            if (h.kind == rbk::OPK_MAT) {
+              std::memcpy(it.m, h.m, sizeof(it.m));
+            } else if (h.kind == rbk::OPK_X) {
+              const double m[8] = {0, 0, 1, 0, 1, 0, 0, 0};
+              std::memcpy(it.m, m, sizeof(it.m));
+            } else if (h.kind == rbk::OPK_Y) {  // (a0, a1) -> (-i a1, i a0)
+              const double m[8] = {0, 0, 0, -1, 0, 1, 0, 0};
+              std::memcpy(it.m, m, sizeof(it.m));
+            } else {
+              return fail(RBK_ERR_STATE, "adjoint sweep: unexpected gate record");
+            }
+            items.push_back(it);
+          }
+          if (int rc = launch_rotations(*w, lam.s, psi.s, items, ov.p)) return rc;
+        }
+        slot = first;
+        i = j;
+        continue;
+      }
       if (first < slot) {
         if (int rc = flush(psi.s)) return rc;
         if (int rc = flush(lam.s)) return rc;

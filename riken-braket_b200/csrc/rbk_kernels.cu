@@ -976,6 +976,232 @@ cudaError_t launch_pair_overlaps(const void* lam, const void* psi, int n, const 
   finish_pair_overlaps_kernel<<<g.nflips, 32, 0, stream>>>(partials, blocks, g.nflips, set, out);
   return cudaGetLastError();
 }
+// pair_rotate_set (rbk_kernels.h): the tile traffic of pair_overlaps_kernel
+// plus a write-back.  Per tile: both states' tiles into shared memory; in each
+// register phase the overlaps of the phase's flips, then their gates on both
+// states in registers, written back to the same slots; after the last phase
+// the tiles go back to HBM where they came from.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads, kPairBlocksPerSm)
+pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Real>::c* __restrict__ psi,
+                   const __grid_constant__ pair_rotate_set PS, uint64_t num_tiles, double* partials)
+{
+  const spin_group& S = PS.g;
+  using C = typename ctype<Real>::c;
+  constexpr int VB = precision_traits<Real>::VB;
+  constexpr int RB = kPairRegBits, NE = 1 << RB, KT = 8 + RB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tl = reinterpret_cast<C*>(smem_raw);
+  C* tp = tl + (1u << KT);
+  // Im(w_f (A_f + s_f B_f)) per flip and thread, kept in shared memory between
+  // tiles to spare registers.
+  __shared__ double acc[kMaxRotFlips][kRedThreads];
+  const uint32_t tid = threadIdx.x;
+#pragma unroll
+  for (int f = 0; f < kMaxRotFlips; ++f) acc[f][tid] = 0.0;
+  uint64_t tphys = 0;
+  for (int b = 0; b < 8; ++b) tphys |= uint64_t((tid >> b) & 1u) << S.tile_phys[b];
+  const uint32_t st = smem_slot<VB>(tid);
+  for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+    uint64_t base = tphys;
+    for (int r = 0; r < S.num_runs; ++r) base |= ((t >> S.run_src[r]) & ((1ull << S.run_len[r]) - 1)) << S.run_dst[r];
+    {
+      C vl[NE], vp[NE];
+#pragma unroll
+      for (int it = 0; it < NE; ++it) {
+        uint64_t p = base;
+#pragma unroll
+        for (int b = 0; b < RB; ++b)
+          if ((it >> b) & 1) p |= 1ull << S.tile_phys[8 + b];
+        vl[it] = __ldcs(lam + p);
+        vp[it] = __ldcs(psi + p);
+      }
+      __syncthreads();  // the previous tile's last shared-memory reads are done
+#pragma unroll
+      for (int it = 0; it < NE; ++it) {
+        const uint32_t s = st ^ smem_slot<VB>(uint32_t(it) << 8);
+        tl[s] = vl[it];
+        tp[s] = vp[it];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kSpinPhases; ++p) {
+      if (p < S.nphases) {
+        uint32_t j = 0;
+        for (int b = 0; b < 8; ++b) j |= ((tid >> b) & 1u) << S.phase_thr[p][b];
+        const uint32_t sbase = smem_slot<VB>(j);
+        uint32_t rs[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) rs[k] = smem_slot<VB>(1u << S.phase_reg[p][k]);
+        C el[NE], ep[NE];
+#pragma unroll
+        for (int i = 0; i < NE; ++i) {
+          uint32_t sidx = sbase;
+#pragma unroll
+          for (int k = 0; k < RB; ++k)
+            if ((i >> k) & 1) sidx ^= rs[k];
+          el[i] = tl[sidx];
+          ep[i] = tp[sidx];
+        }
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+          const int f = p * RB + k;
+          if (f < kMaxRotFlips && f < S.nflips && PS.flip[f].out_slot >= 0) {
+            // Im(w (A + s B)) = wi Re(A + s B) + wr Im(A + s B)
+            const double s = PS.flip[f].minus ? -1.0 : 1.0, wr = PS.flip[f].wr, wi = PS.flip[f].wi;
+            const double swr = s * wr, swi = s * wi;
+            double x = 0.0;
+#pragma unroll
+            for (int i = 0; i < NE; ++i) {
+              if ((i >> k) & 1) continue;
+              const C l0 = el[i], l1 = el[i | (1 << k)], p0 = ep[i], p1 = ep[i | (1 << k)];
+              const double ar = double(l0.x) * double(p1.x) + double(l0.y) * double(p1.y);
+              const double ai = double(l0.x) * double(p1.y) - double(l0.y) * double(p1.x);
+              const double br = double(l1.x) * double(p0.x) + double(l1.y) * double(p0.y);
+              const double bi = double(l1.x) * double(p0.y) - double(l1.y) * double(p0.x);
+              x += wi * ar + swi * br + wr * ai + swr * bi;
+            }
+            acc[f][tid] += x;
+          }
+        }
+        // The gates, lambda's registers first and written back before psi's,
+        // so that fewer registers are live at once.
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+          const int f = p * RB + k;
+          if (f < kMaxRotFlips && f < S.nflips) {
+            const double* m = PS.flip[f].m;
+#pragma unroll
+            for (int i = 0; i < NE; ++i) {
+              if ((i >> k) & 1) continue;
+              const int i1 = i | (1 << k);
+              const C l0 = el[i], l1 = el[i1];
+              el[i] = cmac2(l0, l1, Real(m[0]), Real(m[1]), Real(m[2]), Real(m[3]));
+              el[i1] = cmac2(l0, l1, Real(m[4]), Real(m[5]), Real(m[6]), Real(m[7]));
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < NE; ++i) {
+          uint32_t sidx = sbase;
+#pragma unroll
+          for (int k = 0; k < RB; ++k)
+            if ((i >> k) & 1) sidx ^= rs[k];
+          tl[sidx] = el[i];
+        }
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+          const int f = p * RB + k;
+          if (f < kMaxRotFlips && f < S.nflips) {
+            const double* m = PS.flip[f].m;
+#pragma unroll
+            for (int i = 0; i < NE; ++i) {
+              if ((i >> k) & 1) continue;
+              const int i1 = i | (1 << k);
+              const C p0 = ep[i], p1 = ep[i1];
+              ep[i] = cmac2(p0, p1, Real(m[0]), Real(m[1]), Real(m[2]), Real(m[3]));
+              ep[i1] = cmac2(p0, p1, Real(m[4]), Real(m[5]), Real(m[6]), Real(m[7]));
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < NE; ++i) {
+          uint32_t sidx = sbase;
+#pragma unroll
+          for (int k = 0; k < RB; ++k)
+            if ((i >> k) & 1) sidx ^= rs[k];
+          tp[sidx] = ep[i];
+        }
+        __syncthreads();  // the next phase (or the store) reads other threads' slots
+      }
+    }
+    // The store addresses are recomputed from an opaque copy of the tile base:
+    // kept from the loads, the eight of them would hold 16 registers through the phases.
+    uint64_t sbase_hbm;
+    asm volatile("mov.b64 %0, %1;" : "=l"(sbase_hbm) : "l"(base));
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      const uint32_t s = st ^ smem_slot<VB>(uint32_t(it) << 8);
+      uint64_t p = sbase_hbm;
+#pragma unroll
+      for (int b = 0; b < RB; ++b)
+        if ((it >> b) & 1) p |= 1ull << S.tile_phys[8 + b];
+      __stcs(lam + p, tl[s]);
+      __stcs(psi + p, tp[s]);
+    }
+  }
+  // Block sums in a fixed order, one double per flip.
+  __shared__ double red[kRedThreads / 32][kMaxRotFlips];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int f = 0; f < kMaxRotFlips; ++f) {
+    if (f < S.nflips) {
+      const double a = warp_sum(acc[f][tid]);
+      if (lane == 0) red[warp][f] = a;
+    }
+  }
+  __syncthreads();
+  const int width = S.nflips;
+  for (int k = threadIdx.x; k < width; k += blockDim.x) {
+    double sum = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) sum += red[w][k];
+    partials[size_t(blockIdx.x) * width + k] = sum;
+  }
+}
+
+// One warp per flip that has an overlap: out[2 slot + 1] = Im(w (A + s B)) summed
+// over the blocks; out[2 slot] = 0 (the real part is not formed).
+__global__ void finish_pair_rotate_kernel(const double* __restrict__ partials, int blocks, int nflips,
+                                          const __grid_constant__ pair_rotate_set set, double* __restrict__ out)
+{
+  const int lane = threadIdx.x & 31, f = blockIdx.x;
+  const int slot = set.flip[f].out_slot;
+  if (slot < 0) return;
+  double x = 0;
+  for (int b = lane; b < blocks; b += 32) x += partials[size_t(b) * nflips + f];
+  x = warp_sum(x);
+  if (lane == 0) {
+    out[2 * slot] = 0.0;
+    out[2 * slot + 1] = x;
+  }
+}
+
+size_t pair_rotate_partials_doubles() { return size_t(148) * kPairBlocksPerSm * kMaxRotFlips; }
+
+template <typename Real>
+cudaError_t launch_pair_rotate(void* lam, void* psi, int n, const pair_rotate_set& set, double* partials, double* out,
+                               cudaStream_t stream)
+{
+  const spin_group& g = set.g;
+  if (g.K != 8 + kPairRegBits || g.K > n || g.nflips < 1 || g.nflips > kMaxRotFlips || g.nphases < 1 ||
+      g.nphases > kSpinPhases || g.nphases * kPairRegBits < g.nflips)
+    return cudaErrorInvalidValue;
+  const size_t smem = 2 * sizeof(typename ctype<Real>::c) << g.K;
+  static std::atomic<bool> configured[64] = {};
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!configured[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(pair_rotate_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured[dev].store(true, std::memory_order_release);
+  }
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t tiles = 1ull << (n - g.K);
+  // Capped at 148 SMs' worth: the partials buffer is sized for that.
+  const int blocks = static_cast<int>(std::min<uint64_t>(tiles, uint64_t(std::min(sms, 148)) * kPairBlocksPerSm));
+  pair_rotate_kernel<Real><<<blocks, kRedThreads, smem, stream>>>(static_cast<typename ctype<Real>::c*>(lam),
+                                                                 static_cast<typename ctype<Real>::c*>(psi), set, tiles,
+                                                                 partials);
+  finish_pair_rotate_kernel<<<g.nflips, 32, 0, stream>>>(partials, blocks, g.nflips, set, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_pair_rotate<double>(void*, void*, int, const pair_rotate_set&, double*, double*, cudaStream_t);
+template cudaError_t launch_pair_rotate<float>(void*, void*, int, const pair_rotate_set&, double*, double*, cudaStream_t);
+
 template cudaError_t launch_zsum2<double>(const void*, const void*, int, const zsum2_set&, double*, double*, cudaStream_t);
 template cudaError_t launch_zsum2<float>(const void*, const void*, int, const zsum2_set&, double*, double*, cudaStream_t);
 template cudaError_t launch_pair_overlaps<double>(const void*, const void*, int, const pair_overlap_set&, double*, double*, cudaStream_t);

@@ -130,6 +130,23 @@ struct pair_overlap_set {
   struct { int32_t out_slot, minus; double wr, wi; } flip[kMaxPairFlips];
 };
 size_t pair_overlaps_partials_doubles();
+// The one-qubit gates of an adjoint run applied to both states in the same
+// read and write, with the X / Y-type overlaps of the run's rotations taken
+// from that read.  Same tile layout as pair_overlap_set, up to kMaxRotFlips
+// register-phase bits (every tile bit).  Flip f: the overlap (as in
+// pair_overlap_set; out_slot < 0 for none) from the amplitudes before its
+// gate, then m (m00 m01 m10 m11 as (re, im)) on lam and psi.  The gates act on
+// distinct bits and commute, so an overlap is the same whichever of the other
+// gates are already applied.  Only the imaginary part of w (A + s B), which the
+// gradient takes, is summed: out[2 slot] = 0, out[2 slot + 1] = Im.
+constexpr int kMaxRotFlips = 11;
+struct pair_rotate_set {
+  spin_group g;
+  struct { int32_t out_slot, minus; double wr, wi; double m[8]; } flip[kMaxRotFlips];
+};
+size_t pair_rotate_partials_doubles();
+template <typename Real> cudaError_t launch_pair_rotate(void* lam, void* psi, int n, const pair_rotate_set& set,
+                                                        double* partials, double* out, cudaStream_t stream);
 template <typename Real> cudaError_t launch_zsum2(const void* lam, const void* psi, int n, const zsum2_set& set,
                                                   double* partials, double* out, cudaStream_t stream);
 template <typename Real> cudaError_t launch_pair_overlaps(const void* lam, const void* psi, int n, const pair_overlap_set& set,

@@ -136,3 +136,50 @@ def test_adjoint_context_reuse_matches_one_shot(pkg):
             assert e1 == e2 and np.array_equal(g1, g2)
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["C128", "C64"])
+def test_adjoint_pair_rotate_matches_overlap_path(pkg, monkeypatch, precision):
+    """Runs of one-qubit gates in the reverse sweep: the pair-rotate launches
+    (overlaps and un-apply in one read and write of both states) against the
+    path that reads the overlaps first and queues the inverses on the engine,
+    on the ansatz and on a circuit with fixed gates of every one-qubit kind
+    inside the runs (rotations on the low three bits and on high bits, more than
+    eleven gates in a run)."""
+    A, C = pkg.adjoint, pkg.circuits
+    prec = getattr(pkg, precision)
+    tol = 1e-12 if precision == "C128" else 2e-5
+    rng = np.random.default_rng(11)
+    cases = []
+    n = 16
+    spec, k = A.ansatz_spec(n, 3)
+    cases.append((n, spec, rng.uniform(-np.pi, np.pi, k), C.ansatz_hamiltonian(n)))
+    n = 14
+    spec, k = [], 0
+    kinds = ["EX", "EY", "EZ", "H", "U3", "X", "Y", "Z", "U1", "U2"]
+    for layer in range(3):
+        for q in range(n):
+            mnem = kinds[(q + layer) % len(kinds)]
+            if mnem in ("EX", "EY", "EZ"):
+                spec.append((mnem, (q,), k, 0.5 + 0.1 * layer, (0.2,)))
+                k += 1
+            elif mnem == "U3":
+                spec.append((mnem, (q,), None, 0.0, tuple(rng.uniform(0, 6.28, 3))))
+            elif mnem == "U1":
+                spec.append((mnem, (q,), None, 0.0, (0.7,)))
+            elif mnem == "U2":
+                spec.append((mnem, (q,), None, 0.0, (0.3, 1.9)))
+            else:
+                spec.append((mnem, (q,), None, 0.0, ()))
+        spec += [("CNOT", (q, (q + 5) % n), None, 0.0, ()) for q in range(0, n, 3)]
+        spec += [("CZ", (q, (q + 1) % n), None, 0.0, ()) for q in range(n)]
+    terms = C.ansatz_hamiltonian(n) + [("XYZ" + "I" * (n - 4) + "X", 0.3)]
+    cases.append((n, spec, rng.uniform(-np.pi, np.pi, k), terms))
+    for n, spec, theta, terms in cases:
+        monkeypatch.setenv("RBK_ADJOINT_PAIR_ROTATE", "1")
+        e1, g1 = A.adjoint_gradient(n, spec, theta, terms, precision=prec)
+        monkeypatch.setenv("RBK_ADJOINT_PAIR_ROTATE", "0")
+        e0, g0 = A.adjoint_gradient(n, spec, theta, terms, precision=prec)
+        monkeypatch.delenv("RBK_ADJOINT_PAIR_ROTATE")
+        assert abs(e1 - e0) <= tol
+        assert np.abs(g1 - g0).max() <= tol, (n, np.abs(g1 - g0).max())
