@@ -1498,7 +1498,10 @@ int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state*
       fl.minus = it.spec.sign != 0 ? 1 : 0;
       fl.wr = it.spec.wr;
       fl.wi = it.spec.wi;
+      fl.okind = it.slot < 0 ? 0 : (it.spec.wr == 0.0 ? 1 : 0) | (it.spec.wi == 0.0 ? 2 : 0);
+      if (it.slot >= 0 && fl.okind == 0) fl.okind = 3;
       std::memcpy(fl.m, it.m, sizeof(fl.m));
+      fl.mkind = (it.m[1] == 0.0 && it.m[3] == 0.0 && it.m[5] == 0.0 && it.m[7] == 0.0) ? 1 : 0;
     }
     const cudaError_t e = c128 ? rbk::launch_pair_rotate<double>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream)
                                : rbk::launch_pair_rotate<float>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream);

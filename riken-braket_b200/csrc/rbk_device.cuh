@@ -23,6 +23,16 @@ __device__ __forceinline__ C cmac2(C a0, C a1, Real m0r, Real m0i, Real m1r, Rea
   return r;
 }
 
+// m0 * a0 + m1 * a1 with real m0, m1
+template <typename C, typename Real>
+__device__ __forceinline__ C rmac2(C a0, C a1, Real m0, Real m1)
+{
+  C r;
+  r.x = m0 * a0.x + m1 * a1.x;
+  r.y = m0 * a0.y + m1 * a1.y;
+  return r;
+}
+
 // Inserts a zero bit at position q of v (the index arithmetic of ket's pair
 // loops, e.g. ket/include/ket/gate/hadamard.hpp:57-59).
 __device__ __forceinline__ uint64_t insert_zero(uint64_t v, int q)

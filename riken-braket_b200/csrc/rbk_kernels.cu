@@ -1047,22 +1047,28 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
 #pragma unroll
         for (int k = 0; k < RB; ++k) {
           const int f = p * RB + k;
-          if (f < kMaxRotFlips && f < S.nflips && PS.flip[f].out_slot >= 0) {
-            // Im(w (A + s B)) = wi Re(A + s B) + wr Im(A + s B)
-            const double s = PS.flip[f].minus ? -1.0 : 1.0, wr = PS.flip[f].wr, wi = PS.flip[f].wi;
-            const double swr = s * wr, swi = s * wi;
-            double x = 0.0;
+          const int okind = (f < kMaxRotFlips && f < S.nflips) ? PS.flip[f].okind : 0;
+          if (okind != 0) {
+            // Im(w (A + s B)) = wi Re(A + s B) + wr Im(A + s B); the sums of
+            // A + s B are formed first and weighted once per tile.
+            const double s = PS.flip[f].minus ? -1.0 : 1.0;
+            double xr = 0.0, xi = 0.0;
 #pragma unroll
             for (int i = 0; i < NE; ++i) {
               if ((i >> k) & 1) continue;
               const C l0 = el[i], l1 = el[i | (1 << k)], p0 = ep[i], p1 = ep[i | (1 << k)];
-              const double ar = double(l0.x) * double(p1.x) + double(l0.y) * double(p1.y);
-              const double ai = double(l0.x) * double(p1.y) - double(l0.y) * double(p1.x);
-              const double br = double(l1.x) * double(p0.x) + double(l1.y) * double(p0.y);
-              const double bi = double(l1.x) * double(p0.y) - double(l1.y) * double(p0.x);
-              x += wi * ar + swi * br + wr * ai + swr * bi;
+              if (okind & 1) {
+                const double ar = double(l0.x) * double(p1.x) + double(l0.y) * double(p1.y);
+                const double br = double(l1.x) * double(p0.x) + double(l1.y) * double(p0.y);
+                xr += __fma_rn(s, br, ar);
+              }
+              if (okind & 2) {
+                const double ai = double(l0.x) * double(p1.y) - double(l0.y) * double(p1.x);
+                const double bi = double(l1.x) * double(p0.y) - double(l1.y) * double(p0.x);
+                xi += __fma_rn(s, bi, ai);
+              }
             }
-            acc[f][tid] += x;
+            acc[f][tid] += PS.flip[f].wi * xr + PS.flip[f].wr * xi;
           }
         }
         // The gates, lambda's registers first and written back before psi's,
@@ -1072,13 +1078,24 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
           const int f = p * RB + k;
           if (f < kMaxRotFlips && f < S.nflips) {
             const double* m = PS.flip[f].m;
+            if (PS.flip[f].mkind == 1) {
 #pragma unroll
-            for (int i = 0; i < NE; ++i) {
-              if ((i >> k) & 1) continue;
-              const int i1 = i | (1 << k);
-              const C l0 = el[i], l1 = el[i1];
-              el[i] = cmac2(l0, l1, Real(m[0]), Real(m[1]), Real(m[2]), Real(m[3]));
-              el[i1] = cmac2(l0, l1, Real(m[4]), Real(m[5]), Real(m[6]), Real(m[7]));
+              for (int i = 0; i < NE; ++i) {
+                if ((i >> k) & 1) continue;
+                const int i1 = i | (1 << k);
+                const C l0 = el[i], l1 = el[i1];
+                el[i] = rmac2(l0, l1, Real(m[0]), Real(m[2]));
+                el[i1] = rmac2(l0, l1, Real(m[4]), Real(m[6]));
+              }
+            } else {
+#pragma unroll
+              for (int i = 0; i < NE; ++i) {
+                if ((i >> k) & 1) continue;
+                const int i1 = i | (1 << k);
+                const C l0 = el[i], l1 = el[i1];
+                el[i] = cmac2(l0, l1, Real(m[0]), Real(m[1]), Real(m[2]), Real(m[3]));
+                el[i1] = cmac2(l0, l1, Real(m[4]), Real(m[5]), Real(m[6]), Real(m[7]));
+              }
             }
           }
         }
@@ -1095,13 +1112,24 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
           const int f = p * RB + k;
           if (f < kMaxRotFlips && f < S.nflips) {
             const double* m = PS.flip[f].m;
+            if (PS.flip[f].mkind == 1) {
 #pragma unroll
-            for (int i = 0; i < NE; ++i) {
-              if ((i >> k) & 1) continue;
-              const int i1 = i | (1 << k);
-              const C p0 = ep[i], p1 = ep[i1];
-              ep[i] = cmac2(p0, p1, Real(m[0]), Real(m[1]), Real(m[2]), Real(m[3]));
-              ep[i1] = cmac2(p0, p1, Real(m[4]), Real(m[5]), Real(m[6]), Real(m[7]));
+              for (int i = 0; i < NE; ++i) {
+                if ((i >> k) & 1) continue;
+                const int i1 = i | (1 << k);
+                const C p0 = ep[i], p1 = ep[i1];
+                ep[i] = rmac2(p0, p1, Real(m[0]), Real(m[2]));
+                ep[i1] = rmac2(p0, p1, Real(m[4]), Real(m[6]));
+              }
+            } else {
+#pragma unroll
+              for (int i = 0; i < NE; ++i) {
+                if ((i >> k) & 1) continue;
+                const int i1 = i | (1 << k);
+                const C p0 = ep[i], p1 = ep[i1];
+                ep[i] = cmac2(p0, p1, Real(m[0]), Real(m[1]), Real(m[2]), Real(m[3]));
+                ep[i1] = cmac2(p0, p1, Real(m[4]), Real(m[5]), Real(m[6]), Real(m[7]));
+              }
             }
           }
         }

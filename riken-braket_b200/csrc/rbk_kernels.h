@@ -139,10 +139,13 @@ size_t pair_overlaps_partials_doubles();
 // distinct bits and commute, so an overlap is the same whichever of the other
 // gates are already applied.  Only the imaginary part of w (A + s B), which the
 // gradient takes, is summed: out[2 slot] = 0, out[2 slot + 1] = Im.
+// okind picks the arithmetic of the overlap: 1 when wr = 0 (only the real parts
+// of A and B enter, as for Y types), 2 when wi = 0 (only the imaginary parts, X
+// types), 3 otherwise (0: no overlap); mkind 1 marks a real matrix (EY, H).
 constexpr int kMaxRotFlips = 11;
 struct pair_rotate_set {
   spin_group g;
-  struct { int32_t out_slot, minus; double wr, wi; double m[8]; } flip[kMaxRotFlips];
+  struct { int32_t out_slot, minus, okind, mkind; double wr, wi; double m[8]; } flip[kMaxRotFlips];
 };
 size_t pair_rotate_partials_doubles();
 template <typename Real> cudaError_t launch_pair_rotate(void* lam, void* psi, int n, const pair_rotate_set& set,
