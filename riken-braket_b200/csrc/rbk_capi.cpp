@@ -1399,29 +1399,6 @@ int launch_paired_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_
   return RBK_OK;
 }
 
-// Z-type overlaps (flip 0, one sign bit) of specs[idx...] in two-state Z-sum launches.
-int launch_z_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
-                      const std::vector<rbk::overlap_spec>& specs, const std::vector<size_t>& idx, int first_slot,
-                      double* ov)
-{
-  const bool c128 = w.precision == RBK_C128;
-  for (size_t c0 = 0; c0 < idx.size(); c0 += rbk::kMaxOverlaps) {
-    rbk::zsum2_set set{};
-    set.count = static_cast<int>(std::min<size_t>(rbk::kMaxOverlaps, idx.size() - c0));
-    for (int k = 0; k < set.count; ++k) {
-      const auto& sp = specs[idx[c0 + k]];
-      set.spec[k].bit = __builtin_ctzll(sp.sign);
-      set.spec[k].out_slot = first_slot + static_cast<int>(idx[c0 + k]);
-      set.spec[k].wr = sp.wr;
-      set.spec[k].wi = sp.wi;
-    }
-    const cudaError_t e = c128 ? rbk::launch_zsum2<double>(lam->amps, psi->amps, w.n, set, w.ppart, ov, psi->stream)
-                               : rbk::launch_zsum2<float>(lam->amps, psi->amps, w.n, set, w.ppart, ov, psi->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "Z-sum overlaps");
-  }
-  return RBK_OK;
-}
-
 // One gate of a fused reverse run on its physical bit: the 2x2 matrix of U^dagger
 // and, for a rotation, its X / Y-type overlap (slot < 0: none).
 struct rotate_item {
@@ -1434,9 +1411,59 @@ struct rotate_item {
 // Pair-rotate launches over `items`: tiles of the low kPairLowBits bits plus up
 // to 8 others, up to kMaxRotFlips gates per launch, in register phases of
 // kPairRegBits gates (the layout of launch_paired_overlaps).
-int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi, const std::vector<rotate_item>& items,
-                     double* ov)
+// A diagonal both states owe (the queued records, in physical bits) and the
+// Z-type overlaps to take with it, for the first pair-rotate launch of a run.
+struct owed_diagonal {
+  rbk::pre_diag d{};
+  uint64_t full[rbk::kMaxQubits] = {};  // controlled-Z partners of each bit, both directions
+};
+
+// The queued records of s as an owed_diagonal (false when one of them is not a
+// one-bit diagonal or a controlled Z: a multi-controlled phase, for instance).
+bool owed_from_queue(const rbk_state* s, owed_diagonal& o)
 {
+  using cplx_t = std::complex<double>;
+  cplx_t g{1.0, 0.0};
+  std::vector<cplx_t> u(rbk::kMaxQubits, cplx_t{1.0, 0.0});
+  for (const hgate& h : s->queue) {
+    if (h.kind == rbk::OPK_NEG) {
+      const int c = __builtin_popcountll(h.cmask);
+      if (c == 1) {
+        u[static_cast<size_t>(s->perm[__builtin_ctzll(h.cmask)])] *= -1.0;
+      } else if (c == 2) {
+        const int a = s->perm[__builtin_ctzll(h.cmask)], b = s->perm[63 - __builtin_clzll(h.cmask)];
+        o.d.adj[std::min(a, b)] ^= 1ull << std::max(a, b);
+        o.full[a] ^= 1ull << b;
+        o.full[b] ^= 1ull << a;
+      } else {
+        return false;
+      }
+    } else if (h.kind == rbk::OPK_DIAG && h.cmask == 0) {
+      const size_t t = static_cast<size_t>(s->perm[h.target]);
+      const cplx_t d0{h.m[0], h.m[1]}, d1{h.m[2], h.m[3]};
+      if (h.diag_one) {
+        u[t] *= d1;
+      } else {
+        g *= d0;
+        u[t] *= d1 / d0;
+      }
+    } else {
+      return false;
+    }
+  }
+  o.d.g[0] = g.real();
+  o.d.g[1] = g.imag();
+  for (int b = 0; b < rbk::kMaxQubits; ++b) {
+    o.d.u[b][0] = u[static_cast<size_t>(b)].real();
+    o.d.u[b][1] = u[static_cast<size_t>(b)].imag();
+  }
+  return true;
+}
+
+int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi, const std::vector<rotate_item>& items,
+                     double* ov, const owed_diagonal* owed)
+{
+  bool first_launch = true;
   const bool c128 = w.precision == RBK_C128;
   const int n = w.n;
   constexpr int RB = rbk::kPairRegBits, KT = kPairTileBits;
@@ -1503,6 +1530,26 @@ int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state*
       std::memcpy(fl.m, it.m, sizeof(fl.m));
       fl.mkind = (it.m[1] == 0.0 && it.m[3] == 0.0 && it.m[5] == 0.0 && it.m[7] == 0.0) ? 1 : 0;
     }
+    if (owed && first_launch) {
+      set.pre = owed->d;
+      set.pre.active = 1;
+      // The register slots' partner rows and their pairs among themselves.
+      set.pre.qr = 0;
+      for (int it = 0; it < (1 << RB); ++it) {
+        uint64_t mr = 0;
+        uint32_t par = 0;
+        for (int k = 0; k < RB; ++k) {
+          if (!((it >> k) & 1)) continue;
+          const int a = g.tile_phys[8 + k];
+          mr ^= owed->full[a];
+          for (int k2 = k + 1; k2 < RB; ++k2)
+            if ((it >> k2) & 1) par ^= static_cast<uint32_t>((owed->full[a] >> g.tile_phys[8 + k2]) & 1);
+        }
+        set.pre.mr[it] = mr;
+        set.pre.qr |= par << it;
+      }
+    }
+    first_launch = false;
     const cudaError_t e = c128 ? rbk::launch_pair_rotate<double>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream)
                                : rbk::launch_pair_rotate<float>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pair rotations");
@@ -1769,8 +1816,33 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
     };
     // Runs of one-qubit gates take the pair-rotate path where its tile fits
     // (RBK_ADJOINT_PAIR_ROTATE=0 selects the overlap-then-queue path instead).
+    // RBK_ADJOINT_PAIR_ROTATE=1 keeps the pair-rotate launches but flushes the
+    // owed diagonals and reads the Z-type overlaps separately.
     const char* pr_env = std::getenv("RBK_ADJOINT_PAIR_ROTATE");
     const bool fused_runs = num_qubits >= kPairTileBits && w->ppart && !(pr_env && pr_env[0] == '0');
+    const bool fused_pre = fused_runs && !(pr_env && pr_env[0] == '1');
+    // Z-type overlaps not taken yet: (physical bit, slot).  Valid while both
+    // states owe only diagonal records, which leave conj(lam_j) psi_j unchanged;
+    // settled (one Z-sum read) before any flush.
+    std::vector<std::pair<int, int>> zpend;
+    auto settle_z = [&]() -> int {
+      for (size_t c0 = 0; c0 < zpend.size(); c0 += rbk::kMaxOverlaps) {
+        rbk::zsum2_set set{};
+        set.count = static_cast<int>(std::min<size_t>(rbk::kMaxOverlaps, zpend.size() - c0));
+        for (int k = 0; k < set.count; ++k) {
+          set.spec[k].bit = zpend[c0 + k].first;
+          set.spec[k].out_slot = zpend[c0 + k].second;
+          set.spec[k].wr = 1.0;
+          set.spec[k].wi = 0.0;
+        }
+        const cudaError_t e = precision == RBK_C128
+          ? rbk::launch_zsum2<double>(lam.s->amps, psi.s->amps, num_qubits, set, w->ppart, ov.p, psi.s->stream)
+          : rbk::launch_zsum2<float>(lam.s->amps, psi.s->amps, num_qubits, set, w->ppart, ov.p, psi.s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "Z-sum overlaps");
+      }
+      zpend.clear();
+      return RBK_OK;
+    };
     int i = num_gates - 1;
     while (i >= 0) {
       // A run of single-qubit gates on distinct qubits commutes gate by gate, so
@@ -1821,15 +1893,19 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
         }
         if (!zidx.empty()) {
           if (!queue_is_diagonal(psi.s) || !queue_is_diagonal(lam.s)) {
+            if (int rc = settle_z()) return rc;
             if (int rc = flush(psi.s)) return rc;
             if (int rc = flush(lam.s)) return rc;
           }
           if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
+          if (zpend.size() + zidx.size() > static_cast<size_t>(rbk::kMaxQubits))
+            if (int rc = settle_z()) return rc;
           for (int k = i; k > j; --k) {
             const int sl = slot_of[static_cast<size_t>(i - k)];
-            if (sl >= 0 && gates[k].kind == RBK_GATE_EZ) specs[static_cast<size_t>(sl - first)].sign = 1ull << psi.s->perm[gates[k].qubits[0]];
+            if (sl >= 0 && gates[k].kind == RBK_GATE_EZ) zpend.emplace_back(psi.s->perm[gates[k].qubits[0]], sl);
           }
-          if (int rc = launch_z_overlaps(*w, lam.s, psi.s, specs, zidx, first, ov.p)) return rc;
+          if (!fused_pre)
+            if (int rc = settle_z()) return rc;
         }
         bool any_rotation = false;
         for (int k = i; k > j; --k) {
@@ -1842,8 +1918,26 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
           }
         }
         if (any_rotation) {
-          if (int rc = flush(psi.s)) return rc;
-          if (int rc = flush(lam.s)) return rc;
+          // What both states owe, applied and summed in the first launch when it
+          // is a product of one-bit diagonals and controlled Zs; else flushed.
+          owed_diagonal owed;
+          bool use_owed = fused_pre && (!zpend.empty() || !psi.s->queue.empty()) &&
+                          psi.s->queue.size() == lam.s->queue.size() && owed_from_queue(psi.s, owed);
+          if (use_owed) {
+            owed.d.nz = static_cast<int>(zpend.size());
+            for (size_t k = 0; k < zpend.size(); ++k) {
+              owed.d.z[k].bit = zpend[k].first;
+              owed.d.z[k].out_slot = zpend[k].second;
+              owed.d.z[k].wr = 1.0;
+            }
+            zpend.clear();
+            psi.s->queue.clear();
+            lam.s->queue.clear();
+          } else {
+            if (int rc = settle_z()) return rc;
+            if (int rc = flush(psi.s)) return rc;
+            if (int rc = flush(lam.s)) return rc;
+          }
           if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
           std::vector<rotate_item> items;
           for (int k = i; k > j; --k) {
@@ -1872,13 +1966,14 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
             }
             items.push_back(it);
           }
-          if (int rc = launch_rotations(*w, lam.s, psi.s, items, ov.p)) return rc;
+          if (int rc = launch_rotations(*w, lam.s, psi.s, items, ov.p, use_owed ? &owed : nullptr)) return rc;
         }
         slot = first;
         i = j;
         continue;
       }
       if (first < slot) {
+        if (int rc = settle_z()) return rc;
         if (int rc = flush(psi.s)) return rc;
         if (int rc = flush(lam.s)) return rc;
         if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
@@ -1906,6 +2001,7 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
       }
       i = j;
     }
+    if (int rc = settle_z()) return rc;
     std::vector<double> host(2 * (num_pg + 1));
     RBK_CUDA(cudaMemcpyAsync(host.data(), ov.p, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, psi.s->stream));
     if (int rc = bounded_sync(psi.s)) return rc;

@@ -997,11 +997,34 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
   // tiles to spare registers.
   __shared__ double acc[kMaxRotFlips][kRedThreads];
   const uint32_t tid = threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int f = 0; f < kMaxRotFlips; ++f) acc[f][tid] = 0.0;
   uint64_t tphys = 0;
   for (int b = 0; b < 8; ++b) tphys |= uint64_t((tid >> b) & 1u) << S.tile_phys[b];
   const uint32_t st = smem_slot<VB>(tid);
+  // Pre-step state (PS.pre): the diagonal's factor over this thread's tile bits
+  // and over each register slot's bits; Z sums per thread (total and register
+  // bits) and per warp (bits outside the tile).
+  const pre_diag& D = PS.pre;
+  __shared__ double2 fthr[kRedThreads], freg[1 << kPairRegBits];
+  __shared__ double zt[4][kRedThreads];
+  __shared__ double zh[kMaxQubits][kRedThreads / 32];
+  if (D.active) {
+    double2 f{1.0, 0.0};
+    for (int b = 0; b < 8; ++b)
+      if ((tid >> b) & 1) f = cmul(f, double2{D.u[S.tile_phys[b]][0], D.u[S.tile_phys[b]][1]});
+    fthr[tid] = f;
+    if (tid < (1u << kPairRegBits)) {
+      double2 r{1.0, 0.0};
+      for (int b = 0; b < kPairRegBits; ++b)
+        if ((tid >> b) & 1) r = cmul(r, double2{D.u[S.tile_phys[8 + b]][0], D.u[S.tile_phys[8 + b]][1]});
+      freg[tid] = r;
+    }
+    for (int k = 0; k < 4; ++k) zt[k][tid] = 0.0;
+    for (int q = tid; q < kMaxQubits * (kRedThreads / 32); q += kRedThreads) zh[q / (kRedThreads / 32)][q % (kRedThreads / 32)] = 0.0;
+    __syncthreads();
+  }
   for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
     uint64_t base = tphys;
     for (int r = 0; r < S.num_runs; ++r) base |= ((t >> S.run_src[r]) & ((1ull << S.run_len[r]) - 1)) << S.run_dst[r];
@@ -1015,6 +1038,45 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
           if ((it >> b) & 1) p |= 1ull << S.tile_phys[8 + b];
         vl[it] = __ldcs(lam + p);
         vp[it] = __ldcs(psi + p);
+      }
+      if (D.active) {
+        if (D.nz > 0) {
+          // Im conj(lam_j) psi_j: thread total, register-bit sums, and the warp's
+          // total for the bits outside the tile that are set in this tile.
+          double tot = 0.0, r0 = 0.0, r1 = 0.0, r2 = 0.0;
+#pragma unroll
+          for (int it = 0; it < NE; ++it) {
+            const double c = double(vl[it].x) * double(vp[it].y) - double(vl[it].y) * double(vp[it].x);
+            tot += c;
+            if (it & 1) r0 += c;
+            if (it & 2) r1 += c;
+            if (it & 4) r2 += c;
+          }
+          zt[0][tid] += tot;
+          zt[1][tid] += r0;
+          zt[2][tid] += r1;
+          zt[3][tid] += r2;
+          const double wtot = warp_sum(tot);
+          if (lane == 0)
+            for (uint64_t hb = base ^ tphys; hb; hb &= hb - 1) zh[__ffsll(static_cast<long long>(hb)) - 1][warp] += wtot;
+        }
+        // The diagonal: g times u over the set bits, times (-1)^Q.
+        double2 f{D.g[0], D.g[1]};
+        for (uint64_t hb = base ^ tphys; hb; hb &= hb - 1) {
+          const int q = __ffsll(static_cast<long long>(hb)) - 1;
+          f = cmul(f, double2{D.u[q][0], D.u[q][1]});
+        }
+        f = cmul(f, fthr[tid]);
+        uint32_t qb = 0;
+        for (uint64_t hb = base; hb; hb &= hb - 1) qb ^= __popcll(base & D.adj[__ffsll(static_cast<long long>(hb)) - 1]);
+#pragma unroll
+        for (int it = 0; it < NE; ++it) {
+          double2 fi = cmul(f, freg[it]);
+          if ((qb ^ (D.qr >> it) ^ __popcll(base & D.mr[it])) & 1) fi = double2{-fi.x, -fi.y};
+          const C fc{Real(fi.x), Real(fi.y)};
+          vl[it] = cmul(vl[it], fc);
+          vp[it] = cmul(vp[it], fc);
+        }
       }
       __syncthreads();  // the previous tile's last shared-memory reads are done
 #pragma unroll
@@ -1159,9 +1221,11 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
       __stcs(psi + p, tp[s]);
     }
   }
-  // Block sums in a fixed order, one double per flip.
-  __shared__ double red[kRedThreads / 32][kMaxRotFlips];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // Block sums in a fixed order, one double per flip; then, with Z sums, the
+  // total and the sum over j with each physical bit set (tile bits from the
+  // per-thread sums, the others from the per-warp sums).
+  constexpr int NZ = 1 + 8 + kPairRegBits;
+  __shared__ double red[kRedThreads / 32][kMaxRotFlips + NZ];
 #pragma unroll
   for (int f = 0; f < kMaxRotFlips; ++f) {
     if (f < S.nflips) {
@@ -1169,42 +1233,90 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
       if (lane == 0) red[warp][f] = a;
     }
   }
+  const bool zs = D.active && D.nz > 0;
+  if (zs) {
+    double v[NZ];
+    v[0] = zt[0][tid];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) v[1 + b] = ((tid >> b) & 1) ? zt[0][tid] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kPairRegBits; ++k) v[9 + k] = zt[1 + k][tid];
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      const double a = warp_sum(v[k]);
+      if (lane == 0) red[warp][kMaxRotFlips + k] = a;
+    }
+  }
   __syncthreads();
-  const int width = S.nflips;
+  const int nzw = zs ? 1 + kMaxQubits : 0;
+  const int width = S.nflips + nzw;
   for (int k = threadIdx.x; k < width; k += blockDim.x) {
     double sum = 0.0;
-    for (int w = 0; w < kRedThreads / 32; ++w) sum += red[w][k];
+    if (k < S.nflips) {
+      for (int w = 0; w < kRedThreads / 32; ++w) sum += red[w][k];
+    } else {
+      const int q = k - S.nflips - 1;  // -1: the total
+      int col = -1;
+      if (q < 0) col = 0;
+      for (int b = 0; b < 8 + kPairRegBits; ++b)
+        if (q >= 0 && S.tile_phys[b] == q) col = 1 + b;
+      if (col >= 0) {
+        for (int w = 0; w < kRedThreads / 32; ++w) sum += red[w][kMaxRotFlips + col];
+      } else {
+        for (int w = 0; w < kRedThreads / 32; ++w) sum += zh[q][w];
+      }
+    }
     partials[size_t(blockIdx.x) * width + k] = sum;
   }
 }
 
 // One warp per flip that has an overlap: out[2 slot + 1] = Im(w (A + s B)) summed
 // over the blocks; out[2 slot] = 0 (the real part is not formed).
-__global__ void finish_pair_rotate_kernel(const double* __restrict__ partials, int blocks, int nflips,
+// Blocks past nflips: one per Z entry of the pre-step, out[2 slot + 1] = wr (total - 2 sum over bit q set).
+__global__ void finish_pair_rotate_kernel(const double* __restrict__ partials, int blocks, int nflips, int width,
                                           const __grid_constant__ pair_rotate_set set, double* __restrict__ out)
 {
   const int lane = threadIdx.x & 31, f = blockIdx.x;
-  const int slot = set.flip[f].out_slot;
-  if (slot < 0) return;
-  double x = 0;
-  for (int b = lane; b < blocks; b += 32) x += partials[size_t(b) * nflips + f];
-  x = warp_sum(x);
+  if (f < nflips) {
+    const int slot = set.flip[f].out_slot;
+    if (slot < 0) return;
+    double x = 0;
+    for (int b = lane; b < blocks; b += 32) x += partials[size_t(b) * width + f];
+    x = warp_sum(x);
+    if (lane == 0) {
+      out[2 * slot] = 0.0;
+      out[2 * slot + 1] = x;
+    }
+    return;
+  }
+  const auto& z = set.pre.z[f - nflips];
+  double t = 0, o = 0;
+  for (int b = lane; b < blocks; b += 32) {
+    t += partials[size_t(b) * width + nflips];
+    o += partials[size_t(b) * width + nflips + 1 + z.bit];
+  }
+  t = warp_sum(t);
+  o = warp_sum(o);
   if (lane == 0) {
-    out[2 * slot] = 0.0;
-    out[2 * slot + 1] = x;
+    out[2 * z.out_slot] = 0.0;
+    out[2 * z.out_slot + 1] = z.wr * (t - 2.0 * o);
   }
 }
 
-size_t pair_rotate_partials_doubles() { return size_t(148) * kPairBlocksPerSm * kMaxRotFlips; }
+size_t pair_rotate_partials_doubles() { return size_t(148) * kPairBlocksPerSm * (kMaxRotFlips + 1 + kMaxQubits); }
 
 template <typename Real>
 cudaError_t launch_pair_rotate(void* lam, void* psi, int n, const pair_rotate_set& set, double* partials, double* out,
                                cudaStream_t stream)
 {
   const spin_group& g = set.g;
-  if (g.K != 8 + kPairRegBits || g.K > n || g.nflips < 1 || g.nflips > kMaxRotFlips || g.nphases < 1 ||
+  if (g.K != 8 + kPairRegBits || g.K > n || n > kMaxQubits || g.nflips < 1 || g.nflips > kMaxRotFlips || g.nphases < 1 ||
       g.nphases > kSpinPhases || g.nphases * kPairRegBits < g.nflips)
     return cudaErrorInvalidValue;
+  const int nz = set.pre.active ? set.pre.nz : 0;
+  if (nz < 0 || nz > kMaxQubits) return cudaErrorInvalidValue;
+  for (int k = 0; k < nz; ++k)
+    if (set.pre.z[k].bit < 0 || set.pre.z[k].bit >= n) return cudaErrorInvalidValue;
   const size_t smem = 2 * sizeof(typename ctype<Real>::c) << g.K;
   static std::atomic<bool> configured[64] = {};
   int dev = 0, sms = 0;
@@ -1224,7 +1336,8 @@ cudaError_t launch_pair_rotate(void* lam, void* psi, int n, const pair_rotate_se
   pair_rotate_kernel<Real><<<blocks, kRedThreads, smem, stream>>>(static_cast<typename ctype<Real>::c*>(lam),
                                                                  static_cast<typename ctype<Real>::c*>(psi), set, tiles,
                                                                  partials);
-  finish_pair_rotate_kernel<<<g.nflips, 32, 0, stream>>>(partials, blocks, g.nflips, set, out);
+  const int width = g.nflips + (nz > 0 ? 1 + kMaxQubits : 0);
+  finish_pair_rotate_kernel<<<g.nflips + nz, 32, 0, stream>>>(partials, blocks, g.nflips, width, set, out);
   return cudaGetLastError();
 }
 template cudaError_t launch_pair_rotate<double>(void*, void*, int, const pair_rotate_set&, double*, double*, cudaStream_t);

@@ -141,8 +141,10 @@ def test_adjoint_context_reuse_matches_one_shot(pkg):
 @pytest.mark.parametrize("precision", ["C128", "C64"])
 def test_adjoint_pair_rotate_matches_overlap_path(pkg, monkeypatch, precision):
     """Runs of one-qubit gates in the reverse sweep: the pair-rotate launches
-    (overlaps and un-apply in one read and write of both states) against the
-    path that reads the overlaps first and queues the inverses on the engine,
+    (overlaps and un-apply in one read and write of both states), with and
+    without the owed diagonals and Z-type overlaps folded into their first
+    launch, against the path that reads the overlaps first and queues the
+    inverses on the engine,
     on the ansatz and on a circuit with fixed gates of every one-qubit kind
     inside the runs (rotations on the low three bits and on high bits, more than
     eleven gates in a run)."""
@@ -176,10 +178,13 @@ def test_adjoint_pair_rotate_matches_overlap_path(pkg, monkeypatch, precision):
     terms = C.ansatz_hamiltonian(n) + [("XYZ" + "I" * (n - 4) + "X", 0.3)]
     cases.append((n, spec, rng.uniform(-np.pi, np.pi, k), terms))
     for n, spec, theta, terms in cases:
+        monkeypatch.delenv("RBK_ADJOINT_PAIR_ROTATE", raising=False)
+        e2, g2 = A.adjoint_gradient(n, spec, theta, terms, precision=prec)
         monkeypatch.setenv("RBK_ADJOINT_PAIR_ROTATE", "1")
         e1, g1 = A.adjoint_gradient(n, spec, theta, terms, precision=prec)
         monkeypatch.setenv("RBK_ADJOINT_PAIR_ROTATE", "0")
         e0, g0 = A.adjoint_gradient(n, spec, theta, terms, precision=prec)
         monkeypatch.delenv("RBK_ADJOINT_PAIR_ROTATE")
-        assert abs(e1 - e0) <= tol
-        assert np.abs(g1 - g0).max() <= tol, (n, np.abs(g1 - g0).max())
+        for e, g in ((e1, g1), (e2, g2)):
+            assert abs(e - e0) <= tol
+            assert np.abs(g - g0).max() <= tol, (n, np.abs(g - g0).max())
