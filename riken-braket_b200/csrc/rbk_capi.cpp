@@ -1487,10 +1487,26 @@ int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state*
     g.K = KT;
     uint64_t mask = 0;
     for (int b = 0; b < KT; ++b) { g.tile_phys[b] = static_cast<uint8_t>(tile_bits[static_cast<size_t>(b)]); mask |= 1ull << tile_bits[static_cast<size_t>(b)]; }
-    std::vector<int> local;
-    for (size_t y : mine)
-      local.push_back(static_cast<int>(std::find(tile_bits.begin(), tile_bits.end(), items[y].bit) - tile_bits.begin()));
-    g.nflips = static_cast<int>(mine.size());
+    // Register positions: phase 0 is the load layout (tile bits 8..10, a filler
+    // where no gate acts), then the other gates three to a phase.
+    std::vector<int> local;            // tile bit of each position
+    std::vector<long> pos_item;        // index into items, -1 for a filler
+    {
+      std::vector<int> loc;
+      for (size_t y : mine)
+        loc.push_back(static_cast<int>(std::find(tile_bits.begin(), tile_bits.end(), items[y].bit) - tile_bits.begin()));
+      for (int k = 0; k < RB; ++k) {
+        const int want = KT - RB + k;
+        long found = -1;
+        for (size_t f = 0; f < mine.size(); ++f)
+          if (loc[f] == want) found = static_cast<long>(mine[f]);
+        local.push_back(want);
+        pos_item.push_back(found);
+      }
+      for (size_t f = 0; f < mine.size(); ++f)
+        if (loc[f] < KT - RB) { local.push_back(loc[f]); pos_item.push_back(static_cast<long>(mine[f])); }
+    }
+    g.nflips = static_cast<int>(local.size());
     g.nphases = (g.nflips + RB - 1) / RB;
     for (int p = 0; p < g.nphases; ++p) {
       std::vector<int> regs;
@@ -1518,9 +1534,15 @@ int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state*
       q += len;
     }
     g.num_runs = runs;
-    for (size_t f = 0; f < mine.size(); ++f) {
-      const rotate_item& it = items[mine[f]];
+    for (size_t f = 0; f < local.size(); ++f) {
       auto& fl = set.flip[f];
+      if (pos_item[f] < 0) {
+        fl.out_slot = -1;
+        fl.okind = 0;
+        fl.mkind = 2;
+        continue;
+      }
+      const rotate_item& it = items[static_cast<size_t>(pos_item[f])];
       fl.out_slot = it.slot;
       fl.minus = it.spec.sign != 0 ? 1 : 0;
       fl.wr = it.spec.wr;

@@ -1028,8 +1028,12 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
   for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
     uint64_t base = tphys;
     for (int r = 0; r < S.num_runs; ++r) base |= ((t >> S.run_src[r]) & ((1ull << S.run_len[r]) - 1)) << S.run_dst[r];
+    // Phase 0 is the load layout (register bits = tile bits 8..10, thread bits
+    // 0..7): the tile goes from HBM straight into its registers.
+    C el[NE], ep[NE];
     {
-      C vl[NE], vp[NE];
+      C* vl = el;
+      C* vp = ep;
 #pragma unroll
       for (int it = 0; it < NE; ++it) {
         uint64_t p = base;
@@ -1079,14 +1083,7 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
         }
       }
       __syncthreads();  // the previous tile's last shared-memory reads are done
-#pragma unroll
-      for (int it = 0; it < NE; ++it) {
-        const uint32_t s = st ^ smem_slot<VB>(uint32_t(it) << 8);
-        tl[s] = vl[it];
-        tp[s] = vp[it];
-      }
     }
-    __syncthreads();
 #pragma unroll
     for (int p = 0; p < kSpinPhases; ++p) {
       if (p < S.nphases) {
@@ -1096,15 +1093,16 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
         uint32_t rs[RB];
 #pragma unroll
         for (int k = 0; k < RB; ++k) rs[k] = smem_slot<VB>(1u << S.phase_reg[p][k]);
-        C el[NE], ep[NE];
+        if (p > 0) {
 #pragma unroll
-        for (int i = 0; i < NE; ++i) {
-          uint32_t sidx = sbase;
+          for (int i = 0; i < NE; ++i) {
+            uint32_t sidx = sbase;
 #pragma unroll
-          for (int k = 0; k < RB; ++k)
-            if ((i >> k) & 1) sidx ^= rs[k];
-          el[i] = tl[sidx];
-          ep[i] = tp[sidx];
+            for (int k = 0; k < RB; ++k)
+              if ((i >> k) & 1) sidx ^= rs[k];
+            el[i] = tl[sidx];
+            ep[i] = tp[sidx];
+          }
         }
 #pragma unroll
         for (int k = 0; k < RB; ++k) {
@@ -1138,7 +1136,7 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
 #pragma unroll
         for (int k = 0; k < RB; ++k) {
           const int f = p * RB + k;
-          if (f < kMaxRotFlips && f < S.nflips) {
+          if (f < kMaxRotFlips && f < S.nflips && PS.flip[f].mkind != 2) {
             const double* m = PS.flip[f].m;
             if (PS.flip[f].mkind == 1) {
 #pragma unroll
@@ -1172,7 +1170,7 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
 #pragma unroll
         for (int k = 0; k < RB; ++k) {
           const int f = p * RB + k;
-          if (f < kMaxRotFlips && f < S.nflips) {
+          if (f < kMaxRotFlips && f < S.nflips && PS.flip[f].mkind != 2) {
             const double* m = PS.flip[f].m;
             if (PS.flip[f].mkind == 1) {
 #pragma unroll

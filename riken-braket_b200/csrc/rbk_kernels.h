@@ -141,7 +141,9 @@ size_t pair_overlaps_partials_doubles();
 // gradient takes, is summed: out[2 slot] = 0, out[2 slot + 1] = Im.
 // okind picks the arithmetic of the overlap: 1 when wr = 0 (only the real parts
 // of A and B enter, as for Y types), 2 when wi = 0 (only the imaginary parts, X
-// types), 3 otherwise (0: no overlap); mkind 1 marks a real matrix (EY, H).
+// types), 3 otherwise (0: no overlap); mkind 1 marks a real matrix (EY, H),
+// 2 a filler position without a gate.  Phase 0 must be the load layout:
+// register bits 8, 9, 10 and thread bits 0..7 of the tile, in order.
 constexpr int kMaxRotFlips = 11;
 // Optional first step of a launch: a diagonal that both states still owe,
 // applied at load time, and Z-type overlaps taken there (a diagonal with
