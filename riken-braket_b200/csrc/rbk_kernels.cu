@@ -1008,6 +1008,7 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
   // bits) and per warp (bits outside the tile).
   const pre_diag& D = PS.pre;
   __shared__ double2 fthr[kRedThreads], freg[1 << kPairRegBits];
+  __shared__ uint64_t mthr[kRedThreads];  // partner row of this thread's tile bits, XORed; bit 63: their pair parity
   __shared__ double zt[4][kRedThreads];
   __shared__ double zh[kMaxQubits][kRedThreads / 32];
   if (D.active) {
@@ -1015,6 +1016,14 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
     for (int b = 0; b < 8; ++b)
       if ((tid >> b) & 1) f = cmul(f, double2{D.u[S.tile_phys[b]][0], D.u[S.tile_phys[b]][1]});
     fthr[tid] = f;
+    uint64_t m = 0;
+    uint32_t qt = 0;
+    for (int b = 0; b < 8; ++b)
+      if ((tid >> b) & 1) {
+        m ^= D.full[S.tile_phys[b]];
+        qt ^= __popcll(tphys & D.adj[S.tile_phys[b]]);
+      }
+    mthr[tid] = (m & ~(1ull << 63)) | (uint64_t(qt & 1u) << 63);
     if (tid < (1u << kPairRegBits)) {
       double2 r{1.0, 0.0};
       for (int b = 0; b < kPairRegBits; ++b)
@@ -1071,8 +1080,13 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
           f = cmul(f, double2{D.u[q][0], D.u[q][1]});
         }
         f = cmul(f, fthr[tid]);
+        // Q(base) = Q(bits outside the tile) ^ Q(thread bits) ^ their cross
+        // pairs; the first is the same for the whole CTA (uniform loop).
+        const uint64_t hbase = base ^ tphys;
         uint32_t qb = 0;
-        for (uint64_t hb = base; hb; hb &= hb - 1) qb ^= __popcll(base & D.adj[__ffsll(static_cast<long long>(hb)) - 1]);
+        for (uint64_t hb = hbase; hb; hb &= hb - 1) qb ^= __popcll(hbase & D.adj[__ffsll(static_cast<long long>(hb)) - 1]);
+        const uint64_t mt = mthr[tid];
+        qb ^= uint32_t(mt >> 63) ^ __popcll(hbase & mt & ~(1ull << 63));
 #pragma unroll
         for (int it = 0; it < NE; ++it) {
           double2 fi = cmul(f, freg[it]);

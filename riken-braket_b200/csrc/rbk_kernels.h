@@ -159,6 +159,7 @@ struct pre_diag {
   double g[2];
   double u[kMaxQubits][2];
   uint64_t adj[kMaxQubits];
+  uint64_t full[kMaxQubits];  // all partners of each bit (both directions)
   uint64_t mr[8];
   uint32_t qr, pad;
   struct { int32_t bit, out_slot; double wr; } z[kMaxQubits];
