@@ -1487,40 +1487,42 @@ int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state*
     g.K = KT;
     uint64_t mask = 0;
     for (int b = 0; b < KT; ++b) { g.tile_phys[b] = static_cast<uint8_t>(tile_bits[static_cast<size_t>(b)]); mask |= 1ull << tile_bits[static_cast<size_t>(b)]; }
-    // Register positions: phase 0 is the load layout (tile bits 8..10, a filler
-    // where no gate acts), then the other gates three to a phase.
-    std::vector<int> local;            // tile bit of each position
-    std::vector<long> pos_item;        // index into items, -1 for a filler
+    // Register phases, by groups of tile bits: A = 8..10 (the load layout),
+    // B = 0..2, C = 3, 4 and a spare, D = 5..7.  A, B and C keep tile bits 5..7
+    // on the warp index, so moving between them (and from C to the store) stays
+    // inside each warp; only entering and leaving D needs the whole CTA.
+    // Groups without a gate are left out, except A.
+    std::vector<int> local;      // tile bit of each register position
+    std::vector<long> pos_item;  // index into items, -1 for a filler
     {
-      std::vector<int> loc;
+      std::vector<long> gate_at(KT, -1);
       for (size_t y : mine)
-        loc.push_back(static_cast<int>(std::find(tile_bits.begin(), tile_bits.end(), items[y].bit) - tile_bits.begin()));
-      for (int k = 0; k < RB; ++k) {
-        const int want = KT - RB + k;
-        long found = -1;
-        for (size_t f = 0; f < mine.size(); ++f)
-          if (loc[f] == want) found = static_cast<long>(mine[f]);
-        local.push_back(want);
-        pos_item.push_back(found);
+        gate_at[static_cast<size_t>(std::find(tile_bits.begin(), tile_bits.end(), items[y].bit) - tile_bits.begin())] =
+          static_cast<long>(y);
+      static const int groups[4][3] = {{8, 9, 10}, {0, 1, 2}, {3, 4, 0}, {5, 6, 7}};
+      static const int thr_of[4][8] = {{0, 1, 2, 3, 4, 5, 6, 7}, {3, 4, 8, 9, 10, 5, 6, 7},
+                                       {1, 2, 8, 9, 10, 5, 6, 7}, {0, 1, 2, 3, 4, 8, 9, 10}};
+      int p = 0;
+      int warps_of[rbk::kSpinPhases + 1] = {};
+      for (int gi = 0; gi < 4; ++gi) {
+        const int nreal = gi == 2 ? 2 : 3;  // group C's third bit is a spare
+        bool any = gi == 0;
+        for (int k = 0; k < nreal; ++k) any = any || gate_at[static_cast<size_t>(groups[gi][k])] >= 0;
+        if (!any) continue;
+        for (int k = 0; k < RB; ++k) {
+          local.push_back(groups[gi][k]);
+          pos_item.push_back(k < nreal ? gate_at[static_cast<size_t>(groups[gi][k])] : -1);
+          g.phase_reg[p][k] = static_cast<uint8_t>(groups[gi][k]);
+        }
+        for (int b = 0; b < 8; ++b) g.phase_thr[p][b] = static_cast<uint8_t>(thr_of[gi][b]);
+        warps_of[p] = gi == 3 ? 1 : 0;
+        ++p;
       }
-      for (size_t f = 0; f < mine.size(); ++f)
-        if (loc[f] < KT - RB) { local.push_back(loc[f]); pos_item.push_back(static_cast<long>(mine[f])); }
+      g.nphases = p;
+      warps_of[p] = 0;  // the store reads in the load layout
+      for (int q = 0; q < p; ++q) set.block_sync[q] = warps_of[q] != warps_of[q + 1] ? 1 : 0;
     }
     g.nflips = static_cast<int>(local.size());
-    g.nphases = (g.nflips + RB - 1) / RB;
-    for (int p = 0; p < g.nphases; ++p) {
-      std::vector<int> regs;
-      for (int k = 0; k < RB; ++k) {
-        const int f = p * RB + k;
-        if (f < g.nflips) regs.push_back(local[static_cast<size_t>(f)]);
-      }
-      for (int b = 0; static_cast<int>(regs.size()) < RB; ++b)  // fillers: other tile bits, left alone
-        if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
-      int nt = 0;
-      for (int b = 0; b < KT; ++b)
-        if (std::find(regs.begin(), regs.end(), b) == regs.end()) g.phase_thr[p][nt++] = static_cast<uint8_t>(b);
-      for (int k = 0; k < RB; ++k) g.phase_reg[p][k] = static_cast<uint8_t>(regs[static_cast<size_t>(k)]);
-    }
     int runs = 0, src = 0;
     for (int q = 0; q < n;) {
       if ((mask >> q) & 1) { ++q; continue; }

@@ -1096,7 +1096,9 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
           vp[it] = cmul(vp[it], fc);
         }
       }
-      __syncthreads();  // the previous tile's last shared-memory reads are done
+      // The previous tile's last shared-memory reads (its store, in the load
+      // layout) were made by this warp on the slots phase 0 writes.
+      __syncwarp();
     }
 #pragma unroll
     for (int p = 0; p < kSpinPhases; ++p) {
@@ -1215,7 +1217,10 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
             if ((i >> k) & 1) sidx ^= rs[k];
           tp[sidx] = ep[i];
         }
-        __syncthreads();  // the next phase (or the store) reads other threads' slots
+        // The next phase (or the store) reads other threads' slots: those of
+        // other warps too where the warp index moves to other tile bits.
+        if (PS.block_sync[p]) __syncthreads();
+        else __syncwarp();
       }
     }
     // The store addresses are recomputed from an opaque copy of the tile base:

@@ -144,7 +144,11 @@ size_t pair_overlaps_partials_doubles();
 // types), 3 otherwise (0: no overlap); mkind 1 marks a real matrix (EY, H),
 // 2 a filler position without a gate.  Phase 0 must be the load layout:
 // register bits 8, 9, 10 and thread bits 0..7 of the tile, in order.
-constexpr int kMaxRotFlips = 11;
+// block_sync[p] = 1: the layout after phase p (the next phase's, or the load
+// layout for the store) puts other tile bits on the warp index, so the
+// exchange waits for the whole CTA; 0: every warp reads back only slots it
+// wrote itself, and a warp barrier suffices.
+constexpr int kMaxRotFlips = 12;
 // Optional first step of a launch: a diagonal that both states still owe,
 // applied at load time, and Z-type overlaps taken there (a diagonal with
 // |d| = 1 leaves conj(lam_j) psi_j unchanged, so before or after is the same).
@@ -167,6 +171,8 @@ struct pre_diag {
 struct pair_rotate_set {
   spin_group g;
   struct { int32_t out_slot, minus, okind, mkind; double wr, wi; double m[8]; } flip[kMaxRotFlips];
+  uint8_t block_sync[kSpinPhases];
+  uint8_t pad[4];
   pre_diag pre;
 };
 size_t pair_rotate_partials_doubles();  // per block: nflips overlap sums, then 1 + n Z sums when pre.nz > 0
