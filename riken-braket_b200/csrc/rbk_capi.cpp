@@ -1822,8 +1822,8 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
       if (int rc = apply_circuit_gate(psi.s, gates[i], theta, false)) return rc;
     if (int rc = canonicalize(psi.s)) return rc;
     const bool c128 = precision == RBK_C128;
-    cudaError_t e = c128 ? rbk::launch_pauli_apply<double>(psi.s->amps, lam.s->amps, num_qubits, H, psi.s->stream)
-                         : rbk::launch_pauli_apply<float>(psi.s->amps, lam.s->amps, num_qubits, H, psi.s->stream);
+    cudaError_t e = c128 ? rbk::launch_pauli_apply_tiled<double>(psi.s->amps, lam.s->amps, num_qubits, H, psi.s->stream)
+                         : rbk::launch_pauli_apply_tiled<float>(psi.s->amps, lam.s->amps, num_qubits, H, psi.s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "H psi");
     // E = <psi|lambda>
     e = c128 ? rbk::launch_inner<double>(lam.s->amps, psi.s->amps, num_qubits, psi.s->d_partials, ov.p + 2 * num_pg, psi.s->stream)

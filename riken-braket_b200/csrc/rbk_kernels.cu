@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <vector>
 
 #include "rbk_device.cuh"
 #include "rbk_internal.h"
@@ -525,6 +526,232 @@ cudaError_t launch_pauli_apply(const void* src, void* dst, int n, const pauli_su
     static_cast<const typename ctype<Real>::c*>(src), static_cast<typename ctype<Real>::c*>(dst), size, P);
   return cudaGetLastError();
 }
+
+// One pass of launch_pauli_apply_tiled: tile bits tile_phys[0..10] (the block
+// index deposited run by run into the other bits), the pass's groups as tile
+// masks of their flips and their terms.
+constexpr int kTileSumTerms = 96;
+constexpr int kTileSumBits = 11;
+// pair_group >= 0: that group's terms are all two-bit Z-type strings with one
+// real weight pw (ZZ couplings), and its weight at j is
+//   pw * (count - 2 * (number of pairs with odd parity at j)),
+// the pairs on adjacent bits counted at once as popcount((j ^ j >> 1) & madj)
+// and the others one by one from other[].
+constexpr int kTilePairOthers = 16;
+struct pauli_tile_pass {
+  int32_t num_groups, first;
+  uint8_t tile_phys[16], num_runs, run_src[16], run_len[16], run_dst[16];
+  uint8_t begin[kMaxSumGroups + 1];
+  uint16_t flip_local[kMaxSumGroups];
+  uint64_t sign[kTileSumTerms];
+  double w[kTileSumTerms][2];
+  int32_t pair_group, pair_count, num_others, pad;
+  double pw;
+  uint64_t madj;
+  uint8_t other[kTilePairOthers][2];
+};
+
+// Persistent CTAs, one tile of src at a time in shared memory; thread t holds
+// tile indices t + 256 it (it = 0..7), whose partners j ^ flip it reads from
+// the tile.  dst is written (first pass) or accumulated, in place.
+template <typename Real>
+__global__ void __launch_bounds__(kRedThreads)
+pauli_apply_tile_kernel(const typename ctype<Real>::c* __restrict__ src, typename ctype<Real>::c* __restrict__ dst,
+                        const __grid_constant__ pauli_tile_pass T, uint64_t num_tiles)
+{
+  using C = typename ctype<Real>::c;
+  constexpr int NE = 1 << (kTileSumBits - 8);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tile = reinterpret_cast<C*>(smem_raw);
+  const uint32_t tid = threadIdx.x;
+  uint64_t tphys = 0;
+  for (int b = 0; b < 8; ++b) tphys |= uint64_t((tid >> b) & 1u) << T.tile_phys[b];
+  for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+    uint64_t base = tphys;
+    for (int r = 0; r < T.num_runs; ++r) base |= ((t >> T.run_src[r]) & ((1ull << T.run_len[r]) - 1)) << T.run_dst[r];
+    uint64_t phys[NE];
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      phys[it] = base;
+#pragma unroll
+      for (int b = 0; b < kTileSumBits - 8; ++b)
+        if ((it >> b) & 1) phys[it] |= 1ull << T.tile_phys[8 + b];
+    }
+    // Both loads of the tile issued together: src, and the dst the pass adds to
+    // (read here, before any store to dst, so that the loads stay in flight at once).
+    C v[NE], d[NE];
+#pragma unroll
+    for (int it = 0; it < NE; ++it) v[it] = __ldcs(src + phys[it]);
+    if (!T.first) {
+#pragma unroll
+      for (int it = 0; it < NE; ++it) d[it] = __ldcs(dst + phys[it]);
+    }
+    __syncthreads();  // the previous tile is no longer read
+#pragma unroll
+    for (int it = 0; it < NE; ++it) tile[tid | (uint32_t(it) << 8)] = v[it];
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      const uint32_t j = tid | (uint32_t(it) << 8);
+      double re = 0.0, im = 0.0;
+      if (!T.first) {
+        re = double(d[it].x);
+        im = double(d[it].y);
+      }
+      for (int g = 0; g < T.num_groups; ++g) {
+        const C a = tile[j ^ T.flip_local[g]];
+        double wr = 0.0, wi = 0.0;
+        if (g == T.pair_group) {
+          const uint64_t x = phys[it];
+          int odd = __popcll((x ^ (x >> 1)) & T.madj);
+          for (int k = 0; k < T.num_others; ++k) odd += int(((x >> T.other[k][0]) ^ (x >> T.other[k][1])) & 1);
+          wr = T.pw * double(T.pair_count - 2 * odd);
+        } else {
+          for (int k = T.begin[g]; k < T.begin[g + 1]; ++k) {
+            const double sg = (__popcll(phys[it] & T.sign[k]) & 1) ? -1.0 : 1.0;
+            wr += sg * T.w[k][0];
+            wi += sg * T.w[k][1];
+          }
+        }
+        re += wr * double(a.x) - wi * double(a.y);
+        im += wr * double(a.y) + wi * double(a.x);
+      }
+      v[it] = C{(Real)re, (Real)im};
+    }
+#pragma unroll
+    for (int it = 0; it < NE; ++it) __stcs(dst + phys[it], v[it]);
+  }
+}
+
+template <typename Real>
+cudaError_t launch_pauli_apply_tiled(const void* src, void* dst, int n, const pauli_sum& P, cudaStream_t stream)
+{
+  constexpr int LOWB = 3, FREE = kTileSumBits - LOWB;
+  if (n < kTileSumBits || n > 63) return launch_pauli_apply<Real>(src, dst, n, P, stream);
+  // Group the flips into layouts: each layout's high bits (>= LOWB) number at most FREE.
+  std::vector<std::vector<int>> passes;
+  std::vector<uint64_t> highs;
+  int diag = -1;
+  for (int g = 0; g < P.num_groups; ++g) {
+    const uint64_t f = P.flip[g];
+    if (f == 0) { diag = g; continue; }
+    const uint64_t hb = f & ~((1ull << LOWB) - 1);
+    if (__builtin_popcountll(hb) > FREE) return launch_pauli_apply<Real>(src, dst, n, P, stream);
+    bool placed = false;
+    for (size_t q = 0; q < passes.size() && !placed; ++q) {
+      int terms = 0;
+      for (int h : passes[q]) terms += P.begin[h + 1] - P.begin[h];
+      if (__builtin_popcountll(highs[q] | hb) <= FREE && terms + (P.begin[g + 1] - P.begin[g]) <= kTileSumTerms &&
+          static_cast<int>(passes[q].size()) < kMaxSumGroups) {
+        passes[q].push_back(g);
+        highs[q] |= hb;
+        placed = true;
+      }
+    }
+    if (!placed) { passes.push_back({g}); highs.push_back(hb); }
+  }
+  if (passes.empty()) { passes.push_back({}); highs.push_back(0); }
+  if (diag >= 0) {
+    int terms = P.begin[diag + 1] - P.begin[diag];
+    for (int h : passes[0]) terms += P.begin[h + 1] - P.begin[h];
+    if (terms > kTileSumTerms) return launch_pauli_apply<Real>(src, dst, n, P, stream);
+    passes[0].insert(passes[0].begin(), diag);
+  }
+  static std::atomic<bool> configured[64] = {};
+  const size_t smem = sizeof(typename ctype<Real>::c) << kTileSumBits;
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!configured[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(pauli_apply_tile_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured[dev].store(true, std::memory_order_release);
+  }
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t tiles = 1ull << (n - kTileSumBits);
+  const int blocks = static_cast<int>(std::min<uint64_t>(tiles, uint64_t(sms) * 4));
+  for (size_t q = 0; q < passes.size(); ++q) {
+    pauli_tile_pass T{};
+    T.first = q == 0 ? 1 : 0;
+    std::vector<int> bits;
+    for (int b = 0; b < LOWB; ++b) bits.push_back(b);
+    for (int b = LOWB; b < n; ++b)
+      if ((highs[q] >> b) & 1) bits.push_back(b);
+    for (int b = LOWB; static_cast<int>(bits.size()) < kTileSumBits; ++b)  // fillers
+      if (!((highs[q] >> b) & 1)) bits.push_back(b);
+    std::sort(bits.begin(), bits.end());
+    uint64_t mask = 0;
+    for (int b = 0; b < kTileSumBits; ++b) { T.tile_phys[b] = static_cast<uint8_t>(bits[static_cast<size_t>(b)]); mask |= 1ull << bits[static_cast<size_t>(b)]; }
+    int runs = 0, srcb = 0;
+    for (int b = 0; b < n;) {
+      if ((mask >> b) & 1) { ++b; continue; }
+      int len = 0;
+      while (b + len < n && !((mask >> (b + len)) & 1)) ++len;
+      T.run_src[runs] = static_cast<uint8_t>(srcb);
+      T.run_len[runs] = static_cast<uint8_t>(len);
+      T.run_dst[runs] = static_cast<uint8_t>(b);
+      ++runs;
+      srcb += len;
+      b += len;
+    }
+    T.num_runs = static_cast<uint8_t>(runs);
+    int k = 0;
+    T.num_groups = static_cast<int>(passes[q].size());
+    for (int gi = 0; gi < T.num_groups; ++gi) {
+      const int g = passes[q][static_cast<size_t>(gi)];
+      uint32_t fl = 0;
+      for (int b = 0; b < kTileSumBits; ++b)
+        if ((P.flip[g] >> T.tile_phys[b]) & 1) fl |= 1u << b;
+      T.flip_local[gi] = static_cast<uint16_t>(fl);
+      T.begin[gi] = static_cast<uint8_t>(k);
+      for (int t = P.begin[g]; t < P.begin[g + 1]; ++t, ++k) {
+        T.sign[k] = P.sign[t];
+        T.w[k][0] = P.w[t][0];
+        T.w[k][1] = P.w[t][1];
+      }
+    }
+    T.begin[T.num_groups] = static_cast<uint8_t>(k);
+    // The ZZ-coupling form of the diagonal group, where it applies.
+    T.pair_group = -1;
+    if (q == 0 && diag >= 0 && P.begin[diag + 1] > P.begin[diag]) {
+      const int t0 = P.begin[diag], t1 = P.begin[diag + 1];
+      bool pairs = true;
+      uint64_t madj = 0;
+      int others = 0;
+      for (int t = t0; t < t1 && pairs; ++t) {
+        const uint64_t sg = P.sign[t];
+        pairs = __builtin_popcountll(sg) == 2 && P.w[t][1] == 0.0 && P.w[t][0] == P.w[t0][0];
+        if (!pairs) break;
+        const int a = __builtin_ctzll(sg), b = 63 - __builtin_clzll(sg);
+        if (b == a + 1 && !((madj >> a) & 1)) {
+          madj |= 1ull << a;
+        } else if (others < kTilePairOthers) {
+          T.other[others][0] = static_cast<uint8_t>(a);
+          T.other[others][1] = static_cast<uint8_t>(b);
+          ++others;
+        } else {
+          pairs = false;
+        }
+      }
+      if (pairs) {
+        T.pair_group = 0;  // the diagonal group is the pass's first
+        T.pair_count = t1 - t0;
+        T.pw = P.w[t0][0];
+        T.madj = madj;
+        T.num_others = others;
+      }
+    }
+    pauli_apply_tile_kernel<Real><<<blocks, kRedThreads, smem, stream>>>(
+      static_cast<const typename ctype<Real>::c*>(src), static_cast<typename ctype<Real>::c*>(dst), T, tiles);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+template cudaError_t launch_pauli_apply_tiled<double>(const void*, void*, int, const pauli_sum&, cudaStream_t);
+template cudaError_t launch_pauli_apply_tiled<float>(const void*, void*, int, const pauli_sum&, cudaStream_t);
 
 template <typename Real>
 cudaError_t launch_overlap(const void* lam, const void* psi, int n, uint64_t flip, uint64_t sign, double wr, double wi,

@@ -61,6 +61,13 @@ struct pauli_sum {
 };
 
 template <typename Real> cudaError_t launch_pauli_apply(const void* src, void* dst, int n, const pauli_sum& P, cudaStream_t stream);
+// The same sum in tiled passes: each pass takes the groups whose flip bits lie
+// in one tile layout (the low 3 bits plus up to 8 more), reads src once and
+// writes (first pass) or adds to dst; the diagonal group rides in the first
+// pass.  Falls back to launch_pauli_apply below 11 qubits or when a group's
+// flip does not fit one layout.
+template <typename Real> cudaError_t launch_pauli_apply_tiled(const void* src, void* dst, int n, const pauli_sum& P,
+                                                              cudaStream_t stream);
 // out (device, 2 doubles) = <lam| P |psi> with P = w (-1)^popcount(i & sign) X^flip
 template <typename Real> cudaError_t launch_overlap(const void* lam, const void* psi, int n, uint64_t flip, uint64_t sign,
                                                     double wr, double wi, double* partials, double* out, cudaStream_t stream);
