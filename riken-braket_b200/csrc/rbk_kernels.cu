@@ -601,7 +601,10 @@ pauli_apply_tile_kernel(const typename ctype<Real>::c* __restrict__ src, typenam
       for (int g = 0; g < T.num_groups; ++g) {
         const C a = tile[j ^ T.flip_local[g]];
         double wr = 0.0, wi = 0.0;
-        if (g == T.pair_group) {
+        if (T.begin[g + 1] == T.begin[g] + 1 && T.sign[T.begin[g]] == 0) {  // one term, no sign bits: a constant weight
+          wr = T.w[T.begin[g]][0];
+          wi = T.w[T.begin[g]][1];
+        } else if (g == T.pair_group) {
           const uint64_t x = phys[it];
           int odd = __popcll((x ^ (x >> 1)) & T.madj);
           for (int k = 0; k < T.num_others; ++k) odd += int(((x >> T.other[k][0]) ^ (x >> T.other[k][1])) & 1);
