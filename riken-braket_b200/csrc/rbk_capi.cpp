@@ -1491,7 +1491,10 @@ int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state*
     // B = 0..2, C = 3, 4 and a spare, D = 5..7.  A, B and C keep tile bits 5..7
     // on the warp index, so moving between them (and from C to the store) stays
     // inside each warp; only entering and leaving D needs the whole CTA.
-    // Groups without a gate are left out, except A.
+    // Groups without a gate are left out, except A.  In every layout the tile
+    // bits on lanes 0-2 reach distinct low bits of the swizzled shared-memory
+    // slot (rbk::smem_slot), so that the 8 lanes of a 128-byte wavefront hit
+    // distinct bank groups (c128).
     std::vector<int> local;      // tile bit of each register position
     std::vector<long> pos_item;  // index into items, -1 for a filler
     {
@@ -1501,7 +1504,7 @@ int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state*
           static_cast<long>(y);
       static const int groups[4][3] = {{8, 9, 10}, {0, 1, 2}, {3, 4, 0}, {5, 6, 7}};
       static const int thr_of[4][8] = {{0, 1, 2, 3, 4, 5, 6, 7}, {3, 4, 8, 9, 10, 5, 6, 7},
-                                       {1, 2, 8, 9, 10, 5, 6, 7}, {0, 1, 2, 3, 4, 8, 9, 10}};
+                                       {1, 2, 9, 8, 10, 5, 6, 7}, {0, 1, 2, 3, 4, 8, 9, 10}};
       int p = 0;
       int warps_of[rbk::kSpinPhases + 1] = {};
       for (int gi = 0; gi < 4; ++gi) {
