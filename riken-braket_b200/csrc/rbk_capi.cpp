@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "rbk_adjoint.h"
+#include "rbk_rotate_plan.h"
 #include "rbk_internal.h"
 #include "rbk_kernels.h"
 #include "rbk_plan.h"
@@ -1399,28 +1400,10 @@ int launch_paired_overlaps(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_
   return RBK_OK;
 }
 
-// One gate of a fused reverse run on its physical bit: the 2x2 matrix of U^dagger
-// and, for a rotation, its X / Y-type overlap (slot < 0: none).
-struct rotate_item {
-  int bit;
-  int slot;
-  rbk::overlap_spec spec;
-  double m[8];
-};
-
-// Pair-rotate launches over `items`: tiles of the low kPairLowBits bits plus up
-// to 8 others, up to kMaxRotFlips gates per launch, in register phases of
-// kPairRegBits gates (the layout of launch_paired_overlaps).
-// A diagonal both states owe (the queued records, in physical bits) and the
-// Z-type overlaps to take with it, for the first pair-rotate launch of a run.
-struct owed_diagonal {
-  rbk::pre_diag d{};
-  uint64_t full[rbk::kMaxQubits] = {};  // controlled-Z partners of each bit, both directions
-};
-
-// The queued records of s as an owed_diagonal (false when one of them is not a
-// one-bit diagonal or a controlled Z: a multi-controlled phase, for instance).
-bool owed_from_queue(const rbk_state* s, owed_diagonal& o)
+// The queued records of s as the diagonal both states owe (rbk::pre_diag in
+// physical bits: g, u, adj, full).  false when one of them is not a one-bit
+// diagonal or a controlled Z (a multi-controlled phase, for instance).
+bool owed_from_queue(const rbk_state* s, rbk::pre_diag& o)
 {
   using cplx_t = std::complex<double>;
   cplx_t g{1.0, 0.0};
@@ -1432,7 +1415,7 @@ bool owed_from_queue(const rbk_state* s, owed_diagonal& o)
         u[static_cast<size_t>(s->perm[__builtin_ctzll(h.cmask)])] *= -1.0;
       } else if (c == 2) {
         const int a = s->perm[__builtin_ctzll(h.cmask)], b = s->perm[63 - __builtin_clzll(h.cmask)];
-        o.d.adj[std::min(a, b)] ^= 1ull << std::max(a, b);
+        o.adj[std::min(a, b)] ^= 1ull << std::max(a, b);
         o.full[a] ^= 1ull << b;
         o.full[b] ^= 1ull << a;
       } else {
@@ -1451,135 +1434,24 @@ bool owed_from_queue(const rbk_state* s, owed_diagonal& o)
       return false;
     }
   }
-  o.d.g[0] = g.real();
-  o.d.g[1] = g.imag();
+  o.g[0] = g.real();
+  o.g[1] = g.imag();
   for (int b = 0; b < rbk::kMaxQubits; ++b) {
-    o.d.u[b][0] = u[static_cast<size_t>(b)].real();
-    o.d.u[b][1] = u[static_cast<size_t>(b)].imag();
+    o.u[b][0] = u[static_cast<size_t>(b)].real();
+    o.u[b][1] = u[static_cast<size_t>(b)].imag();
   }
   return true;
 }
 
-int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi, const std::vector<rotate_item>& items,
-                     double* ov, const owed_diagonal* owed)
+// Pair-rotate launches over `items` (rbk::plan_rotations), the owed diagonal,
+// if any, in the first.
+int launch_rotations(const rbk::adjoint_workspace& w, rbk_state* lam, rbk_state* psi,
+                     const std::vector<rbk::rotate_item>& items, double* ov, const rbk::pre_diag* owed)
 {
-  bool first_launch = true;
   const bool c128 = w.precision == RBK_C128;
-  const int n = w.n;
-  constexpr int RB = rbk::kPairRegBits, KT = kPairTileBits;
-  size_t next = 0;
-  while (next < items.size()) {
-    std::vector<int> tile_bits;
-    for (int b = 0; b < kPairLowBits; ++b) tile_bits.push_back(b);
-    std::vector<size_t> mine;
-    while (next < items.size() && static_cast<int>(mine.size()) < rbk::kMaxRotFlips) {
-      const int b = items[next].bit;
-      const bool in = std::find(tile_bits.begin(), tile_bits.end(), b) != tile_bits.end();
-      if (!in && static_cast<int>(tile_bits.size()) >= KT) break;
-      if (!in) tile_bits.push_back(b);
-      mine.push_back(next++);
-    }
-    for (int b = 0; static_cast<int>(tile_bits.size()) < KT; ++b)  // fillers
-      if (std::find(tile_bits.begin(), tile_bits.end(), b) == tile_bits.end()) tile_bits.push_back(b);
-    std::sort(tile_bits.begin(), tile_bits.end());
-    rbk::pair_rotate_set set{};
-    rbk::spin_group& g = set.g;
-    g.K = KT;
-    uint64_t mask = 0;
-    for (int b = 0; b < KT; ++b) { g.tile_phys[b] = static_cast<uint8_t>(tile_bits[static_cast<size_t>(b)]); mask |= 1ull << tile_bits[static_cast<size_t>(b)]; }
-    // Register phases, by groups of tile bits: A = 8..10 (the load layout),
-    // B = 0..2, C = 3, 4 and a spare, D = 5..7.  A, B and C keep tile bits 5..7
-    // on the warp index, so moving between them (and from C to the store) stays
-    // inside each warp; only entering and leaving D needs the whole CTA.
-    // Groups without a gate are left out, except A.  In every layout the tile
-    // bits on lanes 0-2 reach distinct low bits of the swizzled shared-memory
-    // slot (rbk::smem_slot), so that the 8 lanes of a 128-byte wavefront hit
-    // distinct bank groups (c128).
-    std::vector<int> local;      // tile bit of each register position
-    std::vector<long> pos_item;  // index into items, -1 for a filler
-    {
-      std::vector<long> gate_at(KT, -1);
-      for (size_t y : mine)
-        gate_at[static_cast<size_t>(std::find(tile_bits.begin(), tile_bits.end(), items[y].bit) - tile_bits.begin())] =
-          static_cast<long>(y);
-      static const int groups[4][3] = {{8, 9, 10}, {0, 1, 2}, {3, 4, 0}, {5, 6, 7}};
-      static const int thr_of[4][8] = {{0, 1, 2, 3, 4, 5, 6, 7}, {3, 4, 8, 9, 10, 5, 6, 7},
-                                       {1, 2, 9, 8, 10, 5, 6, 7}, {0, 1, 2, 3, 4, 8, 9, 10}};
-      int p = 0;
-      int warps_of[rbk::kSpinPhases + 1] = {};
-      for (int gi = 0; gi < 4; ++gi) {
-        const int nreal = gi == 2 ? 2 : 3;  // group C's third bit is a spare
-        bool any = gi == 0;
-        for (int k = 0; k < nreal; ++k) any = any || gate_at[static_cast<size_t>(groups[gi][k])] >= 0;
-        if (!any) continue;
-        for (int k = 0; k < RB; ++k) {
-          local.push_back(groups[gi][k]);
-          pos_item.push_back(k < nreal ? gate_at[static_cast<size_t>(groups[gi][k])] : -1);
-          g.phase_reg[p][k] = static_cast<uint8_t>(groups[gi][k]);
-        }
-        for (int b = 0; b < 8; ++b) g.phase_thr[p][b] = static_cast<uint8_t>(thr_of[gi][b]);
-        warps_of[p] = gi == 3 ? 1 : 0;
-        ++p;
-      }
-      g.nphases = p;
-      warps_of[p] = 0;  // the store reads in the load layout
-      for (int q = 0; q < p; ++q) set.block_sync[q] = warps_of[q] != warps_of[q + 1] ? 1 : 0;
-    }
-    g.nflips = static_cast<int>(local.size());
-    int runs = 0, src = 0;
-    for (int q = 0; q < n;) {
-      if ((mask >> q) & 1) { ++q; continue; }
-      int len = 0;
-      while (q + len < n && !((mask >> (q + len)) & 1)) ++len;
-      g.run_src[runs] = static_cast<uint8_t>(src);
-      g.run_len[runs] = static_cast<uint8_t>(len);
-      g.run_dst[runs] = static_cast<uint8_t>(q);
-      ++runs;
-      src += len;
-      q += len;
-    }
-    g.num_runs = runs;
-    for (size_t f = 0; f < local.size(); ++f) {
-      auto& fl = set.flip[f];
-      if (pos_item[f] < 0) {
-        fl.out_slot = -1;
-        fl.okind = 0;
-        fl.mkind = 2;
-        continue;
-      }
-      const rotate_item& it = items[static_cast<size_t>(pos_item[f])];
-      fl.out_slot = it.slot;
-      fl.minus = it.spec.sign != 0 ? 1 : 0;
-      fl.wr = it.spec.wr;
-      fl.wi = it.spec.wi;
-      fl.okind = it.slot < 0 ? 0 : (it.spec.wr == 0.0 ? 1 : 0) | (it.spec.wi == 0.0 ? 2 : 0);
-      if (it.slot >= 0 && fl.okind == 0) fl.okind = 3;
-      std::memcpy(fl.m, it.m, sizeof(fl.m));
-      fl.mkind = (it.m[1] == 0.0 && it.m[3] == 0.0 && it.m[5] == 0.0 && it.m[7] == 0.0) ? 1 : 0;
-    }
-    if (owed && first_launch) {
-      set.pre = owed->d;
-      set.pre.active = 1;
-      std::memcpy(set.pre.full, owed->full, sizeof(set.pre.full));
-      // The register slots' partner rows and their pairs among themselves.
-      set.pre.qr = 0;
-      for (int it = 0; it < (1 << RB); ++it) {
-        uint64_t mr = 0;
-        uint32_t par = 0;
-        for (int k = 0; k < RB; ++k) {
-          if (!((it >> k) & 1)) continue;
-          const int a = g.tile_phys[8 + k];
-          mr ^= owed->full[a];
-          for (int k2 = k + 1; k2 < RB; ++k2)
-            if ((it >> k2) & 1) par ^= static_cast<uint32_t>((owed->full[a] >> g.tile_phys[8 + k2]) & 1);
-        }
-        set.pre.mr[it] = mr;
-        set.pre.qr |= par << it;
-      }
-    }
-    first_launch = false;
-    const cudaError_t e = c128 ? rbk::launch_pair_rotate<double>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream)
-                               : rbk::launch_pair_rotate<float>(lam->amps, psi->amps, n, set, w.ppart, ov, psi->stream);
+  for (const rbk::pair_rotate_set& set : rbk::plan_rotations(w.n, items, owed)) {
+    const cudaError_t e = c128 ? rbk::launch_pair_rotate<double>(lam->amps, psi->amps, w.n, set, w.ppart, ov, psi->stream)
+                               : rbk::launch_pair_rotate<float>(lam->amps, psi->amps, w.n, set, w.ppart, ov, psi->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pair rotations");
   }
   return RBK_OK;
@@ -1948,15 +1820,15 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
         if (any_rotation) {
           // What both states owe, applied and summed in the first launch when it
           // is a product of one-bit diagonals and controlled Zs; else flushed.
-          owed_diagonal owed;
+          rbk::pre_diag owed{};
           bool use_owed = fused_pre && (!zpend.empty() || !psi.s->queue.empty()) &&
                           psi.s->queue.size() == lam.s->queue.size() && owed_from_queue(psi.s, owed);
           if (use_owed) {
-            owed.d.nz = static_cast<int>(zpend.size());
+            owed.nz = static_cast<int>(zpend.size());
             for (size_t k = 0; k < zpend.size(); ++k) {
-              owed.d.z[k].bit = zpend[k].first;
-              owed.d.z[k].out_slot = zpend[k].second;
-              owed.d.z[k].wr = 1.0;
+              owed.z[k].bit = zpend[k].first;
+              owed.z[k].out_slot = zpend[k].second;
+              owed.z[k].wr = 1.0;
             }
             zpend.clear();
             psi.s->queue.clear();
@@ -1967,12 +1839,12 @@ int rbk::adjoint_run(adjoint_workspace* w, const rbk_circuit_gate* gates, int nu
             if (int rc = flush(lam.s)) return rc;
           }
           if (psi.s->perm != lam.s->perm) return fail(RBK_ERR_STATE, "adjoint sweep: layouts diverged");
-          std::vector<rotate_item> items;
+          std::vector<rbk::rotate_item> items;
           for (int k = i; k > j; --k) {
             const hgate& h = recs[static_cast<size_t>(i - k)];
             if (is_diag(h)) continue;
             if (h.cmask != 0) return fail(RBK_ERR_STATE, "adjoint sweep: controlled gate in a one-qubit run");
-            rotate_item it{};
+            rbk::rotate_item it{};
             it.bit = psi.s->perm[gates[k].qubits[0]];
             it.slot = slot_of[static_cast<size_t>(i - k)];
             it.spec = rbk::overlap_spec{0, 0, 1.0, 0.0};
