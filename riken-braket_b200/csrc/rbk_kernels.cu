@@ -1264,24 +1264,33 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
     for (int q = tid; q < kMaxQubits * (kRedThreads / 32); q += kRedThreads) zh[q / (kRedThreads / 32)][q % (kRedThreads / 32)] = 0.0;
     __syncthreads();
   }
+  auto tile_base = [&](uint64_t t) {
+    uint64_t b = tphys;
+    for (int r = 0; r < S.num_runs; ++r) b |= ((t >> S.run_src[r]) & ((1ull << S.run_len[r]) - 1)) << S.run_dst[r];
+    return b;
+  };
+  // Phase 0 is the load layout (register bits = tile bits 8..10, thread bits
+  // 0..7): a tile goes from HBM straight into its registers.  The next tile's
+  // loads are issued before this tile's store, so that they are in flight
+  // while the store runs.
+  C el[NE], ep[NE];
+  auto load_tile = [&](uint64_t b) {
+#pragma unroll
+    for (int it = 0; it < NE; ++it) {
+      uint64_t p = b;
+#pragma unroll
+      for (int k = 0; k < RB; ++k)
+        if ((it >> k) & 1) p |= 1ull << S.tile_phys[8 + k];
+      el[it] = __ldcs(lam + p);
+      ep[it] = __ldcs(psi + p);
+    }
+  };
+  if (blockIdx.x < num_tiles) load_tile(tile_base(blockIdx.x));
   for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
-    uint64_t base = tphys;
-    for (int r = 0; r < S.num_runs; ++r) base |= ((t >> S.run_src[r]) & ((1ull << S.run_len[r]) - 1)) << S.run_dst[r];
-    // Phase 0 is the load layout (register bits = tile bits 8..10, thread bits
-    // 0..7): the tile goes from HBM straight into its registers.
-    C el[NE], ep[NE];
+    const uint64_t base = tile_base(t);
     {
       C* vl = el;
       C* vp = ep;
-#pragma unroll
-      for (int it = 0; it < NE; ++it) {
-        uint64_t p = base;
-#pragma unroll
-        for (int b = 0; b < RB; ++b)
-          if ((it >> b) & 1) p |= 1ull << S.tile_phys[8 + b];
-        vl[it] = __ldcs(lam + p);
-        vp[it] = __ldcs(psi + p);
-      }
       if (D.active) {
         if (D.nz > 0) {
           // Im conj(lam_j) psi_j: thread total, register-bit sums, and the warp's
@@ -1457,6 +1466,7 @@ pair_rotate_kernel(typename ctype<Real>::c* __restrict__ lam, typename ctype<Rea
     // kept from the loads, the eight of them would hold 16 registers through the phases.
     uint64_t sbase_hbm;
     asm volatile("mov.b64 %0, %1;" : "=l"(sbase_hbm) : "l"(base));
+    if (t + gridDim.x < num_tiles) load_tile(tile_base(t + gridDim.x));
 #pragma unroll
     for (int it = 0; it < NE; ++it) {
       const uint32_t s = st ^ smem_slot<VB>(uint32_t(it) << 8);
